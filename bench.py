@@ -1,0 +1,351 @@
+"""Benchmark of the split semi-Lagrangian step on B200.
+
+Default workload: Hernquist (M=1, a=1) on the 512x512x256 grid (513 x 513 x
+256 = 67,371,264 cells), r log-scaled on [0.01, 50], v_r linear on [-3, 3],
+J quadratic on [0, 3], dt = 0.0025, FP32-bulk path; the FP64 path is timed on
+the same grid for the FP32/FP64 ratio.  Metric: phase-space cell updates per
+second (N_r N_u N_J steps / device time).  The grid (269 MB FP32) is larger
+than L2 (126 MB), so no flush is needed between steps.
+
+Arms:
+  python bench.py [--gpus N --steps K --warmup W]      this library (CUDA)
+  python bench.py --impl reference ...                   the reference's own
+      CPU implementation (OpenMP, all host cores) on the same workload
+Multi-GPU: replicas only (one independent grid per rank, weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+WORKLOAD = dict(type="Hernquist", Pmin=0.01, Pmax=50.0, Pres=512, Pscale="logarithmic",
+                Umin=(-3.0, 0.0), Umax=(3.0, 3.0), Ures=(512, 256),
+                Uscale=("linear", "quadratic"), dt=0.0025)
+WORKLOAD_NAME = "hernquist_512x512x256"
+METRIC = "phase-space cell updates/s"
+REF_BIN = os.path.join(HERE, "oracle", "_ref", "vlasolve")
+
+
+def cells_of(w):
+    return (w["Pres"] + 1) * (w["Ures"][0] + 1) * w["Ures"][1]
+
+
+def config_json(w, precision):
+    return {"workload": WORKLOAD_NAME, "grid": [w["Pres"] + 1, w["Ures"][0] + 1, w["Ures"][1]],
+            "cells": cells_of(w), "profile": w["type"], "dt": w["dt"],
+            "precision": precision, "l2": "inputs larger than L2 (f is 269 MB FP32)",
+            "parallelism": "replicas"}
+
+
+def ref_args(w):
+    return ["-init.type", w["type"], "-grid.Pmin", repr(w["Pmin"]), "-grid.Pmax",
+            repr(w["Pmax"]), "-grid.Pres", str(w["Pres"]), "-grid.Pscale", w["Pscale"],
+            "-grid.Umin", repr(w["Umin"][0]), repr(w["Umin"][1]),
+            "-grid.Umax", repr(w["Umax"][0]), repr(w["Umax"][1]),
+            "-grid.Ures", str(w["Ures"][0]), str(w["Ures"][1]),
+            "-grid.Uscale", w["Uscale"][0], w["Uscale"][1], "-solver.dt", repr(w["dt"])]
+
+
+def run_reference(w, steps, threads):
+    """Time the reference binary's own loop ('Computed N timesteps in Ts',
+    vlasovSolver.hxx:184-186); returns (cell updates/s, seconds, steps)."""
+    tmp = tempfile.mkdtemp(prefix="vls_ref_")
+    try:
+        args = [REF_BIN, "-threads_per_node", str(threads), "-verbose", "0"] + ref_args(w) + [
+            "-solver.Tmax", repr(w["dt"] * steps), "-solver.statsEvery", "-1",
+            "-solver.snapshotEvery", "-1", "-solver.restartEvery", "-1"]
+        out = subprocess.run(args, cwd=tmp, capture_output=True, text=True, timeout=1800)
+        m = re.search(r"Computed (\d+) timesteps in ([0-9.eE+-]+)s", out.stdout)
+        if out.returncode != 0 or not m:
+            raise RuntimeError("reference run failed: " + out.stdout[-500:] + out.stderr[-500:])
+        n, t = int(m.group(1)), float(m.group(2))
+        return cells_of(w) * n / t, t, n
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def cpu_info():
+    model = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.p = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi") is None:
+            return self
+        fd, self.path = tempfile.mkstemp(prefix="vls_clk_", suffix=".csv")
+        os.close(fd)
+        self.p = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ GPU arm
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def time_steps(solver, steps, warmup, torch, dist):
+    """Device time of `steps` steps on the solver's stream (CUDA events)."""
+    stream = torch.cuda.ExternalStream(solver.stream_ptr())
+    solver.step(warmup)
+    solver.sync()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = solver.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.step(steps)
+    e1.record(stream)
+    solver.sync()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = solver.kernel_launches() - l0
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms, launches
+
+
+def gpu_arm(args):
+    import numpy as np
+    import torch
+    from vlasolve_b200 import VlasovSolver21Spline
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    w = dict(WORKLOAD)
+    cells = cells_of(w)
+    K, W = args.steps, args.warmup
+    peak, peak_kind = measured_peaks()
+
+    res = {}
+    for prec in (args.precision, "fp64") if args.precision != "fp64" else ("fp64",):
+        s = VlasovSolver21Spline(w, precision=prec, device=local)
+        st0 = s.stats()
+        with ClockSampler(local) as clk:
+            ms, launches = time_steps(s, K, W, torch, dist)
+        st1 = s.stats()
+        # per-kernel device times from the library's event profile (1 extra step set)
+        s.set_profiling(True)
+        s.step(min(K, 20))
+        prof = s.profile_read()
+        s.set_profiling(False)
+        res[prec] = dict(ms=ms, launches=launches, clocks=clk.summary(), prof=prof,
+                         dE=(st1["E"] - st0["E"]) / abs(st0["E"]), steps_done=s.stepCount,
+                         solver=s)
+        if prec != args.precision:
+            s.close()
+            res[prec].pop("solver")
+
+    main = res[args.precision]
+    ms = main["ms"]
+    value = world * cells * K / (ms * 1e-3)
+    esize = 4 if args.precision == "fp32" else 8
+    # dominant kernel and its roofline: algorithmic bytes = one read of its input
+    # field + one write of its output field per cell (8 B FP32 / 16 B FP64)
+    prof = main["prof"]
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms = prof[dom][0] / prof[dom][1]
+    algo_bytes = 2 * esize * cells
+    achieved = algo_bytes / (dom_ms * 1e-3) / 1e9
+    step_achieved = 4 * esize * cells * K / (ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(HERE, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dom)
+
+    # end to end through the C-ABI with pinned host buffers: upload the state,
+    # K steps each reading back the step's mass, download the state
+    s = main["solver"]
+    host = torch.empty(cells, dtype=torch.float64).pin_memory()
+    hnp = host.numpy()
+    s.get_f_into(hnp)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.set_f_from(hnp)
+    masses = []
+    for _ in range(K):
+        s.step(1)
+        masses.append(s.last_mass())
+    s.get_f_into(hnp)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * cells * K / e2e_s
+    s.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        model, ncores = cpu_info()
+        if os.path.exists(REF_BIN):
+            v, t, n = run_reference(w, args.cpu_steps, ncores)
+            cpu = {"value": v, "unit": "cell updates/s", "cores": ncores, "kind": "reference",
+                   "sample": f"{n} steps of the full {WORKLOAD_NAME} grid, OpenMP "
+                             f"{ncores} threads, {model}; reference's own loop timer",
+                   "seconds": t}
+        else:
+            cpu = {"value": None, "unit": "cell updates/s", "cores": 0, "kind": "reference",
+                   "sample": "reference binary not built"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell updates/s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+        "data": "synthetic (analytic Hernquist distribution function)",
+        "config": config_json(w, args.precision),
+        "gpu_launches": main["launches"],
+        "clocks": main["clocks"],
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": algo_bytes,
+                     "step_achieved": step_achieved, "step_frac": step_achieved / peak},
+        "kernels_ms_per_step": {k: v[0] / min(K, 20) for k, v in prof.items()},
+        "e2e": {"value": e2e, "unit": "cell updates/s",
+                "h2d_bytes_per_step": cells * 8 / K,
+                "d2h_bytes_per_step": (cells * 8 + 8 * K) / K},
+        "energy_drift_rel": {p: res[p]["dE"] for p in res},
+        "cpu_baseline": cpu,
+    }
+    if "fp64" in res and args.precision != "fp64":
+        v64 = world * cells * K / (res["fp64"]["ms"] * 1e-3)
+        line["fp64"] = {"value": v64, "ms_per_step": res["fp64"]["ms"] / K,
+                        "fp32_over_fp64": value / v64}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = dict(WORKLOAD)
+    model, ncores = cpu_info()
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference binary oracle/_ref/vlasolve was not built"}))
+        return
+    # each timed "step" is one reference step on the full grid; the run is
+    # bounded to a few minutes of host time
+    steps = max(1, min(args.steps, args.ref_max_steps))
+    v, t, n = run_reference(w, steps, ncores)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell updates/s",
+            "n_gpus": args.gpus, "steps": n, "warmup": 0, "ms_per_step": 1e3 * t / n,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic Hernquist distribution function)",
+            "config": config_json(w, "fp64"),
+            "cpu_baseline": {"value": v, "unit": "cell updates/s", "cores": ncores,
+                             "kind": "reference",
+                             "sample": f"{n} steps (of {args.steps} requested) of the full "
+                                       f"grid, {model}"},
+            "e2e": {"value": v, "unit": "cell updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--ref-max-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

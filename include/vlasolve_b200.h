@@ -1,0 +1,204 @@
+/*
+ * vlasolve_b200.h -- C-ABI of the B200 (sm_100a) split semi-Lagrangian step
+ * for the spherically symmetric (r, v_r, J) Vlasov-Poisson system.
+ *
+ * One handle owns one phase-space grid f(r, u=v_r, J) resident in the HBM of
+ * one GPU, the time-invariant footpoint tables of the drift, the delayed-kernel
+ * ring buffers and all scratch.  Every entry point returns an int status
+ * (VLS_OK = 0); a failed call leaves a message in vls_last_error().  No entry
+ * point aborts the process.  Calls on one handle are not re-entrant; distinct
+ * handles may be driven from distinct host threads.
+ *
+ * Layout of every host-side grid array: [j][u][r] with r fastest
+ * (slice21Iterator.hxx:63 of the reference), FP64.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the reference project's src/).  The reference has no C-ABI: the boundary
+ * is its C++ class surface (vlasovSolver21_spline / localSpline<2>), which the
+ * C++ adapter in include/vlasolve_b200.hpp mirrors on top of these calls.
+ */
+#ifndef VLASOLVE_B200_H
+#define VLASOLVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (the reference exits instead, e.g. localSpline.hxx:320-324,
+   typeSelect.hxx:29-38, vlasovSolver21.hxx:296-298) */
+enum {
+  VLS_OK = 0,
+  VLS_EINVAL = 1, /* invalid argument or configuration */
+  VLS_ECUDA = 2,  /* CUDA runtime error, or the CUDA path is unavailable */
+  VLS_ENAN = 3,   /* non-finite value detected in the grid */
+  VLS_EIO = 4,    /* file format / I/O error */
+  VLS_ENOMEM = 5, /* device or host allocation failed */
+  VLS_ESTATE = 6  /* call out of order (e.g. step before initialisation) */
+};
+
+/* scale::scaleTypeV, scale.hxx:17-19 */
+enum { VLS_SCALE_LINEAR = 0, VLS_SCALE_LOG = 1, VLS_SCALE_QUADRATIC = 2 };
+/* vlasovSolver21::kernelTypeV, vlasovSolver21.hxx:66-68 */
+enum { VLS_KERNEL_DELAYED = 0, VLS_KERNEL_REFLECTIVE = 1 };
+/* initGenAll registry, initGen_all.hxx:132-138 ("UDF", "PLDF", "Plummer",
+   "Hernquist") */
+enum { VLS_INIT_UDF = 0, VLS_INIT_PLDF = 1, VLS_INIT_PLUMMER = 2,
+       VLS_INIT_HERNQUIST = 3 };
+/* arithmetic/storage of the step.  FP64: every value FP64.  FP32_BULK: f,
+   spline coefficients and the gathers in FP32; prefilter recursions, footpoint
+   indexing, moments, enclosed-mass scan and statistics in FP64. */
+enum { VLS_FP64 = 0, VLS_FP32_BULK = 1 };
+
+/* gridBase::paramT, grid_base.hxx:58-82, i.e. the grid.* options
+   (grid_handler.hxx:224-238): r is index P, u and J are U[0] and U[1].
+   N_r = Pres+1 and N_u = Ures[0]+1 vertices, N_J = Ures[1] cells. */
+typedef struct {
+  double Pmin, Pmax;
+  int32_t Pres, Pscale;
+  double Umin[2], Umax[2];
+  int32_t Ures[2], Uscale[2];
+} vls_grid_desc;
+
+/* solverParam (solverParam.hxx:6-14) plus the solver.* options of
+   vlasovSolver21 (vlasovSolver21.hxx:537-539) and vlasovSolver.hxx:78 */
+typedef struct {
+  double G, T0, Tmax, dt;
+  int32_t noLinking;        /* solver.noLinking */
+  int32_t kernelType;       /* solver.kernelType: VLS_KERNEL_* */
+  int32_t kernelBufferSize; /* solver.kernelBufferSize */
+  int32_t precision;        /* VLS_FP64 or VLS_FP32_BULK */
+  int32_t device;           /* CUDA device ordinal */
+} vls_solver_desc;
+
+/* init.* options of the four profiles (initGen_UniformDensitySphere.hxx:49-62,
+   initGen_PowerLawDensitySphere.hxx:50-61, initGen_Plummer.hxx:45-48,
+   initGen_Hernquist.hxx:41-48).  R0_given = 0 lets PLDF take R0 = 1/eta. */
+typedef struct {
+  int32_t type; /* VLS_INIT_* */
+  double M, R0, alpha, smoothingRadius, gap[2], eta, n, Ra;
+  int32_t R0_given;
+} vls_init_desc;
+
+/* statistics row of vlasovSolver21::statistics, vlasovSolver21.hxx:644-690 */
+typedef struct {
+  double time;
+  int64_t step;
+  double Mass, E, Ek, Ep, S, L1, L2;
+} vls_stats_out;
+
+typedef struct vls_handle vls_handle;
+
+/* Build number of this library and whether a usable sm_100 device exists.
+   Replaces nothing in the reference (its binary has no device). */
+int vls_version(int32_t *major, int32_t *minor);
+int vls_device_ok(int32_t device);
+
+/* vlasovSolver21::setup + vlasovSolver21_spline::setup
+   (vlasovSolver21.hxx:411-446, :533-548; vlasovSolver21_spline.hxx:296-374):
+   coordinate tables, spline constants, kernel radius, host-tabulated drift
+   footpoints (generateDisplacement :102-204, decomposeDisplacement
+   vlasovSolver21_spline.hxx:76-117) and the delayed-kernel chain layout
+   (setupBoundaryConditions vlasovSolver21.hxx:265-326).  Allocates every
+   device buffer of the handle. */
+int vls_create(const vls_grid_desc *grid, const vls_solver_desc *solver,
+               vls_handle **out);
+/* ~vlasovSolver21_spline: frees the handle and all its device memory */
+int vls_destroy(vls_handle *h);
+/* message of the last failed call on h (or of the last vls_create failure
+   when h is NULL) */
+const char *vls_last_error(const vls_handle *h);
+
+/* grid_21.hxx:150-158 getValCoord21_* sizes */
+int vls_dims(const vls_handle *h, int64_t *nr, int64_t *nu, int64_t *nj);
+/* grid_21.hxx:150-158: R_Val (N_r), U_Val (N_u), J_Val (N_J), J_V (N_J+1) */
+int vls_coords(const vls_handle *h, double *R, double *U, double *J,
+               double *JV);
+/* initGen_*::generate + vlasovSolver21::renormalize(init->getMass(0), 0)
+   (vlasovSolver.hxx:83-96, vlasovSolver21.hxx:468-524): samples the profile
+   at every node, fills the chain values with init->valueAt and rescales both
+   so that the quadrature mass equals M.  Returns the pre-normalisation mass
+   in *mass_before (may be NULL). */
+int vls_init_profile(vls_handle *h, const vls_init_desc *init,
+                     double *mass_before);
+
+/* grid data access (gridBase::getDataPtr): FP64 host array of n = N_r*N_u*N_J
+   values in [j][u][r] order */
+int vls_set_f(vls_handle *h, const double *host, size_t n);
+int vls_get_f(vls_handle *h, double *host, size_t n);
+
+/* footpoint tables as decomposeDisplacement produces them
+   (vlasovSolver21_spline.hxx:69-72, :88-100) and disp_driftOut
+   (vlasovSolver21.hxx:94, :140-143); each array has N_r*N_u*N_J entries.
+   Any pointer may be NULL.  vls_set_footpoints replaces the tables (driftR is
+   only used for the kernel-radius test). */
+int vls_get_footpoints(const vls_handle *h, int32_t *rI, double *rF,
+                       int32_t *uI, double *uF, uint8_t *out, double *driftR);
+int vls_set_footpoints(vls_handle *h, const int32_t *rI, const double *rF,
+                       const int32_t *uI, const double *uF, const uint8_t *out,
+                       const double *driftR);
+
+/* delayed-kernel chains (sphericalKernel.hxx:21-24, cellChain.hxx:85-86) in
+   compressed-row form, in build order: per chain its cell index, first element
+   and length; per element R, U and value, logical front first (the last
+   element of a chain is its tail).  *n_chains / *n_elems report sizes when
+   the arrays are NULL. */
+int vls_get_chains(const vls_handle *h, int64_t *n_chains, int64_t *n_elems,
+                   int64_t *cell, int64_t *start, int32_t *len, double *R,
+                   double *U, double *val);
+int vls_set_chain_values(vls_handle *h, const double *val, int64_t n_elems);
+
+/* vlasovSolver::run body / vlasovSolver21_spline::makeOneStep
+   (vlasovSolver.hxx:158-180, vlasovSolver21_spline.hxx:680-801): nsteps
+   linked (or noLinking) steps on the device; time += dt and step += 1 per
+   step.  Asynchronous with respect to the host except for errors of the
+   launch itself; the handle's stream orders all later calls. */
+int vls_step(vls_handle *h, int32_t nsteps);
+/* wait for all work on the handle's stream; reports device-side errors */
+int vls_sync(vls_handle *h);
+/* number of kernels this handle has launched so far (diagnostic; the
+   reference has no device) */
+int vls_kernel_launches(const vls_handle *h, int64_t *n);
+/* the cudaStream_t every launch of this handle goes to (for CUDA-event
+   timing by the caller); the reference has no device */
+int vls_stream(const vls_handle *h, void **stream);
+/* per-kernel device timing: with profiling on, every launch is bracketed by
+   CUDA events on the handle's stream.  vls_profile_read synchronises, returns
+   the summed milliseconds and launch counts of each kernel kind
+   (VLS_K_* below, nk entries) and clears the record.  Diagnostic only. */
+enum { VLS_K_UCOL_KICK = 0, VLS_K_UCOL = 1, VLS_K_PRER = 2, VLS_K_TAILS = 3,
+       VLS_K_DRIFT = 4, VLS_K_SCAN = 5, VLS_K_MOMENT = 6, VLS_K_STATS = 7,
+       VLS_K_CONVERT = 8, VLS_K_COUNT = 9 };
+int vls_set_profiling(vls_handle *h, int32_t on);
+int vls_profile_read(vls_handle *h, double *ms, int64_t *count, int32_t nk);
+
+/* quadrature21::integrate1D_acc on the current f (vlasovSolver21_spline.hxx:736,
+   quadrature21.hxx:43-52, grid_handler.hxx:387-407): radial bins (N_r),
+   enclosed mass strictly inside R_r (N_r) and the total mass.  Any pointer may
+   be NULL. */
+int vls_moments(vls_handle *h, double *bins, double *Mr, double *mtot);
+/* mass of the most recent step's moment (the value the reference prints as
+   " (M=...)" each step, vlasovSolver21_spline.hxx:744) */
+int vls_last_mass(vls_handle *h, double *mtot);
+
+/* vlasovSolver21::statistics (vlasovSolver21.hxx:627-690) on the current f:
+   FP64 device reductions with compensated summation. */
+int vls_stats(vls_handle *h, vls_stats_out *out);
+
+/* time / step counters of vlasovSolver (vlasovSolver.hxx:202-204) */
+int vls_get_time(const vls_handle *h, double *time, int64_t *step);
+int vls_set_time(vls_handle *h, double time, int64_t step);
+
+/* NDfield snapshot of f (vlasovSolver21::snapshot / NDfieldFromData,
+   vlasovSolver21.hxx:585-598, :717-773; Save_NDfield NDfield.hxx:308-363) */
+int vls_write_ndfield(vls_handle *h, const char *path);
+/* reads the payload of an NDfield written by the reference or by
+   vls_write_ndfield into f (dims and datatype are checked) */
+int vls_read_ndfield(vls_handle *h, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

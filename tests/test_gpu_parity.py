@@ -1,0 +1,208 @@
+"""Parity of the CUDA path (through the C-ABI library) with the reference.
+
+The golden vectors were produced by the reference binary itself
+(tests/golden/make_golden.py); the CPU oracle reproduces them bit for bit
+(tests/test_oracle_golden.py) and supplies the quantities the reference does
+not dump (footpoint tables, moments).
+
+Tolerances, per the specification of the path:
+* integer work (footpoint indices, outside flags, chain layout) and the host
+  set-up (initial grid, chain values): bit-exact;
+* FP64 path: |f_gpu - f_ref| <= 1e-12 * max|f_ref| after every saved step
+  (the GPU solves the same spline systems with a different operation order);
+* FP32-bulk path: relative L2 error <= 2e-6 and max error <= 1e-5 * max|f_ref|
+  per saved step (FP32 storage and gathers, FP64 recursions).
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from oracle.vls_oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+SMALL = golden_cases(full_only=True)
+LARGE = golden_cases(full_only=False)
+
+FP64_TOL = 1e-12
+FP32_L2 = 2e-6
+FP32_MAX = 1e-5
+
+
+def solver(cfg, precision="fp64", **over):
+    from vlasolve_b200 import VlasovSolver21Spline
+    c = dict(cfg)
+    c.update(over)
+    return VlasovSolver21Spline(c, precision=precision)
+
+
+def _saved_steps(g, prefix):
+    return sorted(int(k[len(prefix):]) for k in g.files if k.startswith(prefix))
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_initial_state_and_chains_bitexact(name):
+    g, cfg = load_golden(name)
+    s = solver(cfg)
+    assert s.shape == tuple(g["shape"])
+    np.testing.assert_array_equal(s.f, g["f_0"])
+    ch = s.chains()
+    if "chain0_cell" in g.files:
+        for k in ("cell", "len", "R", "U", "val"):
+            np.testing.assert_array_equal(ch[k], g["chain0_" + k], err_msg=k)
+    else:
+        assert len(ch["cell"]) == 0
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_footpoints_bitexact(name):
+    g, cfg = load_golden(name)
+    s = solver(cfg)
+    o = Oracle(cfg)
+    a, b = s.footpoints(), o.footpoints()
+    for k in ("rI", "uI", "out", "rF", "uF", "driftR"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_fp64_steps_match_reference(name):
+    g, cfg = load_golden(name)
+    s = solver(cfg)
+    cur = 0
+    for st in _saved_steps(g, "f_"):
+        s.step(st - cur)
+        cur = st
+        ref = g["f_%d" % st]
+        err = np.abs(s.f - ref).max()
+        assert err <= FP64_TOL * np.abs(ref).max(), (name, st, err)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_fp32_steps_match_reference(name):
+    g, cfg = load_golden(name)
+    s = solver(cfg, "fp32")
+    cur = 0
+    for st in _saved_steps(g, "f_"):
+        s.step(st - cur)
+        cur = st
+        ref = g["f_%d" % st]
+        d = s.f - ref
+        l2 = np.linalg.norm(d) / np.linalg.norm(ref)
+        assert l2 <= FP32_L2, (name, st, l2)
+        assert np.abs(d).max() <= FP32_MAX * np.abs(ref).max(), (name, st)
+
+
+@pytest.mark.parametrize("name", ["udf_tiny", "plummer_small", "udf_nolink"])
+def test_moments_match_oracle(name):
+    g, cfg = load_golden(name)
+    s = solver(cfg)
+    o = Oracle(cfg)
+    for _ in range(2):
+        b1, M1, t1 = s.moments()
+        b2, M2, t2 = o.moments()
+        np.testing.assert_allclose(b1, b2, rtol=1e-13, atol=1e-15 * abs(t2))
+        np.testing.assert_allclose(M1, M2, rtol=1e-13, atol=1e-15 * abs(t2))
+        assert t1 == pytest.approx(t2, rel=1e-14)
+        s.step(1)
+        o.step(1)
+        o.f = s.f  # keep both on the same state
+
+
+@pytest.mark.parametrize("name", ["udf_tiny", "hernquist_small", "pldf_small"])
+def test_stats_match_reference(name):
+    g, cfg = load_golden(name)
+    s = solver(cfg)
+    ref = g["stats"]
+    for st in range(min(3, len(ref))):
+        row = s.stats()
+        got = [row[k] for k in ("Mass", "E", "Ek", "Ep", "S", "L1", "L2")]
+        # the reference prints 10 significant digits
+        np.testing.assert_allclose(got, ref[st][2:], rtol=2e-9, atol=1e-14)
+        s.step(1)
+
+
+@pytest.mark.parametrize("name", LARGE)
+def test_full_config_fp64_sampled(name):
+    g, cfg = load_golden(name)
+    s = solver(cfg)
+    idx = g["sample_idx"]
+    cur = 0
+    for st in _saved_steps(g, "fs_"):
+        s.step(st - cur)
+        cur = st
+        f = s.f
+        fs = f.ravel()[idx]
+        ref = g["fs_%d" % st]
+        scale = np.abs(ref).max()
+        if st == 0:
+            np.testing.assert_array_equal(fs, ref)
+        assert np.abs(fs - ref).max() <= FP64_TOL * scale, (name, st)
+        np.testing.assert_allclose(f.reshape(f.shape[0], -1).sum(axis=1),
+                                   g["slicesum_%d" % st], rtol=1e-11,
+                                   atol=1e-12 * np.abs(g["slicesum_%d" % st]).max())
+
+
+def test_full_config_fp32_hernquist_sampled():
+    g, cfg = load_golden("hernquist_cfg3")
+    s = solver(cfg, "fp32")
+    idx = g["sample_idx"]
+    cur = 0
+    for st in _saved_steps(g, "fs_"):
+        s.step(st - cur)
+        cur = st
+        fs = s.f.ravel()[idx]
+        ref = g["fs_%d" % st]
+        assert np.abs(fs - ref).max() <= FP32_MAX * np.abs(ref).max(), st
+
+
+def test_linearity_without_gravity_full_size():
+    """With G = 0 the kick shift vanishes and the step is linear in f (the
+    chains carry zeros): step(f1 + 2 f2) = step(f1) + 2 step(f2), checked on
+    the 513x513x256 grid where the oracle would be too slow."""
+    g, cfg = load_golden("hernquist_cfg3")
+    s = solver(cfg, "fp32", G=0.0)
+    s.set_chain_values(np.zeros(len(s.chains()["val"])))
+    rng = np.random.default_rng(7)
+    f0 = s.f
+    f1 = f0 * (1 + 0.1 * rng.standard_normal(f0.shape))
+    f2 = f0[::-1, :, :].copy()
+    outs = []
+    for x in (f1, f2, f1 + 2 * f2):
+        s.f = x
+        s.set_chain_values(np.zeros(len(s.chains()["val"])))
+        s.step(1)
+        outs.append(s.f)
+    lhs, rhs = outs[2], outs[0] + 2 * outs[1]
+    assert np.abs(lhs - rhs).max() <= 1e-6 * np.abs(rhs).max()
+
+
+def test_ndfield_roundtrip_and_layout():
+    g, cfg = load_golden("udf_tiny")
+    s = solver(cfg)
+    s.step(2)
+    f = s.f
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "snap.ND")
+        s.snapshot(p)
+        b = open(p, "rb").read()
+        n = f.size
+        assert len(b) == 688 + 8 * n + 4
+        np.testing.assert_array_equal(np.frombuffer(b[688:688 + 8 * n], "<f8"), f.ravel())
+        assert b[24 + 4: 24 + 4 + 11] == b"1 1 0 1 2 0"
+        s2 = solver(cfg)
+        s2.load_snapshot(p)
+        np.testing.assert_array_equal(s2.f, f)
+
+
+def test_bad_inputs_report_errors():
+    from vlasolve_b200 import _lib
+    g, cfg = load_golden("udf_tiny")
+    with pytest.raises(_lib.VlsError) as e:
+        solver(cfg, Pres=1)
+    assert e.value.code == _lib.VLS_EINVAL
+    s = solver(cfg)
+    with pytest.raises(_lib.VlsError):
+        s.load_snapshot("/nonexistent/file.ND")

@@ -1,0 +1,1107 @@
+// vls_api.cpp -- the C-ABI of include/vlasolve_b200.h: handle life cycle,
+// host set-up upload, step orchestration on the handle's CUDA stream,
+// moments, statistics and NDfield I/O.
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/vlasolve_b200.h"
+#include "vls_internal.h"
+#include "vls_setup.h"
+
+using namespace vls;
+
+struct vls_handle {
+  vls_grid_desc grid{};
+  vls_solver_desc solver{};
+  Coords co;
+  HostDirTables tr, tu;
+  int prec = VLS_FP64;
+  size_t esize = 8;
+  size_t cells = 0;
+  int pc = 0;
+  cudaStream_t st = nullptr;
+  // device buffers
+  void *f = nullptr, *G = nullptr, *C = nullptr;
+  int32_t *idx = nullptr;
+  void *fx = nullptr, *fy = nullptr;
+  int64_t nch = 0, nel = 0;
+  int64_t *ch_start = nullptr;
+  int32_t *ch_len = nullptr;
+  void *ch_val = nullptr;
+  int32_t *t_idx = nullptr;  // [nch] codes then [nch] slice index
+  double *t_x = nullptr, *t_y = nullptr;
+  double *rp_r = nullptr, *q_r = nullptr, *rp_u = nullptr, *q_u = nullptr;
+  double *dU_val = nullptr, *dR_val = nullptr, *dJ_val = nullptr;
+  double *d_dR = nullptr, *d_dU = nullptr, *d_Ct1 = nullptr;
+  double *bu = nullptr, *wj = nullptr, *dR4 = nullptr, *Rcoef = nullptr;
+  double *partial = nullptr, *T2 = nullptr, *bins = nullptr, *Mr = nullptr,
+         *shift = nullptr, *mtot = nullptr;
+  unsigned int *count = nullptr, *flag = nullptr;
+  double *stats_part = nullptr;
+  size_t stats_nblk = 0;
+  double *staging = nullptr;
+  size_t staging_n = 0;
+  // host copies of the chain layout
+  std::vector<int64_t> ch_cell_h, ch_start_h;
+  std::vector<int32_t> ch_len_h;
+  std::vector<double> ch_R_h, ch_U_h;
+  // state
+  bool have_f = false;
+  bool moments_valid = false;
+  int64_t ndrift = 0;
+  double time = 0;
+  int64_t step = 0;
+  int64_t launches = 0;
+  // opt-in per-kernel event timing
+  bool profiling = false;
+  struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof;
+  std::vector<cudaEvent_t> evpool;
+  std::string err;
+  std::vector<void *> allocs;
+};
+
+static std::string g_create_error;
+
+static int fail(vls_handle *h, int code, const std::string &msg) {
+  if (h)
+    h->err = msg;
+  else
+    g_create_error = msg;
+  return code;
+}
+
+#define CK(h, call)                                                       \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess)                                                \
+      return fail((h), VLS_ECUDA,                                         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+template <typename P>
+static int dalloc(vls_handle *h, P **p, size_t bytes) {
+  void *q = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, VLS_ENOMEM,
+                "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                    cudaGetErrorString(e));
+  }
+  h->allocs.push_back(q);
+  *p = reinterpret_cast<P *>(q);
+  return VLS_OK;
+}
+
+static int upload(vls_handle *h, void *dst, const void *src, size_t bytes) {
+  CK(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  return VLS_OK;
+}
+
+#define TRY(x)                 \
+  do {                         \
+    int s_ = (x);              \
+    if (s_ != VLS_OK) return s_; \
+  } while (0)
+
+static Geometry geometry(const vls_handle *h) {
+  Geometry g{};
+  g.nr = h->co.nr;
+  g.nu = h->co.nu;
+  g.nj = h->co.nj;
+  g.pc = h->pc;
+  g.U = h->dU_val;
+  g.Rsq = nullptr;
+  g.u0 = h->co.U.front();
+  g.umax = h->co.U.back();
+  g.su = h->co.sstart[1];
+  g.hu = h->co.sstep_inv[1];
+  return g;
+}
+
+static DirTables dir_tables(const HostDirTables &t, const double *rp,
+                            const double *q) {
+  DirTables d{};
+  d.rp = rp;
+  d.q = q;
+  d.a01 = t.a01;
+  d.a02 = t.a02;
+  d.hi2 = t.hi2;
+  d.L1 = t.L1;
+  d.L2 = t.L2;
+  d.M = t.M;
+  return d;
+}
+
+static MomentTables moment_tables(const vls_handle *h) {
+  MomentTables m{};
+  m.bu = h->bu;
+  m.wj = h->wj;
+  m.dR4 = h->dR4;
+  m.Rcoef = h->Rcoef;
+  return m;
+}
+
+static cudaEvent_t take_event(vls_handle *h) {
+  if (!h->evpool.empty()) {
+    cudaEvent_t e = h->evpool.back();
+    h->evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Runs one launch; counts it and, with profiling on, brackets it with events.
+template <typename F>
+static cudaError_t timed(vls_handle *h, int kind, F &&launch) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (h->profiling) {
+    a = take_event(h);
+    b = take_event(h);
+    cudaEventRecord(a, h->st);
+  }
+  const cudaError_t e = launch();
+  h->launches++;
+  if (h->profiling) {
+    cudaEventRecord(b, h->st);
+    h->prof.push_back({kind, a, b});
+  }
+  return e;
+}
+
+// ------------------------------------------------------------- footpoints
+// Encoding of one cell: -1 -> outside the box (value 0), <= -2 -> delayed
+// kernel chain (-2 - chain id), else rI | uI << 16.
+static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
+  const Coords &c = h->co;
+  const bool linked = !h->solver.noLinking;
+  const double dtd = linked ? h->solver.dt * 2 : h->solver.dt;
+  const bool refl = h->solver.kernelType == VLS_KERNEL_REFLECTIVE;
+  const size_t slice = (size_t)c.nr * c.nu;
+  const int batch = std::max(1, (int)std::min<size_t>(c.nj, (16u << 20) / slice));
+  std::vector<int32_t> idx(slice * batch);
+  std::vector<double> fx(slice * batch), fy(slice * batch);
+  std::vector<float> fx32, fy32;
+  if (h->prec == VLS_FP32_BULK) {
+    fx32.resize(slice * batch);
+    fy32.resize(slice * batch);
+  }
+  std::vector<SliceFootpoints> sfp(batch);
+  std::vector<SliceChains> sch(batch);
+  if (build_chains) {
+    h->ch_cell_h.clear();
+    h->ch_len_h.clear();
+    h->ch_R_h.clear();
+    h->ch_U_h.clear();
+  }
+  std::string bad;
+  for (int j0 = 0; j0 < c.nj; j0 += batch) {
+    const int nb = std::min(batch, c.nj - j0);
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < nb; b++) {
+      slice_footpoints(c, j0 + b, dtd, refl, sfp[b]);
+      if (build_chains && !refl) slice_chains(c, j0 + b, dtd, sfp[b], sch[b]);
+    }
+    // chain ids of this batch continue the running count, in slice order
+    int64_t chain_base = (int64_t)h->ch_cell_h.size();
+    for (int b = 0; b < nb; b++) {
+      const SliceFootpoints &fp = sfp[b];
+      int64_t next_chain = chain_base;
+      for (size_t i = 0; i < slice; i++) {
+        const size_t o = (size_t)b * slice + i;
+        int32_t code;
+        if (fp.driftR[i] < c.kernelRadius) {
+          code = refl ? -1 : (int32_t)(-2 - next_chain++);
+        } else if (fp.out[i]) {
+          code = -1;
+        } else {
+          const int32_t rI = fp.rI[i], uI = fp.uI[i];
+          if (rI < 0 || rI > c.nr - 1 || uI < 0 || uI > c.nu - 1) {
+            bad = "footpoint index outside the spline box at cell " +
+                  std::to_string((size_t)(j0 + b) * slice + i);
+            code = -1;
+          } else {
+            code = rI | (uI << 16);
+          }
+        }
+        idx[o] = code;
+        fx[o] = fp.rF[i];
+        fy[o] = fp.uF[i];
+      }
+      if (build_chains && !refl) {
+        const SliceChains &ch = sch[b];
+        if ((int64_t)ch.cell.size() != next_chain - chain_base)
+          bad = "chain bookkeeping mismatch";
+        h->ch_cell_h.insert(h->ch_cell_h.end(), ch.cell.begin(), ch.cell.end());
+        h->ch_len_h.insert(h->ch_len_h.end(), ch.len.begin(), ch.len.end());
+        h->ch_R_h.insert(h->ch_R_h.end(), ch.R.begin(), ch.R.end());
+        h->ch_U_h.insert(h->ch_U_h.end(), ch.U.begin(), ch.U.end());
+      }
+      chain_base = next_chain;
+    }
+    if (!bad.empty()) return fail(h, VLS_EINVAL, bad);
+    const size_t off = (size_t)j0 * slice, n = (size_t)nb * slice;
+    TRY(upload(h, h->idx + off, idx.data(), n * sizeof(int32_t)));
+    if (h->prec == VLS_FP64) {
+      TRY(upload(h, (double *)h->fx + off, fx.data(), n * sizeof(double)));
+      TRY(upload(h, (double *)h->fy + off, fy.data(), n * sizeof(double)));
+    } else {
+      for (size_t i = 0; i < n; i++) {
+        fx32[i] = (float)fx[i];
+        fy32[i] = (float)fy[i];
+      }
+      TRY(upload(h, (float *)h->fx + off, fx32.data(), n * sizeof(float)));
+      TRY(upload(h, (float *)h->fy + off, fy32.data(), n * sizeof(float)));
+    }
+  }
+  return VLS_OK;
+}
+
+// localSpline::evaluate(R, U) position decomposition of every chain tail
+// (vlasovSolver21_spline.hxx:776-786, localSpline.hxx:477-488)
+static int setup_chain_device(vls_handle *h) {
+  const Coords &c = h->co;
+  const int64_t nch = (int64_t)h->ch_cell_h.size();
+  h->nch = nch;
+  h->ch_start_h.resize(nch);
+  int64_t acc = 0;
+  for (int64_t k = 0; k < nch; k++) {
+    h->ch_start_h[k] = acc;
+    acc += h->ch_len_h[k];
+  }
+  h->nel = acc;
+  std::vector<int32_t> tcode(2 * std::max<int64_t>(nch, 1), 0);
+  std::vector<double> tx(std::max<int64_t>(nch, 1), 0), ty(std::max<int64_t>(nch, 1), 0);
+  for (int64_t k = 0; k < nch; k++) {
+    const int64_t e = h->ch_start_h[k] + h->ch_len_h[k] - 1;
+    const double R = h->ch_R_h[e], U = h->ch_U_h[e];
+    const int j = (int)(h->ch_cell_h[k] / ((int64_t)c.nr * c.nu));
+    tcode[nch + k] = j;
+    if ((U <= c.U.front()) || (U >= c.U.back())) {
+      tcode[k] = -1;
+      continue;
+    }
+    double xr = (rescale(R, c.rscale) - c.sstart[0]) * c.sstep_inv[0];
+    double yu = (rescale(U, c.uscale) - c.sstart[1]) * c.sstep_inv[1];
+    double ix, iy;
+    xr = std::modf(xr, &ix);
+    yu = std::modf(yu, &iy);
+    if (ix < 0 || ix > c.nr - 1 || iy < 0 || iy > c.nu - 1)
+      return fail(h, VLS_EINVAL,
+                  "a delayed-kernel chain tail lies outside the spline box "
+                  "(time step too large for this grid)");
+    tcode[k] = (int32_t)ix | ((int32_t)iy << 16);
+    tx[k] = xr;
+    ty[k] = yu;
+  }
+  const size_t es = h->esize;
+  TRY(dalloc(h, &h->ch_start, sizeof(int64_t) * std::max<int64_t>(nch, 1)));
+  TRY(dalloc(h, &h->ch_len, sizeof(int32_t) * std::max<int64_t>(nch, 1)));
+  TRY(dalloc(h, &h->ch_val, es * std::max<int64_t>(h->nel, 1)));
+  TRY(dalloc(h, &h->t_idx, sizeof(int32_t) * tcode.size()));
+  TRY(dalloc(h, &h->t_x, sizeof(double) * tx.size()));
+  TRY(dalloc(h, &h->t_y, sizeof(double) * ty.size()));
+  CK(h, cudaMemsetAsync(h->ch_val, 0, es * std::max<int64_t>(h->nel, 1), h->st));
+  if (nch) {
+    TRY(upload(h, h->ch_start, h->ch_start_h.data(), sizeof(int64_t) * nch));
+    TRY(upload(h, h->ch_len, h->ch_len_h.data(), sizeof(int32_t) * nch));
+  }
+  TRY(upload(h, h->t_idx, tcode.data(), sizeof(int32_t) * tcode.size()));
+  TRY(upload(h, h->t_x, tx.data(), sizeof(double) * tx.size()));
+  TRY(upload(h, h->t_y, ty.data(), sizeof(double) * ty.size()));
+  return VLS_OK;
+}
+
+// ------------------------------------------------------------- life cycle
+extern "C" int vls_version(int32_t *major, int32_t *minor) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  return VLS_OK;
+}
+
+extern "C" int vls_device_ok(int32_t device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return fail(nullptr, VLS_ECUDA, "no CUDA device " + std::to_string(device));
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess)
+    return fail(nullptr, VLS_ECUDA, "cudaGetDeviceProperties failed");
+  if (p.major < 10)
+    return fail(nullptr, VLS_ECUDA,
+                "device is sm_" + std::to_string(p.major * 10 + p.minor) +
+                    "; this library is built for sm_100a");
+  return VLS_OK;
+}
+
+static void free_all(vls_handle *h) {
+  for (auto &r : h->prof) {
+    h->evpool.push_back(r.a);
+    h->evpool.push_back(r.b);
+  }
+  h->prof.clear();
+  for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
+  h->evpool.clear();
+  for (void *p : h->allocs) cudaFree(p);
+  h->allocs.clear();
+  if (h->st) cudaStreamDestroy(h->st);
+  h->st = nullptr;
+}
+
+extern "C" int vls_create(const vls_grid_desc *grid,
+                          const vls_solver_desc *solver, vls_handle **out) {
+  if (!grid || !solver || !out)
+    return fail(nullptr, VLS_EINVAL, "vls_create: NULL argument");
+  *out = nullptr;
+  if (solver->precision != VLS_FP64 && solver->precision != VLS_FP32_BULK)
+    return fail(nullptr, VLS_EINVAL, "unknown precision");
+  if (solver->kernelType != VLS_KERNEL_DELAYED &&
+      solver->kernelType != VLS_KERNEL_REFLECTIVE)
+    return fail(nullptr, VLS_EINVAL, "unknown kernel type");
+  if (!(solver->dt > 0)) return fail(nullptr, VLS_EINVAL, "solver.dt must be > 0");
+  {
+    int s = vls_device_ok(solver->device);
+    if (s != VLS_OK) return s;
+  }
+  std::unique_ptr<vls_handle> h(new vls_handle());
+  h->grid = *grid;
+  h->solver = *solver;
+  h->prec = solver->precision;
+  h->esize = h->prec == VLS_FP64 ? 8 : 4;
+  h->time = solver->T0;
+  {
+    std::string e;
+    if (!make_coords(*grid, solver->kernelBufferSize, h->co, e))
+      return fail(nullptr, VLS_EINVAL, e);
+  }
+  const Coords &c = h->co;
+  if (c.nr > 2048) return fail(nullptr, VLS_EINVAL, "at most 2048 radial vertices");
+  h->cells = (size_t)c.nr * c.nu * c.nj;
+  h->pc = ((c.nr + 3) + 3) / 4 * 4;
+  h->tr = thomas_tables(c.nr, c.sstep_inv[0]);
+  h->tu = thomas_tables(c.nu, c.sstep_inv[1]);
+  if (cudaSetDevice(solver->device) != cudaSuccess)
+    return fail(nullptr, VLS_ECUDA, "cudaSetDevice failed");
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(nullptr, VLS_ECUDA, "cudaStreamCreate failed");
+
+  vls_handle *hp = h.get();
+  int s = VLS_OK;
+  auto A = [&](int st) {
+    if (s == VLS_OK) s = st;
+  };
+  const size_t es = h->esize, cells = h->cells;
+  A(dalloc(hp, &h->f, es * cells));
+  A(dalloc(hp, &h->G, es * (size_t)c.nj * (c.nu + 2) * c.nr));
+  A(dalloc(hp, &h->C, es * (size_t)c.nj * (c.nu + 3) * h->pc));
+  A(dalloc(hp, &h->idx, sizeof(int32_t) * cells));
+  A(dalloc(hp, &h->fx, es * cells));
+  A(dalloc(hp, &h->fy, es * cells));
+  A(dalloc(hp, &h->rp_r, sizeof(double) * h->tr.M));
+  A(dalloc(hp, &h->q_r, sizeof(double) * h->tr.M));
+  A(dalloc(hp, &h->rp_u, sizeof(double) * h->tu.M));
+  A(dalloc(hp, &h->q_u, sizeof(double) * h->tu.M));
+  A(dalloc(hp, &h->dU_val, sizeof(double) * c.nu));
+  A(dalloc(hp, &h->dR_val, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->dJ_val, sizeof(double) * c.nj));
+  A(dalloc(hp, &h->d_dR, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->d_dU, sizeof(double) * c.nu));
+  A(dalloc(hp, &h->d_Ct1, sizeof(double) * c.nj));
+  A(dalloc(hp, &h->bu, sizeof(double) * c.nu));
+  A(dalloc(hp, &h->wj, sizeof(double) * c.nj));
+  A(dalloc(hp, &h->dR4, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->Rcoef, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->partial, sizeof(double) * (size_t)c.nj * c.nr));
+  A(dalloc(hp, &h->T2, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->bins, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->Mr, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->shift, sizeof(double) * c.nr));
+  A(dalloc(hp, &h->mtot, sizeof(double) * 2));
+  A(dalloc(hp, &h->count, sizeof(unsigned int) * 4));
+  A(dalloc(hp, &h->flag, sizeof(unsigned int) * 4));
+  h->stats_nblk = (size_t)((c.nu + 7) / 8) * c.nj;
+  A(dalloc(hp, &h->stats_part, sizeof(double) * 8 * h->stats_nblk));
+  h->staging_n = std::min<size_t>(cells, (size_t)16 << 20);
+  if (h->prec != VLS_FP64) A(dalloc(hp, &h->staging, sizeof(double) * h->staging_n));
+  if (s != VLS_OK) {
+    g_create_error = hp->err;
+    free_all(hp);
+    return s;
+  }
+  auto fin = [&](int st) -> int {
+    if (st != VLS_OK) {
+      g_create_error = hp->err;
+      free_all(hp);
+    }
+    return st;
+  };
+  if (cudaMemsetAsync(h->C, 0, es * (size_t)c.nj * (c.nu + 3) * h->pc, h->st) !=
+          cudaSuccess ||
+      cudaMemsetAsync(h->count, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess)
+    return fin(fail(hp, VLS_ECUDA, "cudaMemsetAsync failed"));
+  // tables
+  std::vector<double> dR(c.nr), dU(c.nu), Ct1(c.nj), bu(c.nu), wj(c.nj), dR4(c.nr),
+      Rcoef(c.nr);
+  for (int r = 0; r < c.nr; r++) {
+    dR[r] = (r >= c.nr - 1) ? 0 : (c.R[r + 1] - c.R[r]);  // get_dR
+    dR4[r] = dR[r] * 0.25;
+    // vlasovSolver21_spline.hxx:746: Mr[i] *= G/(R*R)*dt
+    Rcoef[r] = h->solver.G / (c.R[r] * c.R[r]) * h->solver.dt;
+  }
+  for (int u = 0; u < c.nu; u++) dU[u] = (u >= c.nu - 1) ? 0 : (c.U[u + 1] - c.U[u]);
+  for (int u = 0; u < c.nu; u++) bu[u] = dU[u] + (u > 0 ? dU[u - 1] : 0.0);
+  for (int j = 0; j < c.nj; j++) {
+    // get_dJ compares j with the u-vertex count (slice21Iterator.hxx:86)
+    const double dJ = (j >= c.nu - 1) ? 0 : (c.JV[j + 1] - c.JV[j]);
+    Ct1[j] = 8 * M_PI * M_PI * c.J[j] * dJ;
+    wj[j] = Ct1[j];
+  }
+  int st2 = VLS_OK;
+  auto U2 = [&](void *d, const void *src, size_t b) {
+    if (st2 == VLS_OK) st2 = upload(hp, d, src, b);
+  };
+  U2(h->rp_r, h->tr.rp.data(), sizeof(double) * h->tr.M);
+  U2(h->q_r, h->tr.q.data(), sizeof(double) * h->tr.M);
+  U2(h->rp_u, h->tu.rp.data(), sizeof(double) * h->tu.M);
+  U2(h->q_u, h->tu.q.data(), sizeof(double) * h->tu.M);
+  U2(h->dU_val, c.U.data(), sizeof(double) * c.nu);
+  U2(h->dR_val, c.R.data(), sizeof(double) * c.nr);
+  U2(h->dJ_val, c.J.data(), sizeof(double) * c.nj);
+  U2(h->d_dR, dR.data(), sizeof(double) * c.nr);
+  U2(h->d_dU, dU.data(), sizeof(double) * c.nu);
+  U2(h->d_Ct1, Ct1.data(), sizeof(double) * c.nj);
+  U2(h->bu, bu.data(), sizeof(double) * c.nu);
+  U2(h->wj, wj.data(), sizeof(double) * c.nj);
+  U2(h->dR4, dR4.data(), sizeof(double) * c.nr);
+  U2(h->Rcoef, Rcoef.data(), sizeof(double) * c.nr);
+  if (fin(st2) != VLS_OK) return st2;
+  if (fin(encode_and_upload_footpoints(hp, true)) != VLS_OK) return VLS_EINVAL;
+  {
+    const int st3 = setup_chain_device(hp);
+    if (fin(st3) != VLS_OK) return st3;
+  }
+  *out = h.release();
+  return VLS_OK;
+}
+
+extern "C" int vls_destroy(vls_handle *h) {
+  if (!h) return VLS_OK;
+  cudaSetDevice(h->solver.device);
+  if (h->st) cudaStreamSynchronize(h->st);
+  free_all(h);
+  delete h;
+  return VLS_OK;
+}
+
+extern "C" const char *vls_last_error(const vls_handle *h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+extern "C" int vls_dims(const vls_handle *h, int64_t *nr, int64_t *nu,
+                        int64_t *nj) {
+  if (!h) return VLS_EINVAL;
+  if (nr) *nr = h->co.nr;
+  if (nu) *nu = h->co.nu;
+  if (nj) *nj = h->co.nj;
+  return VLS_OK;
+}
+
+extern "C" int vls_coords(const vls_handle *h, double *R, double *U, double *J,
+                          double *JV) {
+  if (!h) return VLS_EINVAL;
+  if (R) std::memcpy(R, h->co.R.data(), sizeof(double) * h->co.nr);
+  if (U) std::memcpy(U, h->co.U.data(), sizeof(double) * h->co.nu);
+  if (J) std::memcpy(J, h->co.J.data(), sizeof(double) * h->co.nj);
+  if (JV) std::memcpy(JV, h->co.JV.data(), sizeof(double) * (h->co.nj + 1));
+  return VLS_OK;
+}
+
+// ------------------------------------------------------------- f transfer
+static int put_f(vls_handle *h, const double *host) {
+  if (h->prec == VLS_FP64) {
+    CK(h, cudaMemcpyAsync(h->f, host, sizeof(double) * h->cells,
+                          cudaMemcpyHostToDevice, h->st));
+  } else {
+    for (size_t off = 0; off < h->cells; off += h->staging_n) {
+      const size_t n = std::min(h->staging_n, h->cells - off);
+      CK(h, cudaMemcpyAsync(h->staging, host + off, sizeof(double) * n,
+                            cudaMemcpyHostToDevice, h->st));
+      CK(h, timed(h, VLS_K_CONVERT, [&] {
+           return launch_convert_in<float>(h->staging, (float *)h->f + off, n, h->st);
+         }));
+    }
+  }
+  CK(h, cudaStreamSynchronize(h->st));
+  h->have_f = true;
+  h->moments_valid = false;
+  return VLS_OK;
+}
+
+static int take_f(vls_handle *h, double *host) {
+  if (h->prec == VLS_FP64) {
+    CK(h, cudaMemcpyAsync(host, h->f, sizeof(double) * h->cells,
+                          cudaMemcpyDeviceToHost, h->st));
+  } else {
+    for (size_t off = 0; off < h->cells; off += h->staging_n) {
+      const size_t n = std::min(h->staging_n, h->cells - off);
+      CK(h, timed(h, VLS_K_CONVERT, [&] {
+           return launch_convert_out<float>((const float *)h->f + off, h->staging, n,
+                                            h->st);
+         }));
+      CK(h, cudaMemcpyAsync(host + off, h->staging, sizeof(double) * n,
+                            cudaMemcpyDeviceToHost, h->st));
+    }
+  }
+  CK(h, cudaStreamSynchronize(h->st));
+  return VLS_OK;
+}
+
+extern "C" int vls_set_f(vls_handle *h, const double *host, size_t n) {
+  if (!h || !host) return fail(h, VLS_EINVAL, "vls_set_f: NULL argument");
+  if (n != h->cells) return fail(h, VLS_EINVAL, "vls_set_f: size mismatch");
+  CK(h, cudaSetDevice(h->solver.device));
+  return put_f(h, host);
+}
+
+extern "C" int vls_get_f(vls_handle *h, double *host, size_t n) {
+  if (!h || !host) return fail(h, VLS_EINVAL, "vls_get_f: NULL argument");
+  if (n != h->cells) return fail(h, VLS_EINVAL, "vls_get_f: size mismatch");
+  if (!h->have_f) return fail(h, VLS_ESTATE, "vls_get_f: no grid data yet");
+  CK(h, cudaSetDevice(h->solver.device));
+  return take_f(h, host);
+}
+
+// ----------------------------------------------------------- init profile
+extern "C" int vls_init_profile(vls_handle *h, const vls_init_desc *init,
+                                double *mass_before) {
+  if (!h || !init) return fail(h, VLS_EINVAL, "vls_init_profile: NULL argument");
+  if (init->type < VLS_INIT_UDF || init->type > VLS_INIT_HERNQUIST)
+    return fail(h, VLS_EINVAL, "unknown initial conditions type");
+  CK(h, cudaSetDevice(h->solver.device));
+  const Coords &c = h->co;
+  Profile pr;
+  pr.setup(*init, h->solver.G);
+  std::vector<double> f(h->cells);
+#pragma omp parallel for schedule(dynamic)
+  for (int j = 0; j < c.nj; j++)
+    for (int u = 0; u < c.nu; u++)
+      for (int r = 0; r < c.nr; r++)
+        f[((size_t)j * c.nu + u) * c.nr + r] = pr.value(c.R[r], c.U[u], c.J[j]);
+  // quadrature21::integrate (quadrature21.hxx:56-85) in its one-thread order
+  double mass = 0;
+  for (int j = 0; j < c.nj; j++) {
+    const double J = c.J[j];
+    const double dJ = (j >= c.nu - 1) ? 0 : (c.JV[j + 1] - c.JV[j]);
+    const double Ct1 = 8 * M_PI * M_PI * J * dJ;
+    for (int u = 0; u < c.nu; u++) {
+      const double dU = (u >= c.nu - 1) ? 0 : (c.U[u + 1] - c.U[u]);
+      if (dU <= 0) continue;
+      for (int r = 0; r < c.nr; r++) {
+        const double dR = (r >= c.nr - 1) ? 0 : (c.R[r + 1] - c.R[r]);
+        if (dR <= 0) continue;
+        const double *fi = &f[((size_t)j * c.nu + u) * c.nr + r];
+        const double avg = (fi[0] + fi[1] + fi[c.nr] + fi[c.nr + 1]) * 0.25;
+        mass += Ct1 * dU * dR * avg;
+      }
+    }
+  }
+  if (mass_before) *mass_before = mass;
+  // chain element values: init->valueAt at each element, tail 0
+  // (vlasovSolver21.hxx:307-320)
+  std::vector<double> vals(h->nel, 0.0);
+  for (int64_t k = 0; k < h->nch; k++) {
+    const int j = (int)(h->ch_cell_h[k] / ((int64_t)c.nr * c.nu));
+    const int64_t s0 = h->ch_start_h[k];
+    for (int32_t e = 0; e + 1 < h->ch_len_h[k]; e++)
+      vals[s0 + e] = pr.value(h->ch_R_h[s0 + e], h->ch_U_h[s0 + e], c.J[j]);
+  }
+  // vlasovSolver21::renormalize(init->getMass(0), 0) (vlasovSolver21.hxx:468-524)
+  if (init->M > 0) {
+    const double fac = init->M / mass;
+#pragma omp parallel for
+    for (long long i = 0; i < (long long)h->cells; i++) f[i] *= fac;
+    for (auto &v : vals) v *= fac;
+  }
+  TRY(put_f(h, f.data()));
+  TRY(vls_set_chain_values(h, vals.data(), h->nel));
+  h->ndrift = 0;
+  return VLS_OK;
+}
+
+// ----------------------------------------------------------------- chains
+extern "C" int vls_get_chains(const vls_handle *hc, int64_t *n_chains,
+                              int64_t *n_elems, int64_t *cell, int64_t *start,
+                              int32_t *len, double *R, double *U, double *val) {
+  vls_handle *h = const_cast<vls_handle *>(hc);
+  if (!h) return VLS_EINVAL;
+  if (n_chains) *n_chains = h->nch;
+  if (n_elems) *n_elems = h->nel;
+  if (cell) std::memcpy(cell, h->ch_cell_h.data(), sizeof(int64_t) * h->nch);
+  if (start) std::memcpy(start, h->ch_start_h.data(), sizeof(int64_t) * h->nch);
+  if (len) std::memcpy(len, h->ch_len_h.data(), sizeof(int32_t) * h->nch);
+  if (R) std::memcpy(R, h->ch_R_h.data(), sizeof(double) * h->nel);
+  if (U) std::memcpy(U, h->ch_U_h.data(), sizeof(double) * h->nel);
+  if (val && h->nel) {
+    // device ring buffers -> logical order (front first)
+    CK(h, cudaSetDevice(h->solver.device));
+    std::vector<double> phys(h->nel);
+    if (h->prec == VLS_FP64) {
+      CK(h, cudaMemcpyAsync(phys.data(), h->ch_val, sizeof(double) * h->nel,
+                            cudaMemcpyDeviceToHost, h->st));
+      CK(h, cudaStreamSynchronize(h->st));
+    } else {
+      std::vector<float> p32(h->nel);
+      CK(h, cudaMemcpyAsync(p32.data(), h->ch_val, sizeof(float) * h->nel,
+                            cudaMemcpyDeviceToHost, h->st));
+      CK(h, cudaStreamSynchronize(h->st));
+      for (int64_t i = 0; i < h->nel; i++) phys[i] = p32[i];
+    }
+    for (int64_t k = 0; k < h->nch; k++) {
+      const int64_t s0 = h->ch_start_h[k];
+      const int32_t L = h->ch_len_h[k];
+      for (int32_t e = 0; e < L; e++) val[s0 + e] = phys[s0 + (h->ndrift + e) % L];
+    }
+  }
+  return VLS_OK;
+}
+
+extern "C" int vls_set_chain_values(vls_handle *h, const double *val,
+                                    int64_t n_elems) {
+  if (!h) return VLS_EINVAL;
+  if (n_elems != h->nel) return fail(h, VLS_EINVAL, "chain element count mismatch");
+  if (!h->nel) return VLS_OK;
+  CK(h, cudaSetDevice(h->solver.device));
+  std::vector<double> phys(h->nel);
+  for (int64_t k = 0; k < h->nch; k++) {
+    const int64_t s0 = h->ch_start_h[k];
+    const int32_t L = h->ch_len_h[k];
+    for (int32_t e = 0; e < L; e++) phys[s0 + (h->ndrift + e) % L] = val[s0 + e];
+  }
+  if (h->prec == VLS_FP64) {
+    TRY(upload(h, h->ch_val, phys.data(), sizeof(double) * h->nel));
+  } else {
+    std::vector<float> p32(h->nel);
+    for (int64_t i = 0; i < h->nel; i++) p32[i] = (float)phys[i];
+    TRY(upload(h, h->ch_val, p32.data(), sizeof(float) * h->nel));
+  }
+  return VLS_OK;
+}
+
+// ------------------------------------------------------------- footpoints
+extern "C" int vls_get_footpoints(const vls_handle *hc, int32_t *rI, double *rF,
+                                  int32_t *uI, double *uF, uint8_t *out,
+                                  double *driftR) {
+  vls_handle *h = const_cast<vls_handle *>(hc);
+  if (!h) return VLS_EINVAL;
+  const Coords &c = h->co;
+  const double dtd = h->solver.noLinking ? h->solver.dt : h->solver.dt * 2;
+  const bool refl = h->solver.kernelType == VLS_KERNEL_REFLECTIVE;
+  const size_t slice = (size_t)c.nr * c.nu;
+#pragma omp parallel for schedule(dynamic)
+  for (int j = 0; j < c.nj; j++) {
+    SliceFootpoints fp;
+    slice_footpoints(c, j, dtd, refl, fp);
+    const size_t o = (size_t)j * slice;
+    for (size_t i = 0; i < slice; i++) {
+      if (rI) rI[o + i] = fp.rI[i];
+      if (rF) rF[o + i] = fp.rF[i];
+      if (uI) uI[o + i] = fp.uI[i];
+      if (uF) uF[o + i] = fp.uF[i];
+      if (out) out[o + i] = fp.out[i];
+      if (driftR) driftR[o + i] = fp.driftR[i];
+    }
+  }
+  return VLS_OK;
+}
+
+extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
+                                  const double *rF, const int32_t *uI,
+                                  const double *uF, const uint8_t *out,
+                                  const double *driftR) {
+  if (!h || !rI || !rF || !uI || !uF || !out || !driftR)
+    return fail(h, VLS_EINVAL, "vls_set_footpoints: NULL argument");
+  CK(h, cudaSetDevice(h->solver.device));
+  const Coords &c = h->co;
+  // the chain layout stays the one built at creation: cells whose footpoint
+  // falls inside the kernel radius must be the same cells
+  std::vector<int32_t> idx(h->cells);
+  int64_t next_chain = 0;
+  for (size_t i = 0; i < h->cells; i++) {
+    if (driftR[i] < c.kernelRadius) {
+      if (h->solver.kernelType == VLS_KERNEL_REFLECTIVE) {
+        idx[i] = -1;
+        continue;
+      }
+      if (next_chain >= h->nch || h->ch_cell_h[next_chain] != (int64_t)i)
+        return fail(h, VLS_EINVAL,
+                    "vls_set_footpoints: kernel cells differ from the chain layout");
+      idx[i] = (int32_t)(-2 - next_chain++);
+    } else if (out[i]) {
+      idx[i] = -1;
+    } else {
+      if (rI[i] < 0 || rI[i] > c.nr - 1 || uI[i] < 0 || uI[i] > c.nu - 1)
+        return fail(h, VLS_EINVAL, "vls_set_footpoints: index outside the grid");
+      idx[i] = rI[i] | (uI[i] << 16);
+    }
+  }
+  TRY(upload(h, h->idx, idx.data(), sizeof(int32_t) * h->cells));
+  if (h->prec == VLS_FP64) {
+    TRY(upload(h, h->fx, rF, sizeof(double) * h->cells));
+    TRY(upload(h, h->fy, uF, sizeof(double) * h->cells));
+  } else {
+    std::vector<float> a(h->cells), b(h->cells);
+    for (size_t i = 0; i < h->cells; i++) {
+      a[i] = (float)rF[i];
+      b[i] = (float)uF[i];
+    }
+    TRY(upload(h, h->fx, a.data(), sizeof(float) * h->cells));
+    TRY(upload(h, h->fy, b.data(), sizeof(float) * h->cells));
+  }
+  return VLS_OK;
+}
+
+// ------------------------------------------------------------------ step
+template <typename T>
+static int drift_once(vls_handle *h, bool kick) {
+  const Geometry g = geometry(h);
+  const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
+  const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
+  CK(h, timed(h, kick ? VLS_K_UCOL_KICK : VLS_K_UCOL, [&] {
+       return launch_ucol<T>(kick, (const T *)h->f, (T *)h->G, h->shift, g, tu, h->st);
+     }));
+  CK(h, timed(h, VLS_K_PRER, [&] {
+       return launch_prer<T>((const T *)h->G, (T *)h->C, g, tr, h->st);
+     }));
+  if (h->nch) {
+    CK(h, timed(h, VLS_K_TAILS, [&] {
+         return launch_chain_tails<T>((const T *)h->C, (T *)h->ch_val, h->ch_start,
+                                      h->ch_len, h->t_idx, h->t_x, h->t_y, h->nch,
+                                      h->ndrift, g, h->st);
+       }));
+  }
+  CK(h, timed(h, VLS_K_DRIFT, [&] {
+       return launch_drift<T>((const T *)h->C, (T *)h->f, h->idx, (const T *)h->fx,
+                              (const T *)h->fy, h->ch_start, h->ch_len,
+                              (const T *)h->ch_val, h->ndrift, moment_tables(h),
+                              h->partial, g, h->st);
+     }));
+  h->ndrift++;
+  h->moments_valid = true;
+  return VLS_OK;
+}
+
+template <typename T>
+static int ensure_moments(vls_handle *h) {
+  if (h->moments_valid) return VLS_OK;
+  const Geometry g = geometry(h);
+  CK(h, timed(h, VLS_K_MOMENT, [&] {
+       return launch_moment<T>((const T *)h->f, moment_tables(h), h->partial, g, h->st);
+     }));
+  h->moments_valid = true;
+  return VLS_OK;
+}
+
+static int scan_once(vls_handle *h) {
+  const Geometry g = geometry(h);
+  CK(h, timed(h, VLS_K_SCAN, [&] {
+       return launch_scan(h->partial, moment_tables(h), h->T2, h->bins, h->Mr,
+                          h->shift, h->mtot, h->count, g, h->st);
+     }));
+  return VLS_OK;
+}
+
+template <typename T>
+static int step_impl(vls_handle *h, int nsteps) {
+  for (int s = 0; s < nsteps; s++) {
+    if (h->solver.noLinking) TRY(drift_once<T>(h, false));
+    TRY(ensure_moments<T>(h));
+    TRY(scan_once(h));
+    TRY(drift_once<T>(h, true));
+    h->time += h->solver.dt;
+    h->step++;
+  }
+  return VLS_OK;
+}
+
+extern "C" int vls_step(vls_handle *h, int32_t nsteps) {
+  if (!h) return VLS_EINVAL;
+  if (nsteps < 0) return fail(h, VLS_EINVAL, "nsteps < 0");
+  if (!h->have_f) return fail(h, VLS_ESTATE, "vls_step before the grid was set");
+  CK(h, cudaSetDevice(h->solver.device));
+  return h->prec == VLS_FP64 ? step_impl<double>(h, nsteps)
+                             : step_impl<float>(h, nsteps);
+}
+
+extern "C" int vls_sync(vls_handle *h) {
+  if (!h) return VLS_EINVAL;
+  CK(h, cudaSetDevice(h->solver.device));
+  CK(h, cudaStreamSynchronize(h->st));
+  CK(h, cudaGetLastError());
+  return VLS_OK;
+}
+
+extern "C" int vls_kernel_launches(const vls_handle *h, int64_t *n) {
+  if (!h || !n) return VLS_EINVAL;
+  *n = h->launches;
+  return VLS_OK;
+}
+
+extern "C" int vls_stream(const vls_handle *h, void **stream) {
+  if (!h || !stream) return VLS_EINVAL;
+  *stream = (void *)h->st;
+  return VLS_OK;
+}
+
+extern "C" int vls_set_profiling(vls_handle *h, int32_t on) {
+  if (!h) return VLS_EINVAL;
+  h->profiling = on != 0;
+  return VLS_OK;
+}
+
+extern "C" int vls_profile_read(vls_handle *h, double *ms, int64_t *count,
+                                int32_t nk) {
+  if (!h) return VLS_EINVAL;
+  CK(h, cudaSetDevice(h->solver.device));
+  CK(h, cudaStreamSynchronize(h->st));
+  for (int k = 0; k < nk; k++) {
+    if (ms) ms[k] = 0;
+    if (count) count[k] = 0;
+  }
+  for (auto &r : h->prof) {
+    float t = 0;
+    CK(h, cudaEventElapsedTime(&t, r.a, r.b));
+    if (r.kind < nk) {
+      if (ms) ms[r.kind] += t;
+      if (count) count[r.kind]++;
+    }
+    h->evpool.push_back(r.a);
+    h->evpool.push_back(r.b);
+  }
+  h->prof.clear();
+  return VLS_OK;
+}
+
+// --------------------------------------------------------------- moments
+template <typename T>
+static int moments_impl(vls_handle *h) {
+  TRY(ensure_moments<T>(h));
+  return scan_once(h);
+}
+
+extern "C" int vls_moments(vls_handle *h, double *bins, double *Mr, double *mtot) {
+  if (!h) return VLS_EINVAL;
+  if (!h->have_f) return fail(h, VLS_ESTATE, "vls_moments before the grid was set");
+  CK(h, cudaSetDevice(h->solver.device));
+  TRY(h->prec == VLS_FP64 ? moments_impl<double>(h) : moments_impl<float>(h));
+  const int nr = h->co.nr;
+  if (bins)
+    CK(h, cudaMemcpyAsync(bins, h->bins, sizeof(double) * nr, cudaMemcpyDeviceToHost,
+                          h->st));
+  if (Mr)
+    CK(h, cudaMemcpyAsync(Mr, h->Mr, sizeof(double) * nr, cudaMemcpyDeviceToHost, h->st));
+  if (mtot)
+    CK(h, cudaMemcpyAsync(mtot, h->mtot, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  return VLS_OK;
+}
+
+extern "C" int vls_last_mass(vls_handle *h, double *mtot) {
+  if (!h || !mtot) return VLS_EINVAL;
+  CK(h, cudaSetDevice(h->solver.device));
+  CK(h, cudaMemcpyAsync(mtot, h->mtot, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  return VLS_OK;
+}
+
+// ------------------------------------------------------------------ stats
+static void two_sum_acc(double &s, double &c, double x) {
+  const double t = s + x;
+  const double bb = t - s;
+  c += (s - (t - bb)) + (x - bb);
+  s = t;
+}
+
+template <typename T>
+static int stats_impl(vls_handle *h, vls_stats_out *o) {
+  const Coords &c = h->co;
+  TRY(moments_impl<T>(h));
+  std::vector<double> bins(c.nr);
+  CK(h, cudaMemcpyAsync(bins.data(), h->bins, sizeof(double) * c.nr,
+                        cudaMemcpyDeviceToHost, h->st));
+  CK(h, timed(h, VLS_K_STATS, [&] {
+       return launch_stats<T>((const T *)h->f, h->dR_val, h->dU_val, h->dJ_val,
+                              h->d_dR, h->d_dU, h->d_Ct1, h->stats_part, nullptr,
+                              geometry(h), h->st);
+     }));
+  std::vector<double> part(8 * h->stats_nblk);
+  CK(h, cudaMemcpyAsync(part.data(), h->stats_part, sizeof(double) * part.size(),
+                        cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  double q[4];
+  for (int k = 0; k < 4; k++) {
+    double s = 0, cc = 0;
+    for (size_t b = 0; b < h->stats_nblk; b++) {
+      two_sum_acc(s, cc, part[b * 8 + 2 * k]);
+      two_sum_acc(s, cc, part[b * 8 + 2 * k + 1]);
+    }
+    q[k] = s + cc;
+  }
+  // vlasovSolver21::potentialEnergy (vlasovSolver21.hxx:627-642); the last
+  // shell (mass 0) is skipped instead of reading past R_Val
+  double M = 0, Ep = 0;
+  for (int i = 1; i < c.nr + 1; i++) {
+    const double Mi = bins[i - 1];
+    if (i < c.nr) {
+      const double r = 0.5 * (c.R[i - 1] + c.R[i]);
+      Ep -= (Mi * h->solver.G * M) / r;
+    }
+    M += Mi;
+  }
+  o->time = h->time;
+  o->step = h->step;
+  o->Mass = M;
+  o->Ek = q[0];
+  o->Ep = Ep;
+  o->E = q[0] + Ep;
+  o->S = q[1];
+  o->L1 = q[2];
+  o->L2 = q[3];
+  return VLS_OK;
+}
+
+extern "C" int vls_stats(vls_handle *h, vls_stats_out *out) {
+  if (!h || !out) return fail(h, VLS_EINVAL, "vls_stats: NULL argument");
+  if (!h->have_f) return fail(h, VLS_ESTATE, "vls_stats before the grid was set");
+  CK(h, cudaSetDevice(h->solver.device));
+  return h->prec == VLS_FP64 ? stats_impl<double>(h, out) : stats_impl<float>(h, out);
+}
+
+extern "C" int vls_get_time(const vls_handle *h, double *time, int64_t *step) {
+  if (!h) return VLS_EINVAL;
+  if (time) *time = h->time;
+  if (step) *step = h->step;
+  return VLS_OK;
+}
+
+extern "C" int vls_set_time(vls_handle *h, double time, int64_t step) {
+  if (!h) return VLS_EINVAL;
+  h->time = time;
+  h->step = step;
+  return VLS_OK;
+}
+
+// ---------------------------------------------------------------- NDfield
+// Save_NDfield (NDfield.hxx:308-363) of NDfieldFromData (vlasovSolver21.hxx:717-773)
+namespace {
+const int ND_MAX_DIMS = 20;
+const int ND_DOUBLE_T = 1 << 9;
+}  // namespace
+
+extern "C" int vls_write_ndfield(vls_handle *h, const char *path) {
+  if (!h || !path) return fail(h, VLS_EINVAL, "vls_write_ndfield: NULL argument");
+  if (!h->have_f) return fail(h, VLS_ESTATE, "no grid data");
+  std::vector<double> f(h->cells);
+  TRY(take_f(h, f.data()));
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) return fail(h, VLS_EIO, std::string("cannot open ") + path);
+  const vls_grid_desc &g = h->grid;
+  int dims[3] = {g.Pres + 1, g.Ures[0] + 1, g.Ures[1]};
+  double x0[3] = {g.Pmin, g.Umin[0], g.Umin[1]};
+  double delta[3] = {g.Pmax - g.Pmin, g.Umax[0] - g.Umin[0], g.Umax[1] - g.Umin[1]};
+  char comment[80];
+  std::memset(comment, 0, sizeof(comment));
+  // (Rscale, VERTEX=1, Uscale, VERTEX=1, Jscale, CELL=0)
+  std::snprintf(comment, sizeof(comment), "%d %d %d %d %d %d", g.Pscale, 1,
+                g.Uscale[0], 1, g.Uscale[1], 0);
+  char tag[16];
+  std::memset(tag, 0, sizeof(tag));
+  std::strcpy(tag, "NDFIELD");
+  char dummy[160];
+  std::memset(dummy, 0, sizeof(dummy));
+  int i = 16;
+  bool ok = true;
+  auto W = [&](const void *p, size_t sz, size_t n) {
+    ok = ok && std::fwrite(p, sz, n, fp) == n;
+  };
+  W(&i, sizeof(int), 1);
+  W(tag, 1, 16);
+  W(&i, sizeof(int), 1);
+  i = (int)(sizeof(int) * (ND_MAX_DIMS + 3) + sizeof(double) * (2 * ND_MAX_DIMS) +
+            (160 + 80) * sizeof(char));
+  W(&i, sizeof(int), 1);
+  W(comment, 1, 80);
+  const int ndims = 3;
+  W(&ndims, sizeof(int), 1);
+  W(dims, sizeof(int), 3);
+  W(dummy, sizeof(int), ND_MAX_DIMS - 3);
+  const int fdims_index = 0, dtype = ND_DOUBLE_T;
+  W(&fdims_index, sizeof(int), 1);
+  W(&dtype, sizeof(int), 1);
+  W(x0, sizeof(double), 3);
+  W(dummy, sizeof(double), ND_MAX_DIMS - 3);
+  W(delta, sizeof(double), 3);
+  W(dummy, sizeof(double), ND_MAX_DIMS - 3);
+  W(dummy, 1, 160);
+  W(&i, sizeof(int), 1);
+  // record marker is an int: nval*8 wraps above 2 GiB exactly as the
+  // reference's does (NDfield.hxx:355)
+  const int marker = (int)(uint32_t)(h->cells * sizeof(double));
+  W(&marker, sizeof(int), 1);
+  W(f.data(), sizeof(double), h->cells);
+  W(&marker, sizeof(int), 1);
+  if (std::fclose(fp) != 0) ok = false;
+  if (!ok) return fail(h, VLS_EIO, std::string("write failed: ") + path);
+  return VLS_OK;
+}
+
+extern "C" int vls_read_ndfield(vls_handle *h, const char *path) {
+  if (!h || !path) return fail(h, VLS_EINVAL, "vls_read_ndfield: NULL argument");
+  FILE *fp = std::fopen(path, "rb");
+  if (!fp) return fail(h, VLS_EIO, std::string("cannot open ") + path);
+  std::unique_ptr<FILE, int (*)(FILE *)> guard(fp, std::fclose);
+  int m0, m1, hs;
+  char tag[16];
+  if (std::fread(&m0, 4, 1, fp) != 1 || std::fread(tag, 1, 16, fp) != 16 ||
+      std::fread(&m1, 4, 1, fp) != 1 || m0 != 16 || m1 != 16 ||
+      std::strncmp(tag, "NDFIELD", 7) != 0)
+    return fail(h, VLS_EIO, "not an NDfield file (bad tag record)");
+  if (std::fread(&hs, 4, 1, fp) != 1 || hs != 652)
+    return fail(h, VLS_EIO, "unsupported NDfield header size");
+  char comment[80];
+  int ndims, dims[ND_MAX_DIMS], fdi, dtype;
+  if (std::fread(comment, 1, 80, fp) != 80 || std::fread(&ndims, 4, 1, fp) != 1 ||
+      std::fread(dims, 4, ND_MAX_DIMS, fp) != (size_t)ND_MAX_DIMS ||
+      std::fread(&fdi, 4, 1, fp) != 1 || std::fread(&dtype, 4, 1, fp) != 1)
+    return fail(h, VLS_EIO, "truncated NDfield header");
+  if (ndims != 3 || dims[0] != h->co.nr || dims[1] != h->co.nu || dims[2] != h->co.nj)
+    return fail(h, VLS_EIO, "NDfield dimensions do not match the grid");
+  if (dtype != ND_DOUBLE_T) return fail(h, VLS_EIO, "NDfield datatype is not DOUBLE");
+  if (std::fseek(fp, 4 + 16 + 4 + 4 + 652 + 4, SEEK_SET) != 0)
+    return fail(h, VLS_EIO, "seek failed");
+  int marker;
+  if (std::fread(&marker, 4, 1, fp) != 1 ||
+      marker != (int)(uint32_t)(h->cells * sizeof(double)))
+    return fail(h, VLS_EIO, "NDfield data record size mismatch");
+  std::vector<double> f(h->cells);
+  if (std::fread(f.data(), sizeof(double), h->cells, fp) != h->cells)
+    return fail(h, VLS_EIO, "truncated NDfield data");
+  CK(h, cudaSetDevice(h->solver.device));
+  return put_f(h, f.data());
+}

@@ -1,0 +1,91 @@
+// vls_internal.h -- device buffers of a handle and the kernel launchers.
+//
+// Device layout (HBM), one GPU holds everything:
+//   f      [N_J][N_u][N_r]          T (float or double), r fastest
+//   G      [N_J][N_u+2][N_r]        T: u-direction spline coefficients of the
+//                                     kicked f (rows 0 and N_u+1 are ghosts)
+//   C      [N_J][N_u+3][Pc]         T: 2D coefficients, Pc >= N_r+3; row N_u+2
+//                                     and columns >= N_r+2 stay zero (reads
+//                                     at index N exist for footpoints that
+//                                     land on the last vertex with weight 0)
+//   fp_idx [cells] int32            rI | uI<<16, -1 = outside, <= -2 = chain
+//   fp_x, fp_y [cells] T            fractional footpoint offsets
+//   chains: ch_start/int64, ch_len/int32 per chain, ch_val/T per element
+//           (ring buffer; logical front at (ndrift mod len)), tail footpoint
+//   partial [N_J][N_r] double       per-slice radial moment partial sums
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace vls {
+
+// Thomas tables of one direction of the natural-BC cubic B-spline solve
+// (localSpline.hxx:953-1182).  Row k of the padded line, M = dim + 2.
+struct DirTables {
+  const double *rp;  // 1/p_k (k = 1..M-2), device
+  const double *q;   // normalised super-diagonal q_k (k = 0..M-1), device
+  double a01, a02;   // normalised first row (-2, 1)
+  double hi2, L1, L2;  // last-row constants
+  int M;
+};
+
+struct Geometry {
+  int nr, nu, nj;
+  int pc;  // row pitch of C
+  const double *U;      // U_Val (nu)
+  const double *Rsq;    // unused placeholder for alignment of future data
+  double u0, umax;      // U_Val.front(), U_Val.back()
+  double su, hu;        // spline start / step_inv of u (rescaled, linear)
+};
+
+struct MomentTables {
+  const double *bu;  // a_u + a_{u-1}, a_u = dU_u (0 for the last vertex)
+  const double *wj;  // 8 pi^2 J_j dJ_j
+  const double *dR4; // dR_r / 4 (0 for the last vertex)
+  const double *Rcoef;  // G/(R_r^2) * dt
+};
+
+// launchers (vls_kernels.cu); all asynchronous on `st`
+template <typename T>
+cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
+                        const Geometry &g, const DirTables &tu, cudaStream_t st);
+template <typename T>
+cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr,
+                        cudaStream_t st);
+template <typename T>
+cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
+                         const T *fy, const int64_t *ch_start,
+                         const int32_t *ch_len, const T *ch_val,
+                         int64_t ndrift, const MomentTables &mt, double *partial,
+                         const Geometry &g, cudaStream_t st);
+template <typename T>
+cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
+                               const int32_t *ch_len, const int32_t *t_idx,
+                               const double *t_x, const double *t_y,
+                               int64_t nchains, int64_t ndrift,
+                               const Geometry &g, cudaStream_t st);
+template <typename T>
+cudaError_t launch_moment(const T *f, const MomentTables &mt, double *partial,
+                          const Geometry &g, cudaStream_t st);
+cudaError_t launch_scan(const double *partial, const MomentTables &mt,
+                        double *T2, double *bins, double *Mr, double *shift,
+                        double *mtot, unsigned int *count, const Geometry &g,
+                        cudaStream_t st);
+template <typename T>
+cudaError_t launch_stats(const T *f, const double *R, const double *U,
+                         const double *J, const double *dR, const double *dU,
+                         const double *Ct1, double *part, double *out4,
+                         const Geometry &g, cudaStream_t st);
+template <typename T>
+cudaError_t launch_convert_in(const double *src, T *dst, size_t n,
+                              cudaStream_t st);
+template <typename T>
+cudaError_t launch_convert_out(const T *src, double *dst, size_t n,
+                               cudaStream_t st);
+template <typename T>
+cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
+                             cudaStream_t st);
+
+}  // namespace vls

@@ -1,0 +1,702 @@
+// vls_kernels.cu -- sm_100a kernels of the split semi-Lagrangian step.
+//
+// Per step (linked mode, vlasovSolver21_spline.hxx:680-801):
+//   scan      radial moment partials -> bins -> enclosed mass -> kick shift
+//   ucol      per (J slice, strip of r columns): natural-BC spline solve along
+//             u, kick gather at U+shift(r), second solve along u of the kicked
+//             values -> G (u-direction coefficients of the kicked f)
+//   prer      per (J slice, rows of G): solve along r -> C (2D coefficients)
+//   drift     per cell: 4x4 gather of C at the host-tabulated footpoint, or the
+//             delayed-kernel ring-buffer front, or 0; radial moment partials
+//             of the result (the next step's moment) in the epilogue
+//   tails     per delayed-kernel chain: spline value at the chain tail
+//
+// The 2D prefilter of the reference (r-solves, then u-solves on every column,
+// localSpline.hxx:1238-1258) is applied here as u-solves then r-solves; the
+// tensor-product operator is the same.  The Thomas recursion of one line
+// (localSpline.hxx:953-1182) is split into segments that run in parallel:
+// each segment first replays K rows of the recursion before its start (the
+// forward and backward recursions contract by 2-sqrt(3) = 0.268 per row, so
+// K = 32 rows reach FP64 rounding and K = 20 rows reach 1e-11).  The per-row
+// coefficients are the reference's own (tabulated on the host in its
+// operation order).  Recursions run in FP64 in both precisions.
+#include <cstdio>
+
+#include "vls_internal.h"
+
+namespace vls {
+
+template <typename T>
+struct Prec;
+template <>
+struct Prec<double> {
+  static constexpr int K = 32;  // warm-up rows of a segment
+};
+template <>
+struct Prec<float> {
+  static constexpr int K = 20;
+};
+
+template <typename T>
+__device__ __forceinline__ T bv2(T x) {
+  return x * x * x;
+}
+template <typename T>
+__device__ __forceinline__ T bv1(T x) {
+  return T(1) + T(3) * x + T(3) * x * x - T(3) * x * x * x;
+}
+
+// ----------------------------------------------------------- segment solve
+// One line of the padded natural-BC system lives at b[k*ks], k = 0..M-1.  On
+// entry rows 1..M-2 hold the data; on exit rows 0..M-1 hold the coefficients.
+// A thread owns interior rows [k0, k1).  All four stages are separated by
+// __syncthreads() in the caller.
+template <int K>
+struct Seg {
+  template <typename S>
+  __device__ static double fwd_warm(const S *b, int ks, int k0,
+                                    const DirTables &t) {
+    double d = 0.0;
+    int ks0 = k0 - K;
+    if (ks0 < 1) ks0 = 1;
+    for (int k = ks0; k < k0; ++k)
+      d = ((double)b[k * ks] - d * (1.0 / 6.0)) * __ldg(t.rp + k);
+    return d;
+  }
+  template <typename S>
+  __device__ static void fwd_main(S *b, int ks, int k0, int k1, double d,
+                                  const DirTables &t) {
+    double dprev = d;
+    for (int k = k0; k < k1; ++k) {
+      dprev = d;
+      d = ((double)b[k * ks] - d * (1.0 / 6.0)) * __ldg(t.rp + k);
+      b[k * ks] = (S)d;
+    }
+    if (k1 == t.M - 1 && k1 > k0) {
+      // last row (localSpline.hxx:1145-1152): d = d_{M-2}, dprev = d_{M-3}
+      const double num = (0.0 - t.hi2 * dprev) - t.L1 * d;
+      b[(t.M - 1) * ks] = (S)(num / t.L2);
+    }
+  }
+  template <typename S>
+  __device__ static double bwd_warm(const S *b, int ks, int k1,
+                                    const DirTables &t) {
+    int kst = k1 + K - 1;
+    double c;
+    if (kst >= t.M - 2) {
+      kst = t.M - 2;
+      c = (double)b[(t.M - 1) * ks];
+    } else {
+      c = 0.0;
+    }
+    for (int k = kst; k >= k1; --k) c = (double)b[k * ks] - __ldg(t.q + k) * c;
+    return c;
+  }
+  template <typename S>
+  __device__ static void bwd_main(S *b, int ks, int k0, int k1, double c,
+                                  const DirTables &t) {
+    double cnext = c;
+    for (int k = k1 - 1; k >= k0; --k) {
+      cnext = c;
+      c = (double)b[k * ks] - __ldg(t.q + k) * c;
+      b[k * ks] = (S)c;
+    }
+    if (k0 == 1 && k1 > k0) {
+      // first row (localSpline.hxx:1171): c_0 = (0 - a01 c_1) - a02 c_2
+      b[0] = (S)((0.0 - t.a01 * c) - t.a02 * cnext);
+    }
+  }
+};
+
+// segment bounds: interior rows [1, M-1) split into nseg pieces of odd length
+__device__ __forceinline__ void seg_bounds(int M, int nseg, int s, int &k0,
+                                           int &k1) {
+  int n = M - 2;
+  int L = (n + nseg - 1) / nseg;
+  L |= 1;
+  k0 = 1 + s * L;
+  k1 = k0 + L;
+  if (k0 > M - 1) k0 = M - 1;
+  if (k1 > M - 1) k1 = M - 1;
+}
+
+template <int K, typename S>
+__device__ void solve_lines(S *base, int ks, int k0, int k1,
+                            const DirTables &t) {
+  double d = Seg<K>::fwd_warm(base, ks, k0, t);
+  __syncthreads();
+  Seg<K>::fwd_main(base, ks, k0, k1, d, t);
+  __syncthreads();
+  double c = Seg<K>::bwd_warm(base, ks, k1, t);
+  __syncthreads();
+  Seg<K>::bwd_main(base, ks, k0, k1, c, t);
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------ ucol
+// Block: TW columns (r) x SEG segments (u).  Shared: two buffers of
+// (N_u+3) rows x TW (row N_u+2 is an always-zero guard row).
+constexpr int UC_TW = 16;
+constexpr int UC_THREADS = 256;
+constexpr int UC_SEG = UC_THREADS / UC_TW;
+
+template <typename T, bool KICK>
+__global__ void __launch_bounds__(UC_THREADS)
+    ucol_kernel(const T *__restrict__ f, T *__restrict__ G,
+                const double *__restrict__ shift, Geometry g, DirTables tu) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *bufA = reinterpret_cast<T *>(smem_raw);
+  const int M = g.nu + 2;
+  const int rows = M + 1;
+  T *bufB = bufA + (size_t)rows * UC_TW;
+  const int tid = threadIdx.x;
+  const int col = tid % UC_TW;
+  const int seg = tid / UC_TW;
+  const int r0 = blockIdx.x * UC_TW;
+  const int j = blockIdx.y;
+  const int r = r0 + col;
+  const size_t fslice = (size_t)j * g.nu * g.nr;
+
+  for (int e = tid; e < g.nu * UC_TW; e += UC_THREADS) {
+    const int k = e / UC_TW + 1, c = e % UC_TW;
+    const int rr = r0 + c;
+    bufA[k * UC_TW + c] =
+        rr < g.nr ? f[fslice + (size_t)(k - 1) * g.nr + rr] : T(0);
+  }
+  if (tid < UC_TW) {
+    bufA[0 * UC_TW + tid] = T(0);
+    bufA[(M - 1) * UC_TW + tid] = T(0);
+    bufA[M * UC_TW + tid] = T(0);
+    bufB[0 * UC_TW + tid] = T(0);
+    bufB[(M - 1) * UC_TW + tid] = T(0);
+    bufB[M * UC_TW + tid] = T(0);
+  }
+  __syncthreads();
+  int k0, k1;
+  seg_bounds(M, UC_SEG, seg, k0, k1);
+  solve_lines<Prec<T>::K>(bufA + col, UC_TW, k0, k1, tu);
+
+  T *out = bufA;
+  if (KICK) {
+    // kick gather (localSpline.hxx:423-441 with the r-direction (1,4,1)/6
+    // weights folded into the u-only coefficients), vlasovSolver21_spline.hxx:758-763
+    const double s = (r < g.nr) ? __ldg(shift + r) : 0.0;
+    for (int k = k0; k < k1; ++k) {
+      const int u = k - 1;
+      const double newU = __ldg(g.U + u) + s;
+      T v = T(0);
+      if (!((newU <= g.u0) || (newU >= g.umax))) {
+        const double y = (newU - g.su) * g.hu;
+        const double fl = floor(y);
+        const T fr = (T)(y - fl);
+        const int Ny = 1 + (int)fl;
+        const T *cb = bufA + col;
+        v = (T(1) / T(6)) *
+            (bv2<T>(T(1) - fr) * cb[(Ny - 1) * UC_TW] +
+             bv1<T>(T(1) - fr) * cb[Ny * UC_TW] + bv1<T>(fr) * cb[(Ny + 1) * UC_TW] +
+             bv2<T>(fr) * cb[(Ny + 2) * UC_TW]);
+      }
+      bufB[k * UC_TW + col] = v;
+    }
+    __syncthreads();
+    solve_lines<Prec<T>::K>(bufB + col, UC_TW, k0, k1, tu);
+    out = bufB;
+  }
+  const size_t gslice = (size_t)j * M * g.nr;
+  for (int e = tid; e < M * UC_TW; e += UC_THREADS) {
+    const int k = e / UC_TW, c = e % UC_TW;
+    const int rr = r0 + c;
+    if (rr < g.nr) G[gslice + (size_t)k * g.nr + rr] = out[k * UC_TW + c];
+  }
+}
+
+template <typename T>
+cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
+                        const Geometry &g, const DirTables &tu, cudaStream_t st) {
+  const size_t smem = 2 * (size_t)(g.nu + 3) * UC_TW * sizeof(T);
+  dim3 grid((g.nr + UC_TW - 1) / UC_TW, g.nj);
+  if (kick) {
+    cudaFuncSetAttribute(ucol_kernel<T, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ucol_kernel<T, true><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
+  } else {
+    cudaFuncSetAttribute(ucol_kernel<T, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ucol_kernel<T, false><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ prer
+// Block: PR_ROWS rows of G x PR_SEG segments along r (one warp per row).
+constexpr int PR_SEG = 32;
+constexpr int PR_ROWS = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(PR_SEG *PR_ROWS)
+    prer_kernel(const T *__restrict__ G, T *__restrict__ C, Geometry g,
+                DirTables tr) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *buf = reinterpret_cast<T *>(smem_raw);
+  const int M = g.nr + 2;
+  const int LS = M + 1;
+  const int tid = threadIdx.x;
+  const int rho = tid / PR_SEG;
+  const int seg = tid % PR_SEG;
+  const int j = blockIdx.y;
+  const int kr0 = blockIdx.x * PR_ROWS;
+  const int nrows = g.nu + 2;
+  const size_t gslice = (size_t)j * nrows * g.nr;
+  for (int e = tid; e < PR_ROWS * g.nr; e += PR_SEG * PR_ROWS) {
+    const int p = e / g.nr, k = e % g.nr;
+    const int kr = kr0 + p;
+    buf[p * LS + k + 1] = kr < nrows ? G[gslice + (size_t)kr * g.nr + k] : T(0);
+  }
+  __syncthreads();
+  int k0, k1;
+  seg_bounds(M, PR_SEG, seg, k0, k1);
+  solve_lines<Prec<T>::K>(buf + rho * LS, 1, k0, k1, tr);
+  const size_t cslice = (size_t)j * (g.nu + 3) * g.pc;
+  for (int e = tid; e < PR_ROWS * M; e += PR_SEG * PR_ROWS) {
+    const int p = e / M, k = e % M;
+    const int kr = kr0 + p;
+    if (kr < nrows) C[cslice + (size_t)kr * g.pc + k] = buf[p * LS + k];
+  }
+}
+
+template <typename T>
+cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr,
+                        cudaStream_t st) {
+  const size_t smem = (size_t)PR_ROWS * (g.nr + 3) * sizeof(T);
+  dim3 grid((g.nu + 2 + PR_ROWS - 1) / PR_ROWS, g.nj);
+  cudaFuncSetAttribute(prer_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  prer_kernel<T><<<grid, PR_SEG * PR_ROWS, smem, st>>>(G, C, g, tr);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ gather
+// localSpline::evaluateC(int,double,int,double), localSpline.hxx:381-398:
+// taps at padded columns rI..rI+3 and rows uI..uI+3.
+template <typename T>
+__device__ __forceinline__ T eval2d(const T *__restrict__ Cj, int pc, int rI,
+                                    T x, int uI, T y) {
+  const T b2xI = bv2<T>(T(1) - x), b1xI = bv1<T>(T(1) - x);
+  const T b1x = bv1<T>(x), b2x = bv2<T>(x);
+  const T *p = Cj + (size_t)uI * pc + rI;
+  const T s0 = __ldg(p) * b2xI + __ldg(p + 1) * b1xI + __ldg(p + 2) * b1x +
+               __ldg(p + 3) * b2x;
+  p += pc;
+  const T s1 = __ldg(p) * b2xI + __ldg(p + 1) * b1xI + __ldg(p + 2) * b1x +
+               __ldg(p + 3) * b2x;
+  p += pc;
+  const T s2 = __ldg(p) * b2xI + __ldg(p + 1) * b1xI + __ldg(p + 2) * b1x +
+               __ldg(p + 3) * b2x;
+  p += pc;
+  const T s3 = __ldg(p) * b2xI + __ldg(p + 1) * b1xI + __ldg(p + 2) * b1x +
+               __ldg(p + 3) * b2x;
+  return (T(1) / T(36)) * (bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
+                           bv1<T>(y) * s2 + bv2<T>(y) * s3);
+}
+
+constexpr int DR_W = 8;  // warps per drift block
+
+template <typename T>
+__global__ void __launch_bounds__(32 * DR_W)
+    drift_kernel(const T *__restrict__ C, T *__restrict__ f,
+                 const int32_t *__restrict__ idx, const T *__restrict__ fx,
+                 const T *__restrict__ fy, const int64_t *__restrict__ ch_start,
+                 const int32_t *__restrict__ ch_len,
+                 const T *__restrict__ ch_val, int64_t ndrift, MomentTables mt,
+                 double *__restrict__ partial, Geometry g) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int r = blockIdx.x * 32 + lane;
+  const int j = blockIdx.y;
+  const T *Cj = C + (size_t)j * (g.nu + 3) * g.pc;
+  double acc = 0.0;
+  if (r < g.nr) {
+    for (int u = w; u < g.nu; u += DR_W) {
+      const size_t i = ((size_t)j * g.nu + u) * g.nr + r;
+      const int code = __ldg(idx + i);
+      T v;
+      if (code >= 0) {
+        v = eval2d<T>(Cj, g.pc, code & 0xffff, __ldg(fx + i), code >> 16,
+                      __ldg(fy + i));
+      } else if (code == -1) {
+        v = T(0);
+      } else {
+        const int64_t ch = -2 - (int64_t)code;
+        const int L = __ldg(ch_len + ch);
+        v = ch_val[__ldg(ch_start + ch) + ndrift % L];
+      }
+      f[i] = v;
+      acc += __ldg(mt.bu + u) * (double)v;
+    }
+  }
+  __shared__ double red[DR_W][32];
+  red[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && r < g.nr) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < DR_W; ++k) s += red[k][lane];
+    partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * s;
+  }
+}
+
+template <typename T>
+cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
+                         const T *fy, const int64_t *ch_start,
+                         const int32_t *ch_len, const T *ch_val,
+                         int64_t ndrift, const MomentTables &mt, double *partial,
+                         const Geometry &g, cudaStream_t st) {
+  dim3 grid((g.nr + 31) / 32, g.nj);
+  drift_kernel<T><<<grid, 32 * DR_W, 0, st>>>(C, f, idx, fx, fy, ch_start, ch_len,
+                                               ch_val, ndrift, mt, partial, g);
+  return cudaGetLastError();
+}
+
+// tails: chains are independent; the tail slot (ndrift+L-1) mod L differs
+// from the front slot read by the drift since every chain has L >= 2
+template <typename T>
+__global__ void chain_tail_kernel(const T *__restrict__ C, T *__restrict__ ch_val,
+                                  const int64_t *__restrict__ ch_start,
+                                  const int32_t *__restrict__ ch_len,
+                                  const int32_t *__restrict__ t_idx,
+                                  const double *__restrict__ t_x,
+                                  const double *__restrict__ t_y,
+                                  const int32_t *__restrict__ t_j,
+                                  int64_t nchains, int64_t ndrift, Geometry g) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchains) return;
+  const int L = ch_len[c];
+  const int code = t_idx[c];
+  T v = T(0);
+  if (code >= 0) {
+    const T *Cj = C + (size_t)t_j[c] * (g.nu + 3) * g.pc;
+    v = eval2d<T>(Cj, g.pc, code & 0xffff, (T)t_x[c], code >> 16, (T)t_y[c]);
+  }
+  ch_val[ch_start[c] + (ndrift + L - 1) % L] = v;
+}
+
+template <typename T>
+cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
+                               const int32_t *ch_len, const int32_t *t_idx,
+                               const double *t_x, const double *t_y,
+                               int64_t nchains, int64_t ndrift,
+                               const Geometry &g, cudaStream_t st) {
+  if (nchains == 0) return cudaSuccess;
+  // t_j (slice of each chain) is stored right after t_idx
+  const int32_t *t_j = t_idx + nchains;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((nchains + threads - 1) / threads);
+  chain_tail_kernel<T><<<blocks, threads, 0, st>>>(C, ch_val, ch_start, ch_len, t_idx,
+                                                   t_x, t_y, t_j, nchains, ndrift, g);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ moment
+template <typename T>
+__global__ void __launch_bounds__(32 * DR_W)
+    moment_kernel(const T *__restrict__ f, MomentTables mt,
+                  double *__restrict__ partial, Geometry g) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int r = blockIdx.x * 32 + lane;
+  const int j = blockIdx.y;
+  double acc = 0.0;
+  if (r < g.nr)
+    for (int u = w; u < g.nu; u += DR_W)
+      acc += __ldg(mt.bu + u) * (double)f[((size_t)j * g.nu + u) * g.nr + r];
+  __shared__ double red[DR_W][32];
+  red[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && r < g.nr) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < DR_W; ++k) s += red[k][lane];
+    partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * s;
+  }
+}
+
+template <typename T>
+cudaError_t launch_moment(const T *f, const MomentTables &mt, double *partial,
+                          const Geometry &g, cudaStream_t st) {
+  dim3 grid((g.nr + 31) / 32, g.nj);
+  moment_kernel<T><<<grid, 32 * DR_W, 0, st>>>(f, mt, partial, g);
+  return cudaGetLastError();
+}
+
+// -------------------------------------------------------------- scan
+// Compensated (double-double) arithmetic: TwoSum (Knuth) on hi, lo pairs.
+struct dd {
+  double hi, lo;
+};
+__device__ __forceinline__ dd dd_add(dd a, dd b) {
+  const double s = a.hi + b.hi;
+  const double bb = s - a.hi;
+  double e = (a.hi - (s - bb)) + (b.hi - bb);
+  e += a.lo + b.lo;
+  const double h = s + e;
+  return dd{h, e - (h - s)};
+}
+__device__ __forceinline__ dd dd_shfl_up(dd a, int d) {
+  return dd{__shfl_up_sync(0xffffffffu, a.hi, d),
+            __shfl_up_sync(0xffffffffu, a.lo, d)};
+}
+__device__ __forceinline__ dd dd_shfl_down(dd a, int d) {
+  return dd{__shfl_down_sync(0xffffffffu, a.hi, d),
+            __shfl_down_sync(0xffffffffu, a.lo, d)};
+}
+
+constexpr int SC_THREADS = 1024;
+constexpr int SC_RB = 32;  // r columns per reduction block
+
+// grid: ceil(N_r / SC_RB) blocks; each reduces partial[:, r-strip] over J
+// (compensated) into T2.  The last block to finish (threadfence reduction
+// pattern, no spin-wait) computes bins, the exclusive scan, mtot and shift.
+// `count` is a per-handle device counter that the last block resets to 0.
+
+__global__ void __launch_bounds__(SC_THREADS)
+    scan_kernel(const double *__restrict__ partial, MomentTables mt,
+                double *__restrict__ T2, double *__restrict__ bins,
+                double *__restrict__ Mr, double *__restrict__ shift,
+                double *__restrict__ mtot, unsigned int *count, Geometry g) {
+  __shared__ dd sh[SC_THREADS];
+  __shared__ bool last;
+  const int tid = threadIdx.x;
+  {
+    const int lr = tid % SC_RB, jg = tid / SC_RB;  // 32 groups of J
+    const int ngroups = SC_THREADS / SC_RB;
+    const int r = blockIdx.x * SC_RB + lr;
+    dd acc{0.0, 0.0};
+    if (r < g.nr)
+      for (int j = jg; j < g.nj; j += ngroups)
+        acc = dd_add(acc, dd{partial[(size_t)j * g.nr + r], 0.0});
+    sh[tid] = acc;
+    __syncthreads();
+    for (int s = ngroups / 2; s > 0; s >>= 1) {
+      if (jg < s) sh[tid] = dd_add(sh[tid], sh[tid + s * SC_RB]);
+      __syncthreads();
+    }
+    if (jg == 0 && r < g.nr) T2[r] = sh[tid].hi + sh[tid].lo;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    const unsigned int done = atomicAdd(count, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // bins (each thread up to 2 consecutive r), then a block-wide exclusive scan
+  const int per = (g.nr + SC_THREADS - 1) / SC_THREADS;  // 1 or 2
+  double b[2] = {0.0, 0.0};
+  dd loc{0.0, 0.0};
+  for (int q = 0; q < per; ++q) {
+    const int r = tid * per + q;
+    if (r < g.nr) {
+      const double t2 = *((volatile double *)T2 + r);
+      const double t3 = (r + 1 < g.nr) ? *((volatile double *)T2 + r + 1) : 0.0;
+      b[q] = (r < g.nr - 1) ? __ldg(mt.dR4 + r) * (t2 + t3) : 0.0;
+      bins[r] = b[q];
+      loc = dd_add(loc, dd{b[q], 0.0});
+    }
+  }
+  // inclusive warp scan of loc
+  const int lane = tid & 31, wid = tid >> 5;
+  dd inc = loc;
+  for (int d = 1; d < 32; d <<= 1) {
+    dd o = dd_shfl_up(inc, d);
+    if (lane >= d) inc = dd_add(inc, o);
+  }
+  __shared__ dd wsum[SC_THREADS / 32];
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    dd x = wsum[lane];
+    dd xi = x;
+    for (int d = 1; d < 32; d <<= 1) {
+      dd o = dd_shfl_up(xi, d);
+      if (lane >= d) xi = dd_add(xi, o);
+    }
+    wsum[lane] = dd_add(xi, dd{-x.hi, -x.lo});  // exclusive
+    if (lane == 31) *mtot = xi.hi + xi.lo;
+  }
+  __syncthreads();
+  dd ex = dd_add(wsum[wid], dd_add(inc, dd{-loc.hi, -loc.lo}));
+  for (int q = 0; q < per; ++q) {
+    const int r = tid * per + q;
+    if (r < g.nr) {
+      const double m = ex.hi + ex.lo;
+      Mr[r] = m;
+      shift[r] = m * __ldg(mt.Rcoef + r);
+      ex = dd_add(ex, dd{b[q], 0.0});
+    }
+  }
+  if (tid == 0) *count = 0u;
+}
+
+cudaError_t launch_scan(const double *partial, const MomentTables &mt,
+                        double *T2, double *bins, double *Mr, double *shift,
+                        double *mtot, unsigned int *count, const Geometry &g,
+                        cudaStream_t st) {
+  if (g.nr > 2 * SC_THREADS) return cudaErrorInvalidValue;
+  const unsigned blocks = (g.nr + SC_RB - 1) / SC_RB;
+  scan_kernel<<<blocks, SC_THREADS, 0, st>>>(partial, mt, T2, bins, Mr, shift, mtot,
+                                             count, g);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ stats
+// integrate() of Ek, S, L1, L2 (quadrature21.hxx:56-85, integrand21.hxx:82-145)
+// per block: one J slice, rows u = blockIdx.x*ST_U.., threads over r; block
+// partials in double-double, 4 quantities x (hi, lo).
+constexpr int ST_THREADS = 256;
+constexpr int ST_U = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(ST_THREADS)
+    stats_kernel(const T *__restrict__ f, const double *__restrict__ R,
+                 const double *__restrict__ U, const double *__restrict__ J,
+                 const double *__restrict__ dR, const double *__restrict__ dU,
+                 const double *__restrict__ Ct1, double *__restrict__ part,
+                 Geometry g) {
+  const int j = blockIdx.y;
+  const int u0 = blockIdx.x * ST_U;
+  dd acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  const double Jj = J[j], ct = Ct1[j];
+  for (int uu = 0; uu < ST_U; ++uu) {
+    const int u = u0 + uu;
+    if (u >= g.nu - 1) break;
+    const double du = dU[u];
+    if (du <= 0) continue;
+    const double um = U[u] + 0.5 * du;
+    for (int r = threadIdx.x; r < g.nr - 1; r += ST_THREADS) {
+      const double dr = dR[r];
+      if (dr <= 0) continue;
+      const size_t i = ((size_t)j * g.nu + u) * g.nr + r;
+      const double avg =
+          ((double)f[i] + (double)f[i + 1] + (double)f[i + g.nr] +
+           (double)f[i + g.nr + 1]) *
+          0.25;
+      const double rm = R[r] + 0.5 * dr;
+      const double w = ct * du * dr;
+      acc[0] = dd_add(acc[0], dd{w * (0.5 * avg * (um * um + Jj * Jj / (rm * rm))), 0});
+      acc[1] = dd_add(acc[1], dd{w * ((avg <= 0) ? 0.0 : -avg * log(avg)), 0});
+      acc[2] = dd_add(acc[2], dd{w * fabs(avg), 0});
+      acc[3] = dd_add(acc[3], dd{w * (avg * avg), 0});
+    }
+  }
+  for (int q = 0; q < 4; ++q)
+    for (int d = 16; d > 0; d >>= 1) acc[q] = dd_add(acc[q], dd_shfl_down(acc[q], d));
+  __shared__ dd ws[ST_THREADS / 32][4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int q = 0; q < 4; ++q) ws[wid][q] = acc[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+    for (int q = 0; q < 4; ++q) {
+      dd s{0, 0};
+      for (int k = 0; k < ST_THREADS / 32; ++k) s = dd_add(s, ws[k][q]);
+      part[b * 8 + 2 * q] = s.hi;
+      part[b * 8 + 2 * q + 1] = s.lo;
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_stats(const T *f, const double *R, const double *U,
+                         const double *J, const double *dR, const double *dU,
+                         const double *Ct1, double *part, double *out4,
+                         const Geometry &g, cudaStream_t st) {
+  (void)out4;
+  dim3 grid((g.nu + ST_U - 1) / ST_U, g.nj);
+  stats_kernel<T><<<grid, ST_THREADS, 0, st>>>(f, R, U, J, dR, dU, Ct1, part, g);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ conversions
+template <typename T>
+__global__ void convert_in_kernel(const double *__restrict__ s, T *__restrict__ d,
+                                  size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    d[i] = (T)s[i];
+}
+template <typename T>
+__global__ void convert_out_kernel(const T *__restrict__ s, double *__restrict__ d,
+                                   size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    d[i] = (double)s[i];
+}
+template <typename T>
+__global__ void nonfinite_kernel(const T *__restrict__ s, size_t n,
+                                 unsigned int *flag) {
+  unsigned int bad = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    bad |= !isfinite((double)s[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+static unsigned grid_for(size_t n) {
+  size_t b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b == 0) b = 1;
+  return (unsigned)b;
+}
+
+template <typename T>
+cudaError_t launch_convert_in(const double *src, T *dst, size_t n,
+                              cudaStream_t st) {
+  convert_in_kernel<T><<<grid_for(n), 256, 0, st>>>(src, dst, n);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_convert_out(const T *src, double *dst, size_t n,
+                               cudaStream_t st) {
+  convert_out_kernel<T><<<grid_for(n), 256, 0, st>>>(src, dst, n);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
+                             cudaStream_t st) {
+  nonfinite_kernel<T><<<grid_for(n), 256, 0, st>>>(f, n, flag);
+  return cudaGetLastError();
+}
+
+#define VLS_INST(T)                                                            \
+  template cudaError_t launch_ucol<T>(bool, const T *, T *, const double *,     \
+                                      const Geometry &, const DirTables &,      \
+                                      cudaStream_t);                            \
+  template cudaError_t launch_prer<T>(const T *, T *, const Geometry &,         \
+                                      const DirTables &, cudaStream_t);         \
+  template cudaError_t launch_drift<T>(                                         \
+      const T *, T *, const int32_t *, const T *, const T *, const int64_t *,    \
+      const int32_t *, const T *, int64_t, const MomentTables &, double *,       \
+      const Geometry &, cudaStream_t);                                          \
+  template cudaError_t launch_chain_tails<T>(                                   \
+      const T *, T *, const int64_t *, const int32_t *, const int32_t *,         \
+      const double *, const double *, int64_t, int64_t, const Geometry &,       \
+      cudaStream_t);                                                            \
+  template cudaError_t launch_moment<T>(const T *, const MomentTables &,        \
+                                        double *, const Geometry &,             \
+                                        cudaStream_t);                          \
+  template cudaError_t launch_stats<T>(                                         \
+      const T *, const double *, const double *, const double *,                \
+      const double *, const double *, const double *, double *, double *,       \
+      const Geometry &, cudaStream_t);                                          \
+  template cudaError_t launch_convert_in<T>(const double *, T *, size_t,        \
+                                            cudaStream_t);                      \
+  template cudaError_t launch_convert_out<T>(const T *, double *, size_t,       \
+                                             cudaStream_t);                     \
+  template cudaError_t launch_nonfinite<T>(const T *, size_t, unsigned int *,   \
+                                           cudaStream_t);
+
+VLS_INST(float)
+VLS_INST(double)
+
+}  // namespace vls
