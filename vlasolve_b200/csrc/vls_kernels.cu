@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(UC_THREADS)
       const int u = k - 1;
       const double newU = __ldg(g.U + u) + s;
       T v = T(0);
-      if (!((newU <= g.u0) || (newU >= g.umax))) {
+      // outside (or NaN) -> 0, as vlasovSolver21_spline.hxx:761
+      if (newU > g.u0 && newU < g.umax) {
         const double y = (newU - g.su) * g.hu;
         const double fl = floor(y);
         const T fr = (T)(y - fl);
