@@ -33,6 +33,11 @@ WORKLOAD = dict(type="Hernquist", Pmin=0.01, Pmax=50.0, Pres=512, Pscale="logari
                 Umin=(-3.0, 0.0), Umax=(3.0, 3.0), Ures=(512, 256),
                 Uscale=("linear", "quadratic"), dt=0.0025)
 WORKLOAD_NAME = "hernquist_512x512x256"
+# smaller case of the same kernels for ncu captures (f = 135 MB FP32, > L2)
+WORKLOADS = {
+    "hernquist_512x512x256": WORKLOAD,
+    "hernquist_512x512x128": dict(WORKLOAD, Ures=(512, 128)),
+}
 METRIC = "phase-space cell updates/s"
 REF_BIN = os.path.join(HERE, "oracle", "_ref", "vlasolve")
 
@@ -189,13 +194,25 @@ def gpu_arm(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
-    w = dict(WORKLOAD)
+    w = dict(WORKLOADS[args.workload])
     cells = cells_of(w)
     K, W = args.steps, args.warmup
     peak, peak_kind = measured_peaks()
+    if args.quick:
+        # timing only (used under ncu): no FP64 arm, statistics or end-to-end run
+        s = VlasovSolver21Spline(w, precision=args.precision, device=local)
+        ms, launches = time_steps(s, K, W, torch, dist)
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "precision": args.precision,
+                              "ms_per_step": ms / K, "launches": launches}), flush=True)
+        s.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     res = {}
-    for prec in (args.precision, "fp64") if args.precision != "fp64" else ("fp64",):
+    precs = [args.precision] + [p for p in ("fp32all", "fp64") if p != args.precision]
+    for prec in precs:
         s = VlasovSolver21Spline(w, precision=prec, device=local)
         st0 = s.stats()
         with ClockSampler(local) as clk:
@@ -216,7 +233,7 @@ def gpu_arm(args):
     main = res[args.precision]
     ms = main["ms"]
     value = world * cells * K / (ms * 1e-3)
-    esize = 4 if args.precision == "fp32" else 8
+    esize = 8 if args.precision == "fp64" else 4
     # dominant kernel and its roofline: algorithmic bytes = one read of its input
     # field + one write of its output field per cell (8 B FP32 / 16 B FP64)
     prof = main["prof"]
@@ -274,7 +291,7 @@ def gpu_arm(args):
     line = {
         "metric": METRIC, "value": value, "unit": "cell updates/s", "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
         "data": "synthetic (analytic Hernquist distribution function)",
         "config": config_json(w, args.precision),
         "gpu_launches": main["launches"],
@@ -291,10 +308,15 @@ def gpu_arm(args):
         "energy_drift_rel": {p: res[p]["dE"] for p in res},
         "cpu_baseline": cpu,
     }
-    if "fp64" in res and args.precision != "fp64":
-        v64 = world * cells * K / (res["fp64"]["ms"] * 1e-3)
-        line["fp64"] = {"value": v64, "ms_per_step": res["fp64"]["ms"] / K,
-                        "fp32_over_fp64": value / v64}
+    for p in res:
+        if p == args.precision:
+            continue
+        v = world * cells * K / (res[p]["ms"] * 1e-3)
+        line[p] = {"value": v, "ms_per_step": res[p]["ms"] / K,
+                   "kernels_ms_per_step": {k: x[0] / min(K, 20)
+                                           for k, x in res[p]["prof"].items()}}
+    if "fp64" in line:
+        line["fp32_over_fp64"] = value / line["fp64"]["value"]
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -334,10 +356,13 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp32all", "fp64"])
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-max-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true",
+                    help="timing of the chosen precision only (for profiler runs)")
+    ap.add_argument("--workload", default=WORKLOAD_NAME, choices=sorted(WORKLOADS))
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

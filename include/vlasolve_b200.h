@@ -49,8 +49,11 @@ enum { VLS_INIT_UDF = 0, VLS_INIT_PLDF = 1, VLS_INIT_PLUMMER = 2,
        VLS_INIT_HERNQUIST = 3 };
 /* arithmetic/storage of the step.  FP64: every value FP64.  FP32_BULK: f,
    spline coefficients and the gathers in FP32; prefilter recursions, footpoint
-   indexing, moments, enclosed-mass scan and statistics in FP64. */
-enum { VLS_FP64 = 0, VLS_FP32_BULK = 1 };
+   indexing, moments, enclosed-mass scan and statistics in FP64.  FP32_ALL:
+   as FP32_BULK but the prefilter recursions also run in FP32 (indexing,
+   moments, scan and statistics stay FP64).  In both FP32 modes the drift
+   footpoint fractions are stored with 21 bits (rounded). */
+enum { VLS_FP64 = 0, VLS_FP32_BULK = 1, VLS_FP32_ALL = 2 };
 
 /* gridBase::paramT, grid_base.hxx:58-82, i.e. the grid.* options
    (grid_handler.hxx:224-238): r is index P, u and J are U[0] and U[1].

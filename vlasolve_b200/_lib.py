@@ -18,7 +18,7 @@ STATUS_NAMES = {0: "VLS_OK", 1: "VLS_EINVAL", 2: "VLS_ECUDA", 3: "VLS_ENAN",
 SCALES = {"linear": 0, "logarithmic": 1, "quadratic": 2}
 KERNELS = {"delayed": 0, "reflective": 1}
 PROFILES = {"UDF": 0, "PLDF": 1, "Plummer": 2, "Hernquist": 3}
-PRECISIONS = {"fp64": 0, "fp32": 1}
+PRECISIONS = {"fp64": 0, "fp32": 1, "fp32all": 2}
 
 # every symbol include/vlasolve_b200.h declares
 EXPORTED = [

@@ -30,8 +30,9 @@ struct vls_handle {
   cudaStream_t st = nullptr;
   // device buffers
   void *f = nullptr, *G = nullptr, *C = nullptr;
-  int32_t *idx = nullptr;
+  int32_t *idx = nullptr;        // FP64 footpoints
   void *fx = nullptr, *fy = nullptr;
+  uint2 *fp2 = nullptr;          // FP32 packed footpoints
   int64_t nch = 0, nel = 0;
   int64_t *ch_start = nullptr;
   int32_t *ch_len = nullptr;
@@ -186,8 +187,43 @@ static cudaError_t timed(vls_handle *h, int kind, F &&launch) {
 }
 
 // ------------------------------------------------------------- footpoints
+// FP32 packed word of one direction: index << 21 | fraction rounded to 21
+// bits; a fraction that rounds up to 1 moves to the next node (same spline
+// value, the B-spline is continuous there).
+static uint32_t pack_coord(int32_t I, double F, int32_t maxI) {
+  const double q = std::nearbyint(F * 2097152.0);
+  int64_t qi = (int64_t)q;
+  if (qi >= (int64_t)1 << 21) {
+    if (I < maxI) {
+      I += 1;
+      qi = 0;
+    } else {
+      qi = ((int64_t)1 << 21) - 1;
+    }
+  }
+  if (qi < 0) qi = 0;
+  return ((uint32_t)I << 21) | (uint32_t)qi;
+}
+static const uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu;
+
+static uint2 encode_packed(const Coords &c, int32_t code, double rF, double uF) {
+  uint2 w;
+  if (code == -1) {
+    w.x = FP_OUT;
+    w.y = 0;
+  } else if (code <= -2) {
+    w.x = FP_CHAIN;
+    w.y = (uint32_t)(-2 - (int64_t)code);
+  } else {
+    w.x = pack_coord(code & 0xffff, rF, c.nr - 1);
+    w.y = pack_coord(code >> 16, uF, c.nu - 1);
+  }
+  return w;
+}
+
 // Encoding of one cell: -1 -> outside the box (value 0), <= -2 -> delayed
-// kernel chain (-2 - chain id), else rI | uI << 16.
+// kernel chain (-2 - chain id), else rI | uI << 16 (FP64 tables); the FP32
+// tables pack the same information into two 32-bit words.
 static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
   const Coords &c = h->co;
   const bool linked = !h->solver.noLinking;
@@ -197,11 +233,8 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
   const int batch = std::max(1, (int)std::min<size_t>(c.nj, (16u << 20) / slice));
   std::vector<int32_t> idx(slice * batch);
   std::vector<double> fx(slice * batch), fy(slice * batch);
-  std::vector<float> fx32, fy32;
-  if (h->prec == VLS_FP32_BULK) {
-    fx32.resize(slice * batch);
-    fy32.resize(slice * batch);
-  }
+  std::vector<uint2> packed;
+  if (h->prec != VLS_FP64) packed.resize(slice * batch);
   std::vector<SliceFootpoints> sfp(batch);
   std::vector<SliceChains> sch(batch);
   if (build_chains) {
@@ -257,17 +290,13 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
     }
     if (!bad.empty()) return fail(h, VLS_EINVAL, bad);
     const size_t off = (size_t)j0 * slice, n = (size_t)nb * slice;
-    TRY(upload(h, h->idx + off, idx.data(), n * sizeof(int32_t)));
     if (h->prec == VLS_FP64) {
+      TRY(upload(h, h->idx + off, idx.data(), n * sizeof(int32_t)));
       TRY(upload(h, (double *)h->fx + off, fx.data(), n * sizeof(double)));
       TRY(upload(h, (double *)h->fy + off, fy.data(), n * sizeof(double)));
     } else {
-      for (size_t i = 0; i < n; i++) {
-        fx32[i] = (float)fx[i];
-        fy32[i] = (float)fy[i];
-      }
-      TRY(upload(h, (float *)h->fx + off, fx32.data(), n * sizeof(float)));
-      TRY(upload(h, (float *)h->fy + off, fy32.data(), n * sizeof(float)));
+      for (size_t i = 0; i < n; i++) packed[i] = encode_packed(c, idx[i], fx[i], fy[i]);
+      TRY(upload(h, h->fp2 + off, packed.data(), n * sizeof(uint2)));
     }
   }
   return VLS_OK;
@@ -370,7 +399,8 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   if (!grid || !solver || !out)
     return fail(nullptr, VLS_EINVAL, "vls_create: NULL argument");
   *out = nullptr;
-  if (solver->precision != VLS_FP64 && solver->precision != VLS_FP32_BULK)
+  if (solver->precision != VLS_FP64 && solver->precision != VLS_FP32_BULK &&
+      solver->precision != VLS_FP32_ALL)
     return fail(nullptr, VLS_EINVAL, "unknown precision");
   if (solver->kernelType != VLS_KERNEL_DELAYED &&
       solver->kernelType != VLS_KERNEL_REFLECTIVE)
@@ -392,7 +422,8 @@ extern "C" int vls_create(const vls_grid_desc *grid,
       return fail(nullptr, VLS_EINVAL, e);
   }
   const Coords &c = h->co;
-  if (c.nr > 2048) return fail(nullptr, VLS_EINVAL, "at most 2048 radial vertices");
+  if (c.nr > 2048 || c.nu > 2048)
+    return fail(nullptr, VLS_EINVAL, "at most 2048 vertices along r and along v_r");
   h->cells = (size_t)c.nr * c.nu * c.nj;
   h->pc = ((c.nr + 3) + 3) / 4 * 4;
   h->tr = thomas_tables(c.nr, c.sstep_inv[0]);
@@ -411,9 +442,13 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   A(dalloc(hp, &h->f, es * cells));
   A(dalloc(hp, &h->G, es * (size_t)c.nj * (c.nu + 2) * c.nr));
   A(dalloc(hp, &h->C, es * (size_t)c.nj * (c.nu + 3) * h->pc));
-  A(dalloc(hp, &h->idx, sizeof(int32_t) * cells));
-  A(dalloc(hp, &h->fx, es * cells));
-  A(dalloc(hp, &h->fy, es * cells));
+  if (h->prec == VLS_FP64) {
+    A(dalloc(hp, &h->idx, sizeof(int32_t) * cells));
+    A(dalloc(hp, &h->fx, es * cells));
+    A(dalloc(hp, &h->fy, es * cells));
+  } else {
+    A(dalloc(hp, &h->fp2, sizeof(uint2) * cells));
+  }
   A(dalloc(hp, &h->rp_r, sizeof(double) * h->tr.M));
   A(dalloc(hp, &h->q_r, sizeof(double) * h->tr.M));
   A(dalloc(hp, &h->rp_u, sizeof(double) * h->tu.M));
@@ -761,33 +796,30 @@ extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
       idx[i] = rI[i] | (uI[i] << 16);
     }
   }
-  TRY(upload(h, h->idx, idx.data(), sizeof(int32_t) * h->cells));
   if (h->prec == VLS_FP64) {
+    TRY(upload(h, h->idx, idx.data(), sizeof(int32_t) * h->cells));
     TRY(upload(h, h->fx, rF, sizeof(double) * h->cells));
     TRY(upload(h, h->fy, uF, sizeof(double) * h->cells));
   } else {
-    std::vector<float> a(h->cells), b(h->cells);
-    for (size_t i = 0; i < h->cells; i++) {
-      a[i] = (float)rF[i];
-      b[i] = (float)uF[i];
-    }
-    TRY(upload(h, h->fx, a.data(), sizeof(float) * h->cells));
-    TRY(upload(h, h->fy, b.data(), sizeof(float) * h->cells));
+    std::vector<uint2> p(h->cells);
+    for (size_t i = 0; i < h->cells; i++) p[i] = encode_packed(c, idx[i], rF[i], uF[i]);
+    TRY(upload(h, h->fp2, p.data(), sizeof(uint2) * h->cells));
   }
   return VLS_OK;
 }
 
 // ------------------------------------------------------------------ step
-template <typename T>
+template <typename T, typename R>
 static int drift_once(vls_handle *h, bool kick) {
   const Geometry g = geometry(h);
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
   const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
   CK(h, timed(h, kick ? VLS_K_UCOL_KICK : VLS_K_UCOL, [&] {
-       return launch_ucol<T>(kick, (const T *)h->f, (T *)h->G, h->shift, g, tu, h->st);
+       return launch_ucol<T, R>(kick, (const T *)h->f, (T *)h->G, h->shift, g, tu,
+                                h->st);
      }));
   CK(h, timed(h, VLS_K_PRER, [&] {
-       return launch_prer<T>((const T *)h->G, (T *)h->C, g, tr, h->st);
+       return launch_prer<T, R>((const T *)h->G, (T *)h->C, g, tr, h->st);
      }));
   if (h->nch) {
     CK(h, timed(h, VLS_K_TAILS, [&] {
@@ -798,7 +830,7 @@ static int drift_once(vls_handle *h, bool kick) {
   }
   CK(h, timed(h, VLS_K_DRIFT, [&] {
        return launch_drift<T>((const T *)h->C, (T *)h->f, h->idx, (const T *)h->fx,
-                              (const T *)h->fy, h->ch_start, h->ch_len,
+                              (const T *)h->fy, h->fp2, h->ch_start, h->ch_len,
                               (const T *)h->ch_val, h->ndrift, moment_tables(h),
                               h->partial, g, h->st);
      }));
@@ -827,13 +859,13 @@ static int scan_once(vls_handle *h) {
   return VLS_OK;
 }
 
-template <typename T>
+template <typename T, typename R>
 static int step_impl(vls_handle *h, int nsteps) {
   for (int s = 0; s < nsteps; s++) {
-    if (h->solver.noLinking) TRY(drift_once<T>(h, false));
+    if (h->solver.noLinking) TRY((drift_once<T, R>(h, false)));
     TRY(ensure_moments<T>(h));
     TRY(scan_once(h));
-    TRY(drift_once<T>(h, true));
+    TRY((drift_once<T, R>(h, true)));
     h->time += h->solver.dt;
     h->step++;
   }
@@ -845,8 +877,14 @@ extern "C" int vls_step(vls_handle *h, int32_t nsteps) {
   if (nsteps < 0) return fail(h, VLS_EINVAL, "nsteps < 0");
   if (!h->have_f) return fail(h, VLS_ESTATE, "vls_step before the grid was set");
   CK(h, cudaSetDevice(h->solver.device));
-  return h->prec == VLS_FP64 ? step_impl<double>(h, nsteps)
-                             : step_impl<float>(h, nsteps);
+  switch (h->prec) {
+    case VLS_FP64:
+      return step_impl<double, double>(h, nsteps);
+    case VLS_FP32_BULK:
+      return step_impl<float, double>(h, nsteps);
+    default:
+      return step_impl<float, float>(h, nsteps);
+  }
 }
 
 extern "C" int vls_sync(vls_handle *h) {

@@ -8,8 +8,11 @@
 //                                     and columns >= N_r+2 stay zero (reads
 //                                     at index N exist for footpoints that
 //                                     land on the last vertex with weight 0)
-//   fp_idx [cells] int32            rI | uI<<16, -1 = outside, <= -2 = chain
-//   fp_x, fp_y [cells] T            fractional footpoint offsets
+//   FP64: fp_idx [cells] int32      rI | uI<<16, -1 = outside, <= -2 = chain
+//         fp_x, fp_y [cells] double fractional footpoint offsets
+//   FP32: fp2 [cells] uint2         per direction index<<21 | round(frac*2^21);
+//                                     0xFFFFFFFF = outside, 0xFFFFFFFE = chain
+//                                     (second word = chain id)
 //   chains: ch_start/int64, ch_len/int32 per chain, ch_val/T per element
 //           (ring buffer; logical front at (ndrift mod len)), tail footpoint
 //   partial [N_J][N_r] double       per-slice radial moment partial sums
@@ -48,15 +51,17 @@ struct MomentTables {
 };
 
 // launchers (vls_kernels.cu); all asynchronous on `st`
-template <typename T>
+// T: storage type of f and the coefficients; R: arithmetic of the recursions
+template <typename T, typename R>
 cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
                         const Geometry &g, const DirTables &tu, cudaStream_t st);
-template <typename T>
+template <typename T, typename R>
 cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr,
                         cudaStream_t st);
+// footpoints: FP64 handles use idx/fx/fy, FP32 handles the packed fp2 table
 template <typename T>
 cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
-                         const T *fy, const int64_t *ch_start,
+                         const T *fy, const uint2 *fp2, const int64_t *ch_start,
                          const int32_t *ch_len, const T *ch_val,
                          int64_t ndrift, const MomentTables &mt, double *partial,
                          const Geometry &g, cudaStream_t st);

@@ -26,11 +26,14 @@
 
 namespace vls {
 
+// warm-up rows of a segment: FP64 storage needs the recursion to contract to
+// FP64 rounding (0.268^32 = 5e-19), FP32 storage to well below FP32 rounding
+// (0.268^20 = 3.6e-12)
 template <typename T>
 struct Prec;
 template <>
 struct Prec<double> {
-  static constexpr int K = 32;  // warm-up rows of a segment
+  static constexpr int K = 32;
 };
 template <>
 struct Prec<float> {
@@ -46,64 +49,80 @@ __device__ __forceinline__ T bv1(T x) {
   return T(1) + T(3) * x + T(3) * x * x - T(3) * x * x * x;
 }
 
+// ----------------------------------------------------------- async copies
+// cp.async (LDGSTS): element-wise global -> shared copies that stay in flight
+// together; the tiles' global rows are only 4-byte aligned (r-pitch N_r).
+template <typename T>
+__device__ __forceinline__ void cp_async(T *smem, const T *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem),
+               "n"((int)sizeof(T))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // ----------------------------------------------------------- segment solve
 // One line of the padded natural-BC system lives at b[k*ks], k = 0..M-1.  On
 // entry rows 1..M-2 hold the data; on exit rows 0..M-1 hold the coefficients.
-// A thread owns interior rows [k0, k1).  All four stages are separated by
-// __syncthreads() in the caller.
-template <int K>
+// A thread owns interior rows [k0, k1).  The four stages are separated by
+// __syncthreads() (see solve_lines).  R is the arithmetic of the recursion.
+template <int K, typename R>
 struct Seg {
   template <typename S>
-  __device__ static double fwd_warm(const S *b, int ks, int k0,
-                                    const DirTables &t) {
-    double d = 0.0;
+  __device__ static R fwd_warm(const S *b, int ks, int k0, const R *rp) {
+    R d = R(0);
     int ks0 = k0 - K;
     if (ks0 < 1) ks0 = 1;
-    for (int k = ks0; k < k0; ++k)
-      d = ((double)b[k * ks] - d * (1.0 / 6.0)) * __ldg(t.rp + k);
+#pragma unroll 4
+    for (int k = ks0; k < k0; ++k) d = ((R)b[k * ks] - d * (R(1) / R(6))) * rp[k];
     return d;
   }
   template <typename S>
-  __device__ static void fwd_main(S *b, int ks, int k0, int k1, double d,
-                                  const DirTables &t) {
-    double dprev = d;
+  __device__ static void fwd_main(S *b, int ks, int k0, int k1, R d,
+                                  const DirTables &t, const R *rp) {
+    R dprev = d;
+#pragma unroll 4
     for (int k = k0; k < k1; ++k) {
       dprev = d;
-      d = ((double)b[k * ks] - d * (1.0 / 6.0)) * __ldg(t.rp + k);
+      d = ((R)b[k * ks] - d * (R(1) / R(6))) * rp[k];
       b[k * ks] = (S)d;
     }
     if (k1 == t.M - 1 && k1 > k0) {
       // last row (localSpline.hxx:1145-1152): d = d_{M-2}, dprev = d_{M-3}
-      const double num = (0.0 - t.hi2 * dprev) - t.L1 * d;
-      b[(t.M - 1) * ks] = (S)(num / t.L2);
+      const R num = (R(0) - (R)t.hi2 * dprev) - (R)t.L1 * d;
+      b[(t.M - 1) * ks] = (S)(num / (R)t.L2);
     }
   }
   template <typename S>
-  __device__ static double bwd_warm(const S *b, int ks, int k1,
-                                    const DirTables &t) {
+  __device__ static R bwd_warm(const S *b, int ks, int k1, const DirTables &t,
+                               const R *q) {
     int kst = k1 + K - 1;
-    double c;
+    R c;
     if (kst >= t.M - 2) {
       kst = t.M - 2;
-      c = (double)b[(t.M - 1) * ks];
+      c = (R)b[(t.M - 1) * ks];
     } else {
-      c = 0.0;
+      c = R(0);
     }
-    for (int k = kst; k >= k1; --k) c = (double)b[k * ks] - __ldg(t.q + k) * c;
+#pragma unroll 4
+    for (int k = kst; k >= k1; --k) c = (R)b[k * ks] - q[k] * c;
     return c;
   }
   template <typename S>
-  __device__ static void bwd_main(S *b, int ks, int k0, int k1, double c,
-                                  const DirTables &t) {
-    double cnext = c;
+  __device__ static void bwd_main(S *b, int ks, int k0, int k1, R c,
+                                  const DirTables &t, const R *q) {
+    R cnext = c;
+#pragma unroll 4
     for (int k = k1 - 1; k >= k0; --k) {
       cnext = c;
-      c = (double)b[k * ks] - __ldg(t.q + k) * c;
+      c = (R)b[k * ks] - q[k] * c;
       b[k * ks] = (S)c;
     }
     if (k0 == 1 && k1 > k0) {
       // first row (localSpline.hxx:1171): c_0 = (0 - a01 c_1) - a02 c_2
-      b[0] = (S)((0.0 - t.a01 * c) - t.a02 * cnext);
+      b[0] = (S)((R(0) - (R)t.a01 * c) - (R)t.a02 * cnext);
     }
   }
 };
@@ -120,67 +139,94 @@ __device__ __forceinline__ void seg_bounds(int M, int nseg, int s, int &k0,
   if (k1 > M - 1) k1 = M - 1;
 }
 
-template <int K, typename S>
+// rp, q: the direction's tables in the recursion type (shared memory)
+template <int K, typename R, typename S>
 __device__ void solve_lines(S *base, int ks, int k0, int k1,
-                            const DirTables &t) {
-  double d = Seg<K>::fwd_warm(base, ks, k0, t);
+                            const DirTables &t, const R *rp, const R *q) {
+  R d = Seg<K, R>::fwd_warm(base, ks, k0, rp);
   __syncthreads();
-  Seg<K>::fwd_main(base, ks, k0, k1, d, t);
+  Seg<K, R>::fwd_main(base, ks, k0, k1, d, t, rp);
   __syncthreads();
-  double c = Seg<K>::bwd_warm(base, ks, k1, t);
+  R c = Seg<K, R>::bwd_warm(base, ks, k1, t, q);
   __syncthreads();
-  Seg<K>::bwd_main(base, ks, k0, k1, c, t);
+  Seg<K, R>::bwd_main(base, ks, k0, k1, c, t, q);
   __syncthreads();
 }
 
-// ------------------------------------------------------------------ ucol
-// Block: TW columns (r) x SEG segments (u).  Shared: two buffers of
-// (N_u+3) rows x TW (row N_u+2 is an always-zero guard row).
-constexpr int UC_TW = 16;
-constexpr int UC_THREADS = 256;
-constexpr int UC_SEG = UC_THREADS / UC_TW;
+// copies the direction's Thomas tables into shared memory as type R
+template <typename R>
+__device__ void load_tables(R *rp, R *q, const DirTables &t) {
+  for (int k = threadIdx.x; k < t.M; k += blockDim.x) {
+    rp[k] = (R)__ldg(t.rp + k);
+    q[k] = (R)__ldg(t.q + k);
+  }
+}
 
-template <typename T, bool KICK>
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) / 16 * 16; }
+
+// ------------------------------------------------------------------ ucol
+// Block: TW columns (r) x NSEG segments (u), lane = column so every shared
+// row access is one conflict-free wavefront.  Shared: the Thomas tables and
+// two buffers of (N_u+3) rows x TW (row N_u+2 is an always-zero guard row).
+constexpr int UC_THREADS = 256;
+template <typename T>
+struct UcolCfg {
+  // 16 FP32 / 8 FP64 columns: two (N_u+3)-row buffers stay under 75 KB at
+  // N_u = 513 (three blocks per SM) and fit at N_u = 1025
+  static constexpr int TW = sizeof(T) == 4 ? 16 : 8;
+  static constexpr int NSEG = UC_THREADS / TW;
+};
+
+template <typename T, typename R, bool KICK>
 __global__ void __launch_bounds__(UC_THREADS)
     ucol_kernel(const T *__restrict__ f, T *__restrict__ G,
                 const double *__restrict__ shift, Geometry g, DirTables tu) {
+  constexpr int TW = UcolCfg<T>::TW, NSEG = UcolCfg<T>::NSEG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *bufA = reinterpret_cast<T *>(smem_raw);
   const int M = g.nu + 2;
   const int rows = M + 1;
-  T *bufB = bufA + (size_t)rows * UC_TW;
+  R *rp = reinterpret_cast<R *>(smem_raw);
+  R *qq = rp + M;
+  T *bufA = reinterpret_cast<T *>(smem_raw + align16(2 * M * sizeof(R)));
+  T *bufB = bufA + (size_t)rows * TW;
   const int tid = threadIdx.x;
-  const int col = tid % UC_TW;
-  const int seg = tid / UC_TW;
-  const int r0 = blockIdx.x * UC_TW;
+  const int col = tid % TW;
+  const int seg = tid / TW;
+  const int r0 = blockIdx.x * TW;
   const int j = blockIdx.y;
   const int r = r0 + col;
   const size_t fslice = (size_t)j * g.nu * g.nr;
 
-  for (int e = tid; e < g.nu * UC_TW; e += UC_THREADS) {
-    const int k = e / UC_TW + 1, c = e % UC_TW;
+  for (int e = tid; e < g.nu * TW; e += UC_THREADS) {
+    const int k = e / TW + 1, c = e % TW;
     const int rr = r0 + c;
-    bufA[k * UC_TW + c] =
-        rr < g.nr ? f[fslice + (size_t)(k - 1) * g.nr + rr] : T(0);
+    if (rr < g.nr)
+      cp_async(&bufA[k * TW + c], f + fslice + (size_t)(k - 1) * g.nr + rr);
+    else
+      bufA[k * TW + c] = T(0);
   }
-  if (tid < UC_TW) {
-    bufA[0 * UC_TW + tid] = T(0);
-    bufA[(M - 1) * UC_TW + tid] = T(0);
-    bufA[M * UC_TW + tid] = T(0);
-    bufB[0 * UC_TW + tid] = T(0);
-    bufB[(M - 1) * UC_TW + tid] = T(0);
-    bufB[M * UC_TW + tid] = T(0);
+  load_tables<R>(rp, qq, tu);
+  if (tid < TW) {
+    bufA[0 * TW + tid] = T(0);
+    bufA[(M - 1) * TW + tid] = T(0);
+    bufA[M * TW + tid] = T(0);
+    bufB[0 * TW + tid] = T(0);
+    bufB[(M - 1) * TW + tid] = T(0);
+    bufB[M * TW + tid] = T(0);
   }
+  cp_async_wait_all();
   __syncthreads();
   int k0, k1;
-  seg_bounds(M, UC_SEG, seg, k0, k1);
-  solve_lines<Prec<T>::K>(bufA + col, UC_TW, k0, k1, tu);
+  seg_bounds(M, NSEG, seg, k0, k1);
+  solve_lines<Prec<T>::K, R>(bufA + col, TW, k0, k1, tu, rp, qq);
 
   T *out = bufA;
   if (KICK) {
     // kick gather (localSpline.hxx:423-441 with the r-direction (1,4,1)/6
     // weights folded into the u-only coefficients), vlasovSolver21_spline.hxx:758-763
     const double s = (r < g.nr) ? __ldg(shift + r) : 0.0;
+    const T *cb = bufA + col;
+#pragma unroll 2
     for (int k = k0; k < k1; ++k) {
       const int u = k - 1;
       const double newU = __ldg(g.U + u) + s;
@@ -191,88 +237,119 @@ __global__ void __launch_bounds__(UC_THREADS)
         const double fl = floor(y);
         const T fr = (T)(y - fl);
         const int Ny = 1 + (int)fl;
-        const T *cb = bufA + col;
         v = (T(1) / T(6)) *
-            (bv2<T>(T(1) - fr) * cb[(Ny - 1) * UC_TW] +
-             bv1<T>(T(1) - fr) * cb[Ny * UC_TW] + bv1<T>(fr) * cb[(Ny + 1) * UC_TW] +
-             bv2<T>(fr) * cb[(Ny + 2) * UC_TW]);
+            (bv2<T>(T(1) - fr) * cb[(Ny - 1) * TW] + bv1<T>(T(1) - fr) * cb[Ny * TW] +
+             bv1<T>(fr) * cb[(Ny + 1) * TW] + bv2<T>(fr) * cb[(Ny + 2) * TW]);
       }
-      bufB[k * UC_TW + col] = v;
+      bufB[k * TW + col] = v;
     }
     __syncthreads();
-    solve_lines<Prec<T>::K>(bufB + col, UC_TW, k0, k1, tu);
+    solve_lines<Prec<T>::K, R>(bufB + col, TW, k0, k1, tu, rp, qq);
     out = bufB;
   }
   const size_t gslice = (size_t)j * M * g.nr;
-  for (int e = tid; e < M * UC_TW; e += UC_THREADS) {
-    const int k = e / UC_TW, c = e % UC_TW;
+  for (int e = tid; e < M * TW; e += UC_THREADS) {
+    const int k = e / TW, c = e % TW;
     const int rr = r0 + c;
-    if (rr < g.nr) G[gslice + (size_t)k * g.nr + rr] = out[k * UC_TW + c];
+    if (rr < g.nr) G[gslice + (size_t)k * g.nr + rr] = out[k * TW + c];
   }
 }
 
-template <typename T>
+template <typename T, typename R>
 cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
                         const Geometry &g, const DirTables &tu, cudaStream_t st) {
-  const size_t smem = 2 * (size_t)(g.nu + 3) * UC_TW * sizeof(T);
-  dim3 grid((g.nr + UC_TW - 1) / UC_TW, g.nj);
+  constexpr int TW = UcolCfg<T>::TW;
+  const size_t smem =
+      align16(2 * (size_t)(g.nu + 2) * sizeof(R)) + 2 * (size_t)(g.nu + 3) * TW * sizeof(T);
+  dim3 grid((g.nr + TW - 1) / TW, g.nj);
+  cudaError_t e;
   if (kick) {
-    cudaFuncSetAttribute(ucol_kernel<T, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    ucol_kernel<T, true><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
+    e = cudaFuncSetAttribute(ucol_kernel<T, R, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    ucol_kernel<T, R, true><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
   } else {
-    cudaFuncSetAttribute(ucol_kernel<T, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    ucol_kernel<T, false><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
+    e = cudaFuncSetAttribute(ucol_kernel<T, R, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    ucol_kernel<T, R, false><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
   }
   return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ prer
-// Block: PR_ROWS rows of G x PR_SEG segments along r (one warp per row).
-constexpr int PR_SEG = 32;
-constexpr int PR_ROWS = 8;
-
+// Block: ROWS rows of G (lane = row) x NSEG long segments along r.  The
+// shared row pitch is odd (FP64) or 1 mod 32 (FP32) so that the lanes, which
+// walk different rows at the same column, hit distinct banks.
 template <typename T>
-__global__ void __launch_bounds__(PR_SEG *PR_ROWS)
+struct PrerCfg {
+  static constexpr int ROWS = sizeof(T) == 4 ? 32 : 16;
+  static constexpr int NSEG = 8;
+  static constexpr int THREADS = ROWS * NSEG;
+};
+
+__host__ __device__ inline int prer_pitch(int M, int elem) {
+  int P = M + 1;
+  if (elem == 4)
+    P = (P + 31) / 32 * 32 + 1;
+  else
+    P |= 1;
+  return P;
+}
+
+template <typename T, typename R>
+__global__ void __launch_bounds__(PrerCfg<T>::THREADS)
     prer_kernel(const T *__restrict__ G, T *__restrict__ C, Geometry g,
                 DirTables tr) {
+  constexpr int ROWS = PrerCfg<T>::ROWS, NSEG = PrerCfg<T>::NSEG,
+                NT = PrerCfg<T>::THREADS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *buf = reinterpret_cast<T *>(smem_raw);
   const int M = g.nr + 2;
-  const int LS = M + 1;
+  const int LS = prer_pitch(M, sizeof(T));
+  R *rp = reinterpret_cast<R *>(smem_raw);
+  R *qq = rp + M;
+  T *buf = reinterpret_cast<T *>(smem_raw + align16(2 * M * sizeof(R)));
   const int tid = threadIdx.x;
-  const int rho = tid / PR_SEG;
-  const int seg = tid % PR_SEG;
+  const int rho = tid % ROWS;
+  const int seg = tid / ROWS;
   const int j = blockIdx.y;
-  const int kr0 = blockIdx.x * PR_ROWS;
+  const int kr0 = blockIdx.x * ROWS;
   const int nrows = g.nu + 2;
   const size_t gslice = (size_t)j * nrows * g.nr;
-  for (int e = tid; e < PR_ROWS * g.nr; e += PR_SEG * PR_ROWS) {
+  for (int e = tid; e < ROWS * g.nr; e += NT) {
     const int p = e / g.nr, k = e % g.nr;
     const int kr = kr0 + p;
-    buf[p * LS + k + 1] = kr < nrows ? G[gslice + (size_t)kr * g.nr + k] : T(0);
+    if (kr < nrows)
+      cp_async(&buf[p * LS + k + 1], G + gslice + (size_t)kr * g.nr + k);
+    else
+      buf[p * LS + k + 1] = T(0);
   }
+  load_tables<R>(rp, qq, tr);
+  cp_async_wait_all();
   __syncthreads();
   int k0, k1;
-  seg_bounds(M, PR_SEG, seg, k0, k1);
-  solve_lines<Prec<T>::K>(buf + rho * LS, 1, k0, k1, tr);
+  seg_bounds(M, NSEG, seg, k0, k1);
+  solve_lines<Prec<T>::K, R>(buf + rho * LS, 1, k0, k1, tr, rp, qq);
   const size_t cslice = (size_t)j * (g.nu + 3) * g.pc;
-  for (int e = tid; e < PR_ROWS * M; e += PR_SEG * PR_ROWS) {
+  for (int e = tid; e < ROWS * M; e += NT) {
     const int p = e / M, k = e % M;
     const int kr = kr0 + p;
     if (kr < nrows) C[cslice + (size_t)kr * g.pc + k] = buf[p * LS + k];
   }
 }
 
-template <typename T>
+template <typename T, typename R>
 cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr,
                         cudaStream_t st) {
-  const size_t smem = (size_t)PR_ROWS * (g.nr + 3) * sizeof(T);
-  dim3 grid((g.nu + 2 + PR_ROWS - 1) / PR_ROWS, g.nj);
-  cudaFuncSetAttribute(prer_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
-  prer_kernel<T><<<grid, PR_SEG * PR_ROWS, smem, st>>>(G, C, g, tr);
+  constexpr int ROWS = PrerCfg<T>::ROWS;
+  const int M = g.nr + 2;
+  const size_t smem = align16(2 * (size_t)M * sizeof(R)) +
+                      (size_t)ROWS * prer_pitch(M, sizeof(T)) * sizeof(T);
+  dim3 grid((g.nu + 2 + ROWS - 1) / ROWS, g.nj);
+  cudaError_t e = cudaFuncSetAttribute(
+      prer_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  prer_kernel<T, R><<<grid, PrerCfg<T>::THREADS, smem, st>>>(G, C, g, tr);
   return cudaGetLastError();
 }
 
@@ -302,11 +379,61 @@ __device__ __forceinline__ T eval2d(const T *__restrict__ Cj, int pc, int rI,
 
 constexpr int DR_W = 8;  // warps per drift block
 
+// footpoint of one cell, decoded: taps at (rI.., uI..) with fractions (x, y);
+// kind 0 = gather, 1 = outside (0), 2 = delayed-kernel chain `ch`
 template <typename T>
-__global__ void __launch_bounds__(32 * DR_W)
+struct Foot {
+  int rI, uI, kind;
+  int64_t ch;
+  T x, y;
+};
+
+// FP64 tables: idx = rI | uI<<16, -1 outside, <= -2 chain; FP64 fractions
+__device__ __forceinline__ Foot<double> load_foot(const int32_t *__restrict__ idx,
+                                                  const double *__restrict__ fx,
+                                                  const double *__restrict__ fy,
+                                                  const uint2 *, size_t i) {
+  Foot<double> p;
+  const int code = __ldg(idx + i);
+  p.kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
+  p.ch = -2 - (int64_t)code;
+  p.rI = code >= 0 ? (code & 0xffff) : 0;
+  p.uI = code >= 0 ? (code >> 16) : 0;
+  p.x = code >= 0 ? __ldg(fx + i) : 0.0;
+  p.y = code >= 0 ? __ldg(fy + i) : 0.0;
+  return p;
+}
+
+// FP32 tables, 8 bytes per cell: word = index << FP_FBITS | round(frac * 2^FP_FBITS)
+// per direction; FP_OUT / FP_CHAIN in the first word mark the two special kinds
+// (the second word then holds the chain id)
+constexpr int FP_FBITS = 21;
+constexpr uint32_t FP_FMASK = (1u << FP_FBITS) - 1u;
+constexpr uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu;
+
+__device__ __forceinline__ Foot<float> load_foot(const int32_t *, const float *,
+                                                 const float *,
+                                                 const uint2 *__restrict__ fp2,
+                                                 size_t i) {
+  Foot<float> p;
+  const uint2 w = __ldg(fp2 + i);
+  const bool ok = w.x < FP_CHAIN;
+  p.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
+  p.ch = (int64_t)w.y;
+  p.rI = ok ? (int)(w.x >> FP_FBITS) : 0;
+  p.uI = ok ? (int)(w.y >> FP_FBITS) : 0;
+  const float sc = 1.0f / (float)(1u << FP_FBITS);
+  p.x = ok ? (float)(w.x & FP_FMASK) * sc : 0.f;
+  p.y = ok ? (float)(w.y & FP_FMASK) * sc : 0.f;
+  return p;
+}
+
+template <typename T, int CELLS>
+__global__ void __launch_bounds__(32 * DR_W, 3)
     drift_kernel(const T *__restrict__ C, T *__restrict__ f,
                  const int32_t *__restrict__ idx, const T *__restrict__ fx,
-                 const T *__restrict__ fy, const int64_t *__restrict__ ch_start,
+                 const T *__restrict__ fy, const uint2 *__restrict__ fp2,
+                 const int64_t *__restrict__ ch_start,
                  const int32_t *__restrict__ ch_len,
                  const T *__restrict__ ch_val, int64_t ndrift, MomentTables mt,
                  double *__restrict__ partial, Geometry g) {
@@ -314,24 +441,41 @@ __global__ void __launch_bounds__(32 * DR_W)
   const int r = blockIdx.x * 32 + lane;
   const int j = blockIdx.y;
   const T *Cj = C + (size_t)j * (g.nu + 3) * g.pc;
+  // each warp walks a contiguous band of u rows: consecutive rows have
+  // neighbouring footpoints, so their 4x4 patches overlap in L1
+  const int band = (g.nu + DR_W - 1) / DR_W;
+  const int ub = w * band;
+  const int ue = min(g.nu, ub + band);
   double acc = 0.0;
   if (r < g.nr) {
-    for (int u = w; u < g.nu; u += DR_W) {
-      const size_t i = ((size_t)j * g.nu + u) * g.nr + r;
-      const int code = __ldg(idx + i);
-      T v;
-      if (code >= 0) {
-        v = eval2d<T>(Cj, g.pc, code & 0xffff, __ldg(fx + i), code >> 16,
-                      __ldg(fy + i));
-      } else if (code == -1) {
-        v = T(0);
-      } else {
-        const int64_t ch = -2 - (int64_t)code;
-        const int L = __ldg(ch_len + ch);
-        v = ch_val[__ldg(ch_start + ch) + ndrift % L];
+    for (int u0 = ub; u0 < ue; u0 += CELLS) {
+      Foot<T> p[CELLS];
+#pragma unroll
+      for (int c = 0; c < CELLS; ++c) {
+        const int u = u0 + c;
+        const size_t i = ((size_t)j * g.nu + (u < ue ? u : ub)) * g.nr + r;
+        p[c] = load_foot(idx, fx, fy, fp2, i);
+        if (u >= ue) p[c].kind = 1;
       }
-      f[i] = v;
-      acc += __ldg(mt.bu + u) * (double)v;
+      T v[CELLS];
+#pragma unroll
+      for (int c = 0; c < CELLS; ++c) {
+        // branch-free gather (special cells read a valid patch with weight 0)
+        v[c] = eval2d<T>(Cj, g.pc, p[c].rI, p[c].x, p[c].uI, p[c].y);
+        if (p[c].kind == 1) v[c] = T(0);
+      }
+#pragma unroll
+      for (int c = 0; c < CELLS; ++c) {
+        const int u = u0 + c;
+        if (u < ue) {
+          if (p[c].kind == 2) {
+            const int L = __ldg(ch_len + p[c].ch);
+            v[c] = ch_val[__ldg(ch_start + p[c].ch) + ndrift % L];
+          }
+          f[((size_t)j * g.nu + u) * g.nr + r] = v[c];
+          acc += __ldg(mt.bu + u) * (double)v[c];
+        }
+      }
     }
   }
   __shared__ double red[DR_W][32];
@@ -347,13 +491,15 @@ __global__ void __launch_bounds__(32 * DR_W)
 
 template <typename T>
 cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
-                         const T *fy, const int64_t *ch_start,
+                         const T *fy, const uint2 *fp2, const int64_t *ch_start,
                          const int32_t *ch_len, const T *ch_val,
                          int64_t ndrift, const MomentTables &mt, double *partial,
                          const Geometry &g, cudaStream_t st) {
   dim3 grid((g.nr + 31) / 32, g.nj);
-  drift_kernel<T><<<grid, 32 * DR_W, 0, st>>>(C, f, idx, fx, fy, ch_start, ch_len,
-                                               ch_val, ndrift, mt, partial, g);
+  constexpr int CELLS = sizeof(T) == 4 ? 4 : 2;
+  drift_kernel<T, CELLS><<<grid, 32 * DR_W, 0, st>>>(C, f, idx, fx, fy, fp2, ch_start,
+                                                      ch_len, ch_val, ndrift, mt,
+                                                      partial, g);
   return cudaGetLastError();
 }
 
@@ -670,15 +816,10 @@ cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
 }
 
 #define VLS_INST(T)                                                            \
-  template cudaError_t launch_ucol<T>(bool, const T *, T *, const double *,     \
-                                      const Geometry &, const DirTables &,      \
-                                      cudaStream_t);                            \
-  template cudaError_t launch_prer<T>(const T *, T *, const Geometry &,         \
-                                      const DirTables &, cudaStream_t);         \
   template cudaError_t launch_drift<T>(                                         \
-      const T *, T *, const int32_t *, const T *, const T *, const int64_t *,    \
-      const int32_t *, const T *, int64_t, const MomentTables &, double *,       \
-      const Geometry &, cudaStream_t);                                          \
+      const T *, T *, const int32_t *, const T *, const T *, const uint2 *,      \
+      const int64_t *, const int32_t *, const T *, int64_t,                     \
+      const MomentTables &, double *, const Geometry &, cudaStream_t);          \
   template cudaError_t launch_chain_tails<T>(                                   \
       const T *, T *, const int64_t *, const int32_t *, const int32_t *,         \
       const double *, const double *, int64_t, int64_t, const Geometry &,       \
@@ -699,5 +840,16 @@ cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
 
 VLS_INST(float)
 VLS_INST(double)
+
+#define VLS_INST_TR(T, R)                                                       \
+  template cudaError_t launch_ucol<T, R>(bool, const T *, T *, const double *,  \
+                                         const Geometry &, const DirTables &,   \
+                                         cudaStream_t);                         \
+  template cudaError_t launch_prer<T, R>(const T *, T *, const Geometry &,      \
+                                         const DirTables &, cudaStream_t);
+
+VLS_INST_TR(double, double)
+VLS_INST_TR(float, double)
+VLS_INST_TR(float, float)
 
 }  // namespace vls
