@@ -165,81 +165,137 @@ __device__ void load_tables(R *rp, R *q, const DirTables &t) {
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) / 16 * 16; }
 
 // ------------------------------------------------------------------ ucol
-// Block: TW columns (r) x NSEG segments (u), lane = column so every shared
-// row access is one conflict-free wavefront.  Shared: the Thomas tables and
-// two buffers of (N_u+3) rows x TW (row N_u+2 is an always-zero guard row).
+// Block: TW columns (r) x NSEG segments (u), lane = column, so a shared row
+// access by a warp is one (FP32) or two (FP64) wavefronts.  Shared memory:
+// the Thomas tables and two buffers of (N_u+3) rows x TW in the recursion
+// type R (row N_u+2 is an always-zero guard row); global f and G are type T,
+// so T -> R and R -> T conversions happen once per element, at the tile load
+// and at the tile store.
 constexpr int UC_THREADS = 256;
-template <typename T>
+template <typename R>
 struct UcolCfg {
-  // 16 FP32 / 8 FP64 columns: two (N_u+3)-row buffers stay under 75 KB at
-  // N_u = 513 (three blocks per SM) and fit at N_u = 1025
-  static constexpr int TW = sizeof(T) == 4 ? 16 : 8;
+  static constexpr int TW = sizeof(R) == 4 ? 16 : 8;
   static constexpr int NSEG = UC_THREADS / TW;
 };
+
+// loads rows 1..nu of a TW-column tile of f (r0.., slice base fs) into buf
+template <typename T, typename R, int TW>
+__device__ __forceinline__ void load_col_tile(R *buf, const T *__restrict__ fs,
+                                              int nu, int nr, int r0) {
+  if constexpr (sizeof(T) == sizeof(R)) {
+    for (int e = threadIdx.x; e < nu * TW; e += blockDim.x) {
+      const int k = e / TW + 1, c = e % TW;
+      const int rr = r0 + c;
+      if (rr < nr)
+        cp_async(reinterpret_cast<T *>(&buf[k * TW + c]), fs + (size_t)(k - 1) * nr + rr);
+      else
+        buf[k * TW + c] = R(0);
+    }
+    cp_async_wait_all();
+  } else {
+    // four loads in flight per thread, then convert
+    const int n = nu * TW;
+    for (int e0 = threadIdx.x; e0 < n; e0 += 4 * blockDim.x) {
+      T v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int e = e0 + q * blockDim.x;
+        const int k = e / TW + 1, c = e % TW, rr = r0 + c;
+        v[q] = (e < n && rr < nr) ? __ldg(fs + (size_t)(k - 1) * nr + rr) : T(0);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int e = e0 + q * blockDim.x;
+        if (e < n) buf[(e / TW + 1) * TW + e % TW] = (R)v[q];
+      }
+    }
+  }
+}
+
+// exact per-cell kick index computation (vlasovSolver21_spline.hxx:760-762,
+// localSpline.hxx:426-429), used where the column's fractional shift lies
+// within 1e-9 of a node
+template <typename R, int TW>
+__device__ __forceinline__ R kick_exact(const R *cb, const Geometry &g, int u,
+                                        double s) {
+  const double newU = __ldg(g.U + u) + s;
+  if (!(newU > g.u0 && newU < g.umax)) return R(0);  // outside (or NaN) -> 0
+  const double y = (newU - g.su) * g.hu;
+  const double fl = floor(y);
+  const R fr = (R)(y - fl);
+  const int Ny = 1 + (int)fl;
+  return (R(1) / R(6)) *
+         (bv2<R>(R(1) - fr) * cb[(Ny - 1) * TW] + bv1<R>(R(1) - fr) * cb[Ny * TW] +
+          bv1<R>(fr) * cb[(Ny + 1) * TW] + bv2<R>(fr) * cb[(Ny + 2) * TW]);
+}
 
 template <typename T, typename R, bool KICK>
 __global__ void __launch_bounds__(UC_THREADS)
     ucol_kernel(const T *__restrict__ f, T *__restrict__ G,
                 const double *__restrict__ shift, Geometry g, DirTables tu) {
-  constexpr int TW = UcolCfg<T>::TW, NSEG = UcolCfg<T>::NSEG;
+  constexpr int TW = UcolCfg<R>::TW, NSEG = UcolCfg<R>::NSEG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int M = g.nu + 2;
   const int rows = M + 1;
   R *rp = reinterpret_cast<R *>(smem_raw);
   R *qq = rp + M;
-  T *bufA = reinterpret_cast<T *>(smem_raw + align16(2 * M * sizeof(R)));
-  T *bufB = bufA + (size_t)rows * TW;
+  R *bufA = reinterpret_cast<R *>(smem_raw + align16(2 * M * sizeof(R)));
+  R *bufB = bufA + (size_t)rows * TW;
   const int tid = threadIdx.x;
   const int col = tid % TW;
   const int seg = tid / TW;
   const int r0 = blockIdx.x * TW;
   const int j = blockIdx.y;
   const int r = r0 + col;
-  const size_t fslice = (size_t)j * g.nu * g.nr;
 
-  for (int e = tid; e < g.nu * TW; e += UC_THREADS) {
-    const int k = e / TW + 1, c = e % TW;
-    const int rr = r0 + c;
-    if (rr < g.nr)
-      cp_async(&bufA[k * TW + c], f + fslice + (size_t)(k - 1) * g.nr + rr);
-    else
-      bufA[k * TW + c] = T(0);
-  }
   load_tables<R>(rp, qq, tu);
   if (tid < TW) {
-    bufA[0 * TW + tid] = T(0);
-    bufA[(M - 1) * TW + tid] = T(0);
-    bufA[M * TW + tid] = T(0);
-    bufB[0 * TW + tid] = T(0);
-    bufB[(M - 1) * TW + tid] = T(0);
-    bufB[M * TW + tid] = T(0);
+    bufA[0 * TW + tid] = R(0);
+    bufA[(M - 1) * TW + tid] = R(0);
+    bufA[M * TW + tid] = R(0);
+    bufB[0 * TW + tid] = R(0);
+    bufB[(M - 1) * TW + tid] = R(0);
+    bufB[M * TW + tid] = R(0);
   }
-  cp_async_wait_all();
+  load_col_tile<T, R, TW>(bufA, f + (size_t)j * g.nu * g.nr, g.nu, g.nr, r0);
   __syncthreads();
   int k0, k1;
   seg_bounds(M, NSEG, seg, k0, k1);
   solve_lines<Prec<T>::K, R>(bufA + col, TW, k0, k1, tu, rp, qq);
 
-  T *out = bufA;
+  R *out = bufA;
   if (KICK) {
-    // kick gather (localSpline.hxx:423-441 with the r-direction (1,4,1)/6
-    // weights folded into the u-only coefficients), vlasovSolver21_spline.hxx:758-763
+    // kick (vlasovSolver21_spline.hxx:758-763, localSpline.hxx:423-441 with
+    // the r-direction (1,4,1)/6 weights folded into the u-only coefficients).
+    // The shift is constant along the column and the u grid is uniform, so
+    // y_u = u + s*hu: one fraction and one integer offset serve every row,
+    // unless that fraction is within 1e-9 of a node (then every row takes
+    // the exact per-cell path).
     const double s = (r < g.nr) ? __ldg(shift + r) : 0.0;
-    const T *cb = bufA + col;
-#pragma unroll 2
+    const double qf = s * g.hu;
+    const double fl = floor(qf);
+    const double frd = qf - fl;
+    const bool fast = frd > 1e-9 && frd < 1.0 - 1e-9 && fabs(qf) < 1e6;
+    const int o = fast ? (int)fl : 0;
+    const R fr = (R)frd;
+    const R w0 = bv2<R>(R(1) - fr) * (R(1) / R(6)), w1 = bv1<R>(R(1) - fr) * (R(1) / R(6));
+    const R w2 = bv1<R>(fr) * (R(1) / R(6)), w3 = bv2<R>(fr) * (R(1) / R(6));
+    // rows with 0 < u + qf < nu - 1 are inside (strictly, as :761)
+    const int ulo = fast ? (int)floor(-qf) + 1 : 0;
+    const int uhi = fast ? (int)ceil((double)(g.nu - 1) - qf) - 1 : -1;
+    const R *cb = bufA + col;
+#pragma unroll 4
     for (int k = k0; k < k1; ++k) {
       const int u = k - 1;
-      const double newU = __ldg(g.U + u) + s;
-      T v = T(0);
-      // outside (or NaN) -> 0, as vlasovSolver21_spline.hxx:761
-      if (newU > g.u0 && newU < g.umax) {
-        const double y = (newU - g.su) * g.hu;
-        const double fl = floor(y);
-        const T fr = (T)(y - fl);
-        const int Ny = 1 + (int)fl;
-        v = (T(1) / T(6)) *
-            (bv2<T>(T(1) - fr) * cb[(Ny - 1) * TW] + bv1<T>(T(1) - fr) * cb[Ny * TW] +
-             bv1<T>(fr) * cb[(Ny + 1) * TW] + bv2<T>(fr) * cb[(Ny + 2) * TW]);
+      R v;
+      if (fast) {
+        v = R(0);
+        if (u >= ulo && u <= uhi) {
+          const R *p = cb + (k + o - 1) * TW;
+          v = w0 * p[0] + w1 * p[TW] + w2 * p[2 * TW] + w3 * p[3 * TW];
+        }
+      } else {
+        v = kick_exact<R, TW>(cb, g, u, s);
       }
       bufB[k * TW + col] = v;
     }
@@ -247,20 +303,20 @@ __global__ void __launch_bounds__(UC_THREADS)
     solve_lines<Prec<T>::K, R>(bufB + col, TW, k0, k1, tu, rp, qq);
     out = bufB;
   }
-  const size_t gslice = (size_t)j * M * g.nr;
+  T *Gs = G + (size_t)j * M * g.nr;
   for (int e = tid; e < M * TW; e += UC_THREADS) {
     const int k = e / TW, c = e % TW;
     const int rr = r0 + c;
-    if (rr < g.nr) G[gslice + (size_t)k * g.nr + rr] = out[k * TW + c];
+    if (rr < g.nr) Gs[(size_t)k * g.nr + rr] = (T)out[k * TW + c];
   }
 }
 
 template <typename T, typename R>
 cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
                         const Geometry &g, const DirTables &tu, cudaStream_t st) {
-  constexpr int TW = UcolCfg<T>::TW;
+  constexpr int TW = UcolCfg<R>::TW;
   const size_t smem =
-      align16(2 * (size_t)(g.nu + 2) * sizeof(R)) + 2 * (size_t)(g.nu + 3) * TW * sizeof(T);
+      align16(2 * (size_t)(g.nu + 2) * sizeof(R)) + 2 * (size_t)(g.nu + 3) * TW * sizeof(R);
   dim3 grid((g.nr + TW - 1) / TW, g.nj);
   cudaError_t e;
   if (kick) {
@@ -279,11 +335,12 @@ cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
 
 // ------------------------------------------------------------------ prer
 // Block: ROWS rows of G (lane = row) x NSEG long segments along r.  The
-// shared row pitch is odd (FP64) or 1 mod 32 (FP32) so that the lanes, which
-// walk different rows at the same column, hit distinct banks.
-template <typename T>
+// shared row pitch is 1 mod 32 (FP32) or odd (FP64) so that the lanes, which
+// walk different rows at the same column, hit distinct banks.  Shared rows
+// are in the recursion type R.
+template <typename R>
 struct PrerCfg {
-  static constexpr int ROWS = sizeof(T) == 4 ? 32 : 16;
+  static constexpr int ROWS = sizeof(R) == 4 ? 32 : 16;
   static constexpr int NSEG = 8;
   static constexpr int THREADS = ROWS * NSEG;
 };
@@ -298,64 +355,82 @@ __host__ __device__ inline int prer_pitch(int M, int elem) {
 }
 
 template <typename T, typename R>
-__global__ void __launch_bounds__(PrerCfg<T>::THREADS)
+__global__ void __launch_bounds__(PrerCfg<R>::THREADS)
     prer_kernel(const T *__restrict__ G, T *__restrict__ C, Geometry g,
                 DirTables tr) {
-  constexpr int ROWS = PrerCfg<T>::ROWS, NSEG = PrerCfg<T>::NSEG,
-                NT = PrerCfg<T>::THREADS;
+  constexpr int ROWS = PrerCfg<R>::ROWS, NSEG = PrerCfg<R>::NSEG,
+                NT = PrerCfg<R>::THREADS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int M = g.nr + 2;
-  const int LS = prer_pitch(M, sizeof(T));
+  const int LS = prer_pitch(M, sizeof(R));
   R *rp = reinterpret_cast<R *>(smem_raw);
   R *qq = rp + M;
-  T *buf = reinterpret_cast<T *>(smem_raw + align16(2 * M * sizeof(R)));
+  R *buf = reinterpret_cast<R *>(smem_raw + align16(2 * M * sizeof(R)));
   const int tid = threadIdx.x;
   const int rho = tid % ROWS;
   const int seg = tid / ROWS;
   const int j = blockIdx.y;
   const int kr0 = blockIdx.x * ROWS;
   const int nrows = g.nu + 2;
-  const size_t gslice = (size_t)j * nrows * g.nr;
-  for (int e = tid; e < ROWS * g.nr; e += NT) {
-    const int p = e / g.nr, k = e % g.nr;
-    const int kr = kr0 + p;
-    if (kr < nrows)
-      cp_async(&buf[p * LS + k + 1], G + gslice + (size_t)kr * g.nr + k);
-    else
-      buf[p * LS + k + 1] = T(0);
-  }
+  const T *Gs = G + (size_t)j * nrows * g.nr;
   load_tables<R>(rp, qq, tr);
-  cp_async_wait_all();
+  if constexpr (sizeof(T) == sizeof(R)) {
+    for (int e = tid; e < ROWS * g.nr; e += NT) {
+      const int p = e / g.nr, k = e % g.nr;
+      const int kr = kr0 + p;
+      if (kr < nrows)
+        cp_async(reinterpret_cast<T *>(&buf[p * LS + k + 1]), Gs + (size_t)kr * g.nr + k);
+      else
+        buf[p * LS + k + 1] = R(0);
+    }
+    cp_async_wait_all();
+  } else {
+    const int n = ROWS * g.nr;
+    for (int e0 = tid; e0 < n; e0 += 4 * NT) {
+      T v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int e = e0 + q * NT;
+        const int p = e / g.nr, k = e % g.nr, kr = kr0 + p;
+        v[q] = (e < n && kr < nrows) ? __ldg(Gs + (size_t)kr * g.nr + k) : T(0);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int e = e0 + q * NT;
+        if (e < n) buf[(e / g.nr) * LS + e % g.nr + 1] = (R)v[q];
+      }
+    }
+  }
   __syncthreads();
   int k0, k1;
   seg_bounds(M, NSEG, seg, k0, k1);
   solve_lines<Prec<T>::K, R>(buf + rho * LS, 1, k0, k1, tr, rp, qq);
-  const size_t cslice = (size_t)j * (g.nu + 3) * g.pc;
+  T *Cs = C + (size_t)j * (g.nu + 3) * g.pc;
   for (int e = tid; e < ROWS * M; e += NT) {
     const int p = e / M, k = e % M;
     const int kr = kr0 + p;
-    if (kr < nrows) C[cslice + (size_t)kr * g.pc + k] = buf[p * LS + k];
+    if (kr < nrows) Cs[(size_t)kr * g.pc + k] = (T)buf[p * LS + k];
   }
 }
 
 template <typename T, typename R>
 cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr,
                         cudaStream_t st) {
-  constexpr int ROWS = PrerCfg<T>::ROWS;
+  constexpr int ROWS = PrerCfg<R>::ROWS;
   const int M = g.nr + 2;
   const size_t smem = align16(2 * (size_t)M * sizeof(R)) +
-                      (size_t)ROWS * prer_pitch(M, sizeof(T)) * sizeof(T);
+                      (size_t)ROWS * prer_pitch(M, sizeof(R)) * sizeof(R);
   dim3 grid((g.nu + 2 + ROWS - 1) / ROWS, g.nj);
   cudaError_t e = cudaFuncSetAttribute(
       prer_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  prer_kernel<T, R><<<grid, PrerCfg<T>::THREADS, smem, st>>>(G, C, g, tr);
+  prer_kernel<T, R><<<grid, PrerCfg<R>::THREADS, smem, st>>>(G, C, g, tr);
   return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ gather
 // localSpline::evaluateC(int,double,int,double), localSpline.hxx:381-398:
-// taps at padded columns rI..rI+3 and rows uI..uI+3.
+// taps at padded columns rI..rI+3 and rows uI..uI+3 (FP64 form).
 template <typename T>
 __device__ __forceinline__ T eval2d(const T *__restrict__ Cj, int pc, int rI,
                                     T x, int uI, T y) {
@@ -377,13 +452,45 @@ __device__ __forceinline__ T eval2d(const T *__restrict__ Cj, int pc, int rI,
                            bv1<T>(y) * s2 + bv2<T>(y) * s3);
 }
 
+// FP32 form with packed f32x2 arithmetic: the x and y weights are computed
+// pairwise, and rows (0,1) and (2,3) are accumulated pairwise.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+__device__ __forceinline__ float eval2d_f32x2(const float *__restrict__ Cj, int pc,
+                                              int off, float x, float y) {
+  const float2 t = f2(x, y);
+  const float2 one = f2(1.f, 1.f), three = f2(3.f, 3.f), m3 = f2(-3.f, -3.f);
+  const float2 s = __fadd2_rn(one, f2(-t.x, -t.y));        // 1 - t
+  const float2 t2 = __fmul2_rn(t, t), t3 = __fmul2_rn(t2, t);
+  const float2 s2 = __fmul2_rn(s, s), s3 = __fmul2_rn(s2, s);
+  // BV1(v) = 1 + 3v + 3v^2 - 3v^3
+  const float2 a1 = __ffma2_rn(m3, s3, __ffma2_rn(three, s2, __ffma2_rn(three, s, one)));
+  const float2 b1 = __ffma2_rn(m3, t3, __ffma2_rn(three, t2, __ffma2_rn(three, t, one)));
+  // x weights: (s3.x, a1.x, b1.x, t3.x); y weights: (s3.y, a1.y, b1.y, t3.y)
+  const float *p = Cj + off;
+  const float2 wx0 = f2(s3.x, s3.x), wx1 = f2(a1.x, a1.x), wx2 = f2(b1.x, b1.x),
+               wx3 = f2(t3.x, t3.x);
+  float2 r01 = __fmul2_rn(f2(__ldg(p), __ldg(p + pc)), wx0);
+  r01 = __ffma2_rn(f2(__ldg(p + 1), __ldg(p + pc + 1)), wx1, r01);
+  r01 = __ffma2_rn(f2(__ldg(p + 2), __ldg(p + pc + 2)), wx2, r01);
+  r01 = __ffma2_rn(f2(__ldg(p + 3), __ldg(p + pc + 3)), wx3, r01);
+  const float *p2 = p + 2 * pc;
+  float2 r23 = __fmul2_rn(f2(__ldg(p2), __ldg(p2 + pc)), wx0);
+  r23 = __ffma2_rn(f2(__ldg(p2 + 1), __ldg(p2 + pc + 1)), wx1, r23);
+  r23 = __ffma2_rn(f2(__ldg(p2 + 2), __ldg(p2 + pc + 2)), wx2, r23);
+  r23 = __ffma2_rn(f2(__ldg(p2 + 3), __ldg(p2 + pc + 3)), wx3, r23);
+  // y weights (rows 0..3) applied pairwise, times 1/36
+  const float2 acc = __ffma2_rn(r23, f2(b1.y, t3.y), __fmul2_rn(r01, f2(s3.y, a1.y)));
+  return (acc.x + acc.y) * (1.f / 36.f);
+}
+
 constexpr int DR_W = 8;  // warps per drift block
 
 // footpoint of one cell, decoded: taps at (rI.., uI..) with fractions (x, y);
 // kind 0 = gather, 1 = outside (0), 2 = delayed-kernel chain `ch`
 template <typename T>
 struct Foot {
-  int rI, uI, kind;
+  int off, kind;
   int64_t ch;
   T x, y;
 };
@@ -392,13 +499,12 @@ struct Foot {
 __device__ __forceinline__ Foot<double> load_foot(const int32_t *__restrict__ idx,
                                                   const double *__restrict__ fx,
                                                   const double *__restrict__ fy,
-                                                  const uint2 *, size_t i) {
+                                                  const uint2 *, size_t i, int pc) {
   Foot<double> p;
   const int code = __ldg(idx + i);
   p.kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
   p.ch = -2 - (int64_t)code;
-  p.rI = code >= 0 ? (code & 0xffff) : 0;
-  p.uI = code >= 0 ? (code >> 16) : 0;
+  p.off = code >= 0 ? (code >> 16) * pc + (code & 0xffff) : 0;
   p.x = code >= 0 ? __ldg(fx + i) : 0.0;
   p.y = code >= 0 ? __ldg(fy + i) : 0.0;
   return p;
@@ -406,26 +512,42 @@ __device__ __forceinline__ Foot<double> load_foot(const int32_t *__restrict__ id
 
 // FP32 tables, 8 bytes per cell: word = index << FP_FBITS | round(frac * 2^FP_FBITS)
 // per direction; FP_OUT / FP_CHAIN in the first word mark the two special kinds
-// (the second word then holds the chain id)
+// (the second word then holds the chain id).  The 21 fraction bits are placed
+// straight into a float mantissa (value 1.frac, minus 1): no int->float convert.
 constexpr int FP_FBITS = 21;
 constexpr uint32_t FP_FMASK = (1u << FP_FBITS) - 1u;
 constexpr uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu;
 
+__device__ __forceinline__ float frac21(uint32_t w) {
+  return __uint_as_float(0x3F800000u | ((w & FP_FMASK) << 2)) - 1.0f;
+}
+
 __device__ __forceinline__ Foot<float> load_foot(const int32_t *, const float *,
                                                  const float *,
                                                  const uint2 *__restrict__ fp2,
-                                                 size_t i) {
+                                                 size_t i, int pc) {
   Foot<float> p;
   const uint2 w = __ldg(fp2 + i);
   const bool ok = w.x < FP_CHAIN;
   p.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
   p.ch = (int64_t)w.y;
-  p.rI = ok ? (int)(w.x >> FP_FBITS) : 0;
-  p.uI = ok ? (int)(w.y >> FP_FBITS) : 0;
-  const float sc = 1.0f / (float)(1u << FP_FBITS);
-  p.x = ok ? (float)(w.x & FP_FMASK) * sc : 0.f;
-  p.y = ok ? (float)(w.y & FP_FMASK) * sc : 0.f;
+  p.off = ok ? (int)(w.y >> FP_FBITS) * pc + (int)(w.x >> FP_FBITS) : 0;
+  p.x = frac21(w.x);
+  p.y = frac21(w.y);
   return p;
+}
+
+template <typename T>
+__device__ __forceinline__ T eval_cell(const T *Cj, int pc, const Foot<T> &p);
+template <>
+__device__ __forceinline__ double eval_cell<double>(const double *Cj, int pc,
+                                                    const Foot<double> &p) {
+  return eval2d<double>(Cj + p.off, pc, 0, p.x, 0, p.y);
+}
+template <>
+__device__ __forceinline__ float eval_cell<float>(const float *Cj, int pc,
+                                                  const Foot<float> &p) {
+  return eval2d_f32x2(Cj, pc, p.off, p.x, p.y);
 }
 
 template <typename T, int CELLS>
@@ -454,16 +576,17 @@ __global__ void __launch_bounds__(32 * DR_W, 3)
       for (int c = 0; c < CELLS; ++c) {
         const int u = u0 + c;
         const size_t i = ((size_t)j * g.nu + (u < ue ? u : ub)) * g.nr + r;
-        p[c] = load_foot(idx, fx, fy, fp2, i);
+        p[c] = load_foot(idx, fx, fy, fp2, i, g.pc);
         if (u >= ue) p[c].kind = 1;
       }
       T v[CELLS];
 #pragma unroll
       for (int c = 0; c < CELLS; ++c) {
-        // branch-free gather (special cells read a valid patch with weight 0)
-        v[c] = eval2d<T>(Cj, g.pc, p[c].rI, p[c].x, p[c].uI, p[c].y);
+        // branch-free gather (special cells read a valid patch, then drop it)
+        v[c] = eval_cell<T>(Cj, g.pc, p[c]);
         if (p[c].kind == 1) v[c] = T(0);
       }
+      T part = T(0);
 #pragma unroll
       for (int c = 0; c < CELLS; ++c) {
         const int u = u0 + c;
@@ -473,9 +596,11 @@ __global__ void __launch_bounds__(32 * DR_W, 3)
             v[c] = ch_val[__ldg(ch_start + p[c].ch) + ndrift % L];
           }
           f[((size_t)j * g.nu + u) * g.nr + r] = v[c];
-          acc += __ldg(mt.bu + u) * (double)v[c];
+          part += (T)__ldg(mt.bu + u) * v[c];
         }
       }
+      // moment partial: CELLS products summed in T, then accumulated in FP64
+      acc += (double)part;
     }
   }
   __shared__ double red[DR_W][32];
