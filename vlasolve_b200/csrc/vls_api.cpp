@@ -1,8 +1,12 @@
 // vls_api.cpp -- the C-ABI of include/vlasolve_b200.h: handle life cycle,
 // host set-up upload, step orchestration on the handle's CUDA stream,
 // moments, statistics and NDfield I/O.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <omp.h>
+
+#include <cstdlib>
 
 #include <algorithm>
 #include <cmath>
@@ -61,6 +65,9 @@ struct vls_handle {
   double time = 0;
   int64_t step = 0;
   int64_t launches = 0;
+  // TMA descriptor of C for the drift's staged coefficient windows
+  CUtensorMap tmC{};
+  bool have_tma = false;
   // opt-in per-kernel event timing
   bool profiling = false;
   struct ProfRec {
@@ -145,6 +152,10 @@ static DirTables dir_tables(const HostDirTables &t, const double *rp,
   d.L1 = t.L1;
   d.L2 = t.L2;
   d.M = t.M;
+  d.kc64 = t.kc64;
+  d.kc32 = t.kc32;
+  d.rp_inf = t.rp_inf;
+  d.q_inf = t.q_inf;
   return d;
 }
 
@@ -357,6 +368,37 @@ static int setup_chain_device(vls_handle *h) {
   return VLS_OK;
 }
 
+// 3D tiled tensor map of C ([N_J][N_u+3][pc], element T): boxes of 64
+// columns x 40 rows x 1 slice for the drift windows.  The encoder is the
+// driver's cuTensorMapEncodeTiled, reached through the runtime (no libcuda
+// link).  Returns false when unavailable (the drift then gathers from global
+// memory directly).
+static bool make_tensor_map(vls_handle *h) {
+  if (std::getenv("VLS_NO_TMA")) return false;
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    cudaGetLastError();
+    return false;
+  }
+  auto enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  const cuuint64_t es = h->esize;
+  const cuuint64_t dims[3] = {(cuuint64_t)h->pc, (cuuint64_t)h->co.nu + 3,
+                              (cuuint64_t)h->co.nj};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->pc * es,
+                                 (cuuint64_t)h->pc * es * (cuuint64_t)(h->co.nu + 3)};
+  const cuuint32_t box[3] = {64, 40, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(&h->tmC,
+                         es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         3, h->C, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 // ------------------------------------------------------------- life cycle
 extern "C" int vls_version(int32_t *major, int32_t *minor) {
   if (major) *major = 0;
@@ -489,8 +531,10 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   };
   if (cudaMemsetAsync(h->C, 0, es * (size_t)c.nj * (c.nu + 3) * h->pc, h->st) !=
           cudaSuccess ||
-      cudaMemsetAsync(h->count, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess)
+      cudaMemsetAsync(h->count, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess ||
+      cudaMemsetAsync(h->flag, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess)
     return fin(fail(hp, VLS_ECUDA, "cudaMemsetAsync failed"));
+  h->have_tma = make_tensor_map(hp);
   // tables
   std::vector<double> dR(c.nr), dU(c.nu), Ct1(c.nj), bu(c.nu), wj(c.nj), dR4(c.nr),
       Rcoef(c.nr);
@@ -568,6 +612,8 @@ extern "C" int vls_coords(const vls_handle *h, double *R, double *U, double *J,
   return VLS_OK;
 }
 
+static int check_device_flags(vls_handle *h);
+
 // ------------------------------------------------------------- f transfer
 static int put_f(vls_handle *h, const double *host) {
   if (h->prec == VLS_FP64) {
@@ -605,7 +651,7 @@ static int take_f(vls_handle *h, double *host) {
     }
   }
   CK(h, cudaStreamSynchronize(h->st));
-  return VLS_OK;
+  return check_device_flags(h);
 }
 
 extern "C" int vls_set_f(vls_handle *h, const double *host, size_t n) {
@@ -829,6 +875,12 @@ static int drift_once(vls_handle *h, bool kick) {
        }));
   }
   CK(h, timed(h, VLS_K_DRIFT, [&] {
+       if (h->have_tma)
+         return launch_drift_tma<T>(&h->tmC, (const T *)h->C, (T *)h->f, h->idx,
+                                    (const T *)h->fx, (const T *)h->fy, h->fp2,
+                                    h->ch_start, h->ch_len, (const T *)h->ch_val,
+                                    h->ndrift, moment_tables(h), h->partial,
+                                    h->flag + 1, g, h->st);
        return launch_drift<T>((const T *)h->C, (T *)h->f, h->idx, (const T *)h->fx,
                               (const T *)h->fy, h->fp2, h->ch_start, h->ch_len,
                               (const T *)h->ch_val, h->ndrift, moment_tables(h),
@@ -887,12 +939,26 @@ extern "C" int vls_step(vls_handle *h, int32_t nsteps) {
   }
 }
 
+// device-side status words: flag[1] bit 0/1 = a bounded mbarrier wait of the
+// drift timed out (the step then read global memory instead; results stay
+// valid but the hardware path misbehaved)
+static int check_device_flags(vls_handle *h) {
+  unsigned int fl[4] = {0, 0, 0, 0};
+  CK(h, cudaMemcpyAsync(fl, h->flag, sizeof(fl), cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  if (fl[1]) {
+    CK(h, cudaMemsetAsync(h->flag, 0, sizeof(fl), h->st));
+    return fail(h, VLS_ECUDA, "a bounded device wait timed out in the drift kernel");
+  }
+  return VLS_OK;
+}
+
 extern "C" int vls_sync(vls_handle *h) {
   if (!h) return VLS_EINVAL;
   CK(h, cudaSetDevice(h->solver.device));
   CK(h, cudaStreamSynchronize(h->st));
   CK(h, cudaGetLastError());
-  return VLS_OK;
+  return check_device_flags(h);
 }
 
 extern "C" int vls_kernel_launches(const vls_handle *h, int64_t *n) {

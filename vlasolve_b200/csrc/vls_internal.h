@@ -20,6 +20,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace vls {
@@ -32,6 +33,10 @@ struct DirTables {
   double a01, a02;   // normalised first row (-2, 1)
   double hi2, L1, L2;  // last-row constants
   int M;
+  // from row kc on (up to M-2) rp_k and q_k equal rp_inf, q_inf when rounded
+  // to the recursion's precision: kc64 for FP64, kc32 for FP32 recursions
+  int kc64, kc32;
+  double rp_inf, q_inf;
 };
 
 struct Geometry {
@@ -65,6 +70,15 @@ cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
                          const int32_t *ch_len, const T *ch_val,
                          int64_t ndrift, const MomentTables &mt, double *partial,
                          const Geometry &g, cudaStream_t st);
+// drift with the coefficient windows staged by TMA (tmC: 3D map of C, box
+// 64 columns x 40 rows x 1 slice); err receives bit 0 / 1 on a wait timeout
+template <typename T>
+cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int32_t *idx,
+                             const T *fx, const T *fy, const uint2 *fp2,
+                             const int64_t *ch_start, const int32_t *ch_len,
+                             const T *ch_val, int64_t ndrift, const MomentTables &mt,
+                             double *partial, unsigned int *err, const Geometry &g,
+                             cudaStream_t st);
 template <typename T>
 cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
                                const int32_t *ch_len, const int32_t *t_idx,

@@ -28,7 +28,7 @@ namespace vls {
 
 // warm-up rows of a segment: FP64 storage needs the recursion to contract to
 // FP64 rounding (0.268^32 = 5e-19), FP32 storage to well below FP32 rounding
-// (0.268^20 = 3.6e-12)
+// (0.268^16 = 7e-10)
 template <typename T>
 struct Prec;
 template <>
@@ -37,7 +37,7 @@ struct Prec<double> {
 };
 template <>
 struct Prec<float> {
-  static constexpr int K = 20;
+  static constexpr int K = 16;
 };
 
 template <typename T>
@@ -68,25 +68,45 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // entry rows 1..M-2 hold the data; on exit rows 0..M-1 hold the coefficients.
 // A thread owns interior rows [k0, k1).  The four stages are separated by
 // __syncthreads() (see solve_lines).  R is the arithmetic of the recursion.
+// The per-row coefficients rp_k, q_k are read from shared memory for rows
+// below kc and replaced by their limits from row kc on (they are equal there
+// in the recursion's precision), which removes two shared loads per element.
+template <typename R>
+struct Coef {
+  const R *rp, *q;
+  R rpi, qi, sixth;
+  int kc;
+  __device__ __forceinline__ R rpk(int k) const { return k < kc ? rp[k] : rpi; }
+  __device__ __forceinline__ R qk(int k) const { return k < kc ? q[k] : qi; }
+};
+
 template <int K, typename R>
 struct Seg {
   template <typename S>
-  __device__ static R fwd_warm(const S *b, int ks, int k0, const R *rp) {
+  __device__ __forceinline__ static R fwd_warm(const S *b, int ks, int k0, const Coef<R> &cf) {
     R d = R(0);
     int ks0 = k0 - K;
     if (ks0 < 1) ks0 = 1;
 #pragma unroll 4
-    for (int k = ks0; k < k0; ++k) d = ((R)b[k * ks] - d * (R(1) / R(6))) * rp[k];
+    for (int k = ks0; k < k0; ++k) d = ((R)b[k * ks] - d * cf.sixth) * cf.rpk(k);
     return d;
   }
   template <typename S>
-  __device__ static void fwd_main(S *b, int ks, int k0, int k1, R d,
-                                  const DirTables &t, const R *rp) {
+  __device__ __forceinline__ static void fwd_main(S *b, int ks, int k0, int k1, R d,
+                                  const DirTables &t, const Coef<R> &cf) {
     R dprev = d;
+    int k = k0;
+    const int kt = min(k1, max(k0, cf.kc));
 #pragma unroll 4
-    for (int k = k0; k < k1; ++k) {
+    for (; k < kt; ++k) {
       dprev = d;
-      d = ((R)b[k * ks] - d * (R(1) / R(6))) * rp[k];
+      d = ((R)b[k * ks] - d * cf.sixth) * cf.rp[k];
+      b[k * ks] = (S)d;
+    }
+#pragma unroll 4
+    for (; k < k1; ++k) {
+      dprev = d;
+      d = ((R)b[k * ks] - d * cf.sixth) * cf.rpi;
       b[k * ks] = (S)d;
     }
     if (k1 == t.M - 1 && k1 > k0) {
@@ -96,8 +116,8 @@ struct Seg {
     }
   }
   template <typename S>
-  __device__ static R bwd_warm(const S *b, int ks, int k1, const DirTables &t,
-                               const R *q) {
+  __device__ __forceinline__ static R bwd_warm(const S *b, int ks, int k1, const DirTables &t,
+                               const Coef<R> &cf) {
     int kst = k1 + K - 1;
     R c;
     if (kst >= t.M - 2) {
@@ -107,17 +127,25 @@ struct Seg {
       c = R(0);
     }
 #pragma unroll 4
-    for (int k = kst; k >= k1; --k) c = (R)b[k * ks] - q[k] * c;
+    for (int k = kst; k >= k1; --k) c = (R)b[k * ks] - cf.qk(k) * c;
     return c;
   }
   template <typename S>
-  __device__ static void bwd_main(S *b, int ks, int k0, int k1, R c,
-                                  const DirTables &t, const R *q) {
+  __device__ __forceinline__ static void bwd_main(S *b, int ks, int k0, int k1, R c,
+                                  const DirTables &t, const Coef<R> &cf) {
     R cnext = c;
+    int k = k1 - 1;
+    const int kt = max(k0, cf.kc);
 #pragma unroll 4
-    for (int k = k1 - 1; k >= k0; --k) {
+    for (; k >= kt; --k) {
       cnext = c;
-      c = (R)b[k * ks] - q[k] * c;
+      c = (R)b[k * ks] - cf.qi * c;
+      b[k * ks] = (S)c;
+    }
+#pragma unroll 4
+    for (; k >= k0; --k) {
+      cnext = c;
+      c = (R)b[k * ks] - cf.q[k] * c;
       b[k * ks] = (S)c;
     }
     if (k0 == 1 && k1 > k0) {
@@ -141,21 +169,28 @@ __device__ __forceinline__ void seg_bounds(int M, int nseg, int s, int &k0,
 
 // rp, q: the direction's tables in the recursion type (shared memory)
 template <int K, typename R, typename S>
-__device__ void solve_lines(S *base, int ks, int k0, int k1,
+__device__ __forceinline__ void solve_lines(S *base, int ks, int k0, int k1,
                             const DirTables &t, const R *rp, const R *q) {
-  R d = Seg<K, R>::fwd_warm(base, ks, k0, rp);
+  Coef<R> cf;
+  cf.rp = rp;
+  cf.q = q;
+  cf.rpi = (R)t.rp_inf;
+  cf.qi = (R)t.q_inf;
+  cf.sixth = R(1) / R(6);
+  cf.kc = sizeof(R) == 4 ? t.kc32 : t.kc64;
+  R d = Seg<K, R>::fwd_warm(base, ks, k0, cf);
   __syncthreads();
-  Seg<K, R>::fwd_main(base, ks, k0, k1, d, t, rp);
+  Seg<K, R>::fwd_main(base, ks, k0, k1, d, t, cf);
   __syncthreads();
-  R c = Seg<K, R>::bwd_warm(base, ks, k1, t, q);
+  R c = Seg<K, R>::bwd_warm(base, ks, k1, t, cf);
   __syncthreads();
-  Seg<K, R>::bwd_main(base, ks, k0, k1, c, t, q);
+  Seg<K, R>::bwd_main(base, ks, k0, k1, c, t, cf);
   __syncthreads();
 }
 
 // copies the direction's Thomas tables into shared memory as type R
 template <typename R>
-__device__ void load_tables(R *rp, R *q, const DirTables &t) {
+__device__ __forceinline__ void load_tables(R *rp, R *q, const DirTables &t) {
   for (int k = threadIdx.x; k < t.M; k += blockDim.x) {
     rp[k] = (R)__ldg(t.rp + k);
     q[k] = (R)__ldg(t.q + k);
@@ -234,7 +269,7 @@ __global__ void __launch_bounds__(UC_THREADS)
     ucol_kernel(const T *__restrict__ f, T *__restrict__ G,
                 const double *__restrict__ shift, Geometry g, DirTables tu) {
   constexpr int TW = UcolCfg<R>::TW, NSEG = UcolCfg<R>::NSEG;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int M = g.nu + 2;
   const int rows = M + 1;
   R *rp = reinterpret_cast<R *>(smem_raw);
@@ -284,20 +319,19 @@ __global__ void __launch_bounds__(UC_THREADS)
     const int ulo = fast ? (int)floor(-qf) + 1 : 0;
     const int uhi = fast ? (int)ceil((double)(g.nu - 1) - qf) - 1 : -1;
     const R *cb = bufA + col;
+    if (fast) {
 #pragma unroll 4
-    for (int k = k0; k < k1; ++k) {
-      const int u = k - 1;
-      R v;
-      if (fast) {
-        v = R(0);
+      for (int k = k0; k < k1; ++k) {
+        const int u = k - 1;
+        R v = R(0);
         if (u >= ulo && u <= uhi) {
           const R *p = cb + (k + o - 1) * TW;
           v = w0 * p[0] + w1 * p[TW] + w2 * p[2 * TW] + w3 * p[3 * TW];
         }
-      } else {
-        v = kick_exact<R, TW>(cb, g, u, s);
+        bufB[k * TW + col] = v;
       }
-      bufB[k * TW + col] = v;
+    } else {
+      for (int k = k0; k < k1; ++k) bufB[k * TW + col] = kick_exact<R, TW>(cb, g, k - 1, s);
     }
     __syncthreads();
     solve_lines<Prec<T>::K, R>(bufB + col, TW, k0, k1, tu, rp, qq);
@@ -360,7 +394,7 @@ __global__ void __launch_bounds__(PrerCfg<R>::THREADS)
                 DirTables tr) {
   constexpr int ROWS = PrerCfg<R>::ROWS, NSEG = PrerCfg<R>::NSEG,
                 NT = PrerCfg<R>::THREADS;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int M = g.nr + 2;
   const int LS = prer_pitch(M, sizeof(R));
   R *rp = reinterpret_cast<R *>(smem_raw);
@@ -374,42 +408,33 @@ __global__ void __launch_bounds__(PrerCfg<R>::THREADS)
   const int nrows = g.nu + 2;
   const T *Gs = G + (size_t)j * nrows * g.nr;
   load_tables<R>(rp, qq, tr);
-  if constexpr (sizeof(T) == sizeof(R)) {
-    for (int e = tid; e < ROWS * g.nr; e += NT) {
-      const int p = e / g.nr, k = e % g.nr;
-      const int kr = kr0 + p;
-      if (kr < nrows)
-        cp_async(reinterpret_cast<T *>(&buf[p * LS + k + 1]), Gs + (size_t)kr * g.nr + k);
-      else
-        buf[p * LS + k + 1] = R(0);
-    }
-    cp_async_wait_all();
-  } else {
-    const int n = ROWS * g.nr;
-    for (int e0 = tid; e0 < n; e0 += 4 * NT) {
-      T v[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int e = e0 + q * NT;
-        const int p = e / g.nr, k = e % g.nr, kr = kr0 + p;
-        v[q] = (e < n && kr < nrows) ? __ldg(Gs + (size_t)kr * g.nr + k) : T(0);
+  // rows of the tile, each copied by the whole block (no index division)
+  for (int p = 0; p < ROWS; ++p) {
+    const int kr = kr0 + p;
+    R *dst = buf + p * LS + 1;
+    if (kr < nrows) {
+      const T *src = Gs + (size_t)kr * g.nr;
+      if constexpr (sizeof(T) == sizeof(R)) {
+        for (int k = tid; k < g.nr; k += NT) cp_async(reinterpret_cast<T *>(dst + k), src + k);
+      } else {
+        for (int k = tid; k < g.nr; k += NT) dst[k] = (R)__ldg(src + k);
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int e = e0 + q * NT;
-        if (e < n) buf[(e / g.nr) * LS + e % g.nr + 1] = (R)v[q];
-      }
+    } else {
+      for (int k = tid; k < g.nr; k += NT) dst[k] = R(0);
     }
   }
+  if constexpr (sizeof(T) == sizeof(R)) cp_async_wait_all();
   __syncthreads();
   int k0, k1;
   seg_bounds(M, NSEG, seg, k0, k1);
   solve_lines<Prec<T>::K, R>(buf + rho * LS, 1, k0, k1, tr, rp, qq);
   T *Cs = C + (size_t)j * (g.nu + 3) * g.pc;
-  for (int e = tid; e < ROWS * M; e += NT) {
-    const int p = e / M, k = e % M;
+  for (int p = 0; p < ROWS; ++p) {
     const int kr = kr0 + p;
-    if (kr < nrows) Cs[(size_t)kr * g.pc + k] = (T)buf[p * LS + k];
+    if (kr >= nrows) break;
+    T *dst = Cs + (size_t)kr * g.pc;
+    const R *src = buf + p * LS;
+    for (int k = tid; k < M; k += NT) dst[k] = (T)src[k];
   }
 }
 
@@ -550,8 +575,28 @@ __device__ __forceinline__ float eval_cell<float>(const float *Cj, int pc,
   return eval2d_f32x2(Cj, pc, p.off, p.x, p.y);
 }
 
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <typename T, int CELLS>
-__global__ void __launch_bounds__(32 * DR_W, 3)
+__device__ __forceinline__ void load_group(Foot<T> (&p)[CELLS],
+                                           const int32_t *__restrict__ idx,
+                                           const T *__restrict__ fx,
+                                           const T *__restrict__ fy,
+                                           const uint2 *__restrict__ fp2,
+                                           size_t row0, int nr, int u0, int ue,
+                                           int pc) {
+#pragma unroll
+  for (int c = 0; c < CELLS; ++c) {
+    const int u = u0 + c;
+    p[c] = load_foot(idx, fx, fy, fp2, row0 + (size_t)(u < ue ? u : u0) * nr, pc);
+    if (u >= ue) p[c].kind = 1;
+  }
+}
+
+template <typename T, int CELLS>
+__global__ void __launch_bounds__(32 * DR_W, 4)
     drift_kernel(const T *__restrict__ C, T *__restrict__ f,
                  const int32_t *__restrict__ idx, const T *__restrict__ fx,
                  const T *__restrict__ fy, const uint2 *__restrict__ fp2,
@@ -568,17 +613,21 @@ __global__ void __launch_bounds__(32 * DR_W, 3)
   const int band = (g.nu + DR_W - 1) / DR_W;
   const int ub = w * band;
   const int ue = min(g.nu, ub + band);
+  const size_t row0 = (size_t)j * g.nu * g.nr + r;  // cell (j, u, r) = row0 + u*nr
   double acc = 0.0;
-  if (r < g.nr) {
+  if (r < g.nr && ub < ue) {
+    Foot<T> nxt[CELLS];
+    load_group<T, CELLS>(nxt, idx, fx, fy, fp2, row0, g.nr, ub, ue, g.pc);
     for (int u0 = ub; u0 < ue; u0 += CELLS) {
       Foot<T> p[CELLS];
 #pragma unroll
-      for (int c = 0; c < CELLS; ++c) {
-        const int u = u0 + c;
-        const size_t i = ((size_t)j * g.nu + (u < ue ? u : ub)) * g.nr + r;
-        p[c] = load_foot(idx, fx, fy, fp2, i, g.pc);
-        if (u >= ue) p[c].kind = 1;
-      }
+      for (int c = 0; c < CELLS; ++c) p[c] = nxt[c];
+      // footpoints of the next group are in flight while this one gathers
+      if (u0 + CELLS < ue)
+        load_group<T, CELLS>(nxt, idx, fx, fy, fp2, row0, g.nr, u0 + CELLS, ue, g.pc);
+      // most footpoints lie within a cell of their own node: warm L2 with
+      // the coefficient rows this warp reaches a few iterations from now
+      prefetch_l2(Cj + (size_t)min(u0 + 16, g.nu + 2) * g.pc + r);
       T v[CELLS];
 #pragma unroll
       for (int c = 0; c < CELLS; ++c) {
@@ -595,7 +644,7 @@ __global__ void __launch_bounds__(32 * DR_W, 3)
             const int L = __ldg(ch_len + p[c].ch);
             v[c] = ch_val[__ldg(ch_start + p[c].ch) + ndrift % L];
           }
-          f[((size_t)j * g.nu + u) * g.nr + r] = v[c];
+          f[row0 + (size_t)u * g.nr] = v[c];
           part += (T)__ldg(mt.bu + u) * v[c];
         }
       }
@@ -614,6 +663,272 @@ __global__ void __launch_bounds__(32 * DR_W, 3)
   }
 }
 
+// ------------------------------------------------------- TMA-staged drift
+// Most drift footpoints lie within a few cells of their own node, so each
+// block (a strip of 32 r columns of one J slice) walks down the rows in
+// chunks of DW_CH and has the tensor-memory accelerator bring the matching
+// DW_ROWS x DW_COLS window of the coefficient slice into shared memory,
+// double buffered and signalled through an mbarrier.  Taps inside the window
+// are read from shared memory; footpoints outside it (far displacements) read
+// the coefficients from global memory.  Every mbarrier wait is bounded: on
+// timeout the block records an error flag and falls back to global reads.
+constexpr int DW_COLS = 64, DW_ROWS = 40, DW_CH = 16, DW_XOFF = 16, DW_YOFF = 12;
+constexpr int DT_THREADS = 256;  // 8 warps x 32 columns; 2 rows per warp per chunk
+// a wait gives up after ~2^20 polls (tens of milliseconds at most)
+constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// non-blocking polls with a short sleep between them, at most MBAR_SPIN_LIMIT
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (uint32_t i = 0; i < MBAR_SPIN_LIMIT; ++i) {
+    if (mbar_test_wait(bar, parity)) return true;
+    if (i >= 32) __nanosleep(20);
+  }
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// 3D tiled TMA load (no multicast) of one box into shared memory
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, int x, int y,
+                                            int z, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <typename T>
+struct Cell {
+  int rI, uI, kind;
+  uint32_t ch;
+  T x, y;
+};
+
+__device__ __forceinline__ Cell<double> load_cell(const int32_t *__restrict__ idx,
+                                                  const double *__restrict__ fx,
+                                                  const double *__restrict__ fy,
+                                                  const uint2 *, size_t i) {
+  Cell<double> c;
+  const int code = __ldg(idx + i);
+  c.kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
+  c.ch = (uint32_t)(-2 - code);
+  c.rI = code >= 0 ? (code & 0xffff) : 0;
+  c.uI = code >= 0 ? (code >> 16) : 0;
+  c.x = code >= 0 ? __ldg(fx + i) : 0.0;
+  c.y = code >= 0 ? __ldg(fy + i) : 0.0;
+  return c;
+}
+__device__ __forceinline__ Cell<float> load_cell(const int32_t *, const float *,
+                                                 const float *,
+                                                 const uint2 *__restrict__ fp2, size_t i) {
+  Cell<float> c;
+  const uint2 w = __ldg(fp2 + i);
+  const bool ok = w.x < FP_CHAIN;
+  c.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
+  c.ch = w.y;
+  c.rI = ok ? (int)(w.x >> FP_FBITS) : 0;
+  c.uI = ok ? (int)(w.y >> FP_FBITS) : 0;
+  c.x = frac21(w.x);
+  c.y = frac21(w.y);
+  return c;
+}
+
+// 4x4 gather from a shared window row-pitched DW_COLS (immediate offsets)
+template <typename T>
+__device__ __forceinline__ T eval_window(const T *p, T x, T y) {
+  const T b2xI = bv2<T>(T(1) - x), b1xI = bv1<T>(T(1) - x);
+  const T b1x = bv1<T>(x), b2x = bv2<T>(x);
+  const T s0 = p[0] * b2xI + p[1] * b1xI + p[2] * b1x + p[3] * b2x;
+  const T s1 = p[DW_COLS] * b2xI + p[DW_COLS + 1] * b1xI + p[DW_COLS + 2] * b1x +
+               p[DW_COLS + 3] * b2x;
+  const T s2 = p[2 * DW_COLS] * b2xI + p[2 * DW_COLS + 1] * b1xI +
+               p[2 * DW_COLS + 2] * b1x + p[2 * DW_COLS + 3] * b2x;
+  const T s3 = p[3 * DW_COLS] * b2xI + p[3 * DW_COLS + 1] * b1xI +
+               p[3 * DW_COLS + 2] * b1x + p[3 * DW_COLS + 3] * b2x;
+  return (T(1) / T(36)) * (bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
+                           bv1<T>(y) * s2 + bv2<T>(y) * s3);
+}
+template <>
+__device__ __forceinline__ float eval_window<float>(const float *p, float x, float y) {
+  const float2 t = f2(x, y);
+  const float2 one = f2(1.f, 1.f), three = f2(3.f, 3.f), m3 = f2(-3.f, -3.f);
+  const float2 sv = __fadd2_rn(one, f2(-t.x, -t.y));
+  const float2 t2 = __fmul2_rn(t, t), t3 = __fmul2_rn(t2, t);
+  const float2 s2 = __fmul2_rn(sv, sv), s3 = __fmul2_rn(s2, sv);
+  const float2 a1 = __ffma2_rn(m3, s3, __ffma2_rn(three, s2, __ffma2_rn(three, sv, one)));
+  const float2 b1 = __ffma2_rn(m3, t3, __ffma2_rn(three, t2, __ffma2_rn(three, t, one)));
+  const float2 wx0 = f2(s3.x, s3.x), wx1 = f2(a1.x, a1.x), wx2 = f2(b1.x, b1.x),
+               wx3 = f2(t3.x, t3.x);
+  float2 r01 = __fmul2_rn(f2(p[0], p[DW_COLS]), wx0);
+  r01 = __ffma2_rn(f2(p[1], p[DW_COLS + 1]), wx1, r01);
+  r01 = __ffma2_rn(f2(p[2], p[DW_COLS + 2]), wx2, r01);
+  r01 = __ffma2_rn(f2(p[3], p[DW_COLS + 3]), wx3, r01);
+  const float *q = p + 2 * DW_COLS;
+  float2 r23 = __fmul2_rn(f2(q[0], q[DW_COLS]), wx0);
+  r23 = __ffma2_rn(f2(q[1], q[DW_COLS + 1]), wx1, r23);
+  r23 = __ffma2_rn(f2(q[2], q[DW_COLS + 2]), wx2, r23);
+  r23 = __ffma2_rn(f2(q[3], q[DW_COLS + 3]), wx3, r23);
+  const float2 acc = __ffma2_rn(r23, f2(b1.y, t3.y), __fmul2_rn(r01, f2(s3.y, a1.y)));
+  return (acc.x + acc.y) * (1.f / 36.f);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DT_THREADS)
+    drift_tma_kernel(const __grid_constant__ CUtensorMap tmC, const T *__restrict__ C,
+                     T *__restrict__ f, const int32_t *__restrict__ idx,
+                     const T *__restrict__ fx, const T *__restrict__ fy,
+                     const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
+                     const int32_t *__restrict__ ch_len, const T *__restrict__ ch_val,
+                     int64_t ndrift, MomentTables mt, double *__restrict__ partial,
+                     unsigned int *err, Geometry g) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T *win = reinterpret_cast<T *>(smem_raw);  // two windows
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + 2 * DW_COLS * DW_ROWS * sizeof(T));
+  __shared__ double red[DT_THREADS / 32][32];
+  constexpr uint32_t BYTES = DW_COLS * DW_ROWS * sizeof(T);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int r0 = blockIdx.x * 32, r = r0 + lane, j = blockIdx.y;
+  const int nch = (g.nu + DW_CH - 1) / DW_CH;
+  const int x0 = r0 - DW_XOFF;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+    for (int c = 0; c < 2 && c < nch; ++c) {
+      mbar_expect_tx(&bar[c], BYTES);
+      tma_load_3d(win + c * DW_COLS * DW_ROWS, &tmC, x0, c * DW_CH - DW_YOFF, j, &bar[c]);
+    }
+  }
+  __syncthreads();
+  const T *Cj = C + (size_t)j * (g.nu + 3) * g.pc;
+  const size_t row0 = (size_t)j * g.nu * g.nr + r;
+  const bool col_ok = r < g.nr;
+  Cell<T> nxt[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int u = w + 8 * q;
+    nxt[q] = load_cell(idx, fx, fy, fp2, row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
+  }
+  double acc = 0.0;
+  // copy bookkeeping (meaningful in thread 0, which issues every copy): the
+  // chunk last sent to each buffer and whether its completion was observed
+  int last[2] = {0, 1};
+  bool pending[2] = {true, nch > 1};
+  bool issuing = true;
+  for (int c = 0; c < nch; ++c) {
+    Cell<T> cur[2] = {nxt[0], nxt[1]};
+    if (c + 1 < nch) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int u = (c + 1) * DW_CH + w + 8 * q;
+        nxt[q] = load_cell(idx, fx, fy, fp2,
+                           row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
+      }
+    }
+    const int b = c & 1;
+    // after one failed wait this thread waits no more (it reads C globally)
+    const bool have = issuing && mbar_wait_bounded(&bar[b], (uint32_t)((c >> 1) & 1));
+    if (have) pending[b] = false;
+    if (!have && issuing) {
+      issuing = false;  // never stack a second copy onto an unfinished one
+      atomicOr(err, 1u);
+    }
+    const T *wb = win + b * DW_COLS * DW_ROWS;
+    const int y0 = c * DW_CH - DW_YOFF;
+    T part = T(0);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int u = c * DW_CH + w + 8 * q;
+      if (u < g.nu && col_ok) {
+        const Cell<T> &cl = cur[q];
+        T v = T(0);
+        if (cl.kind == 0) {
+          const int wr = cl.uI - y0, wc = cl.rI - x0;
+          if (have && wr >= 0 && wr <= DW_ROWS - 4 && wc >= 0 && wc <= DW_COLS - 4)
+            v = eval_window<T>(wb + wr * DW_COLS + wc, cl.x, cl.y);
+          else
+            v = eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
+        } else if (cl.kind == 2) {
+          const int L = __ldg(ch_len + cl.ch);
+          v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
+        }
+        f[row0 + (size_t)u * g.nr] = v;
+        part += (T)__ldg(mt.bu + u) * v;
+      }
+    }
+    acc += (double)part;
+    __syncthreads();  // every warp is done with window b
+    if (tid == 0 && issuing && c + 2 < nch) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[b], BYTES);
+      tma_load_3d(win + b * DW_COLS * DW_ROWS, &tmC, x0, (c + 2) * DW_CH - DW_YOFF, j,
+                  &bar[b]);
+      last[b] = c + 2;
+      pending[b] = true;
+    }
+  }
+  // a copy whose wait timed out may still be in flight: wait for it (bounded)
+  // before the block's shared memory is released
+  if (tid == 0) {
+    for (int b = 0; b < 2; ++b)
+      if (pending[b] && last[b] < nch &&
+          !mbar_wait_bounded(&bar[b], (uint32_t)((last[b] >> 1) & 1)))
+        atomicOr(err, 2u);
+  }
+  red[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && col_ok) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < DT_THREADS / 32; ++k) s += red[k][lane];
+    partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * s;
+  }
+}
+
+template <typename T>
+cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int32_t *idx,
+                             const T *fx, const T *fy, const uint2 *fp2,
+                             const int64_t *ch_start, const int32_t *ch_len,
+                             const T *ch_val, int64_t ndrift, const MomentTables &mt,
+                             double *partial, unsigned int *err, const Geometry &g,
+                             cudaStream_t st) {
+  const size_t smem = 2 * DW_COLS * DW_ROWS * sizeof(T) + 2 * sizeof(uint64_t);
+  cudaError_t e = cudaFuncSetAttribute(drift_tma_kernel<T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((g.nr + 31) / 32, g.nj);
+  drift_tma_kernel<T><<<grid, DT_THREADS, smem, st>>>(*tmC, C, f, idx, fx, fy, fp2, ch_start,
+                                                       ch_len, ch_val, ndrift, mt, partial,
+                                                       err, g);
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
                          const T *fy, const uint2 *fp2, const int64_t *ch_start,
@@ -621,7 +936,7 @@ cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
                          int64_t ndrift, const MomentTables &mt, double *partial,
                          const Geometry &g, cudaStream_t st) {
   dim3 grid((g.nr + 31) / 32, g.nj);
-  constexpr int CELLS = sizeof(T) == 4 ? 4 : 2;
+  constexpr int CELLS = 2;
   drift_kernel<T, CELLS><<<grid, 32 * DR_W, 0, st>>>(C, f, idx, fx, fy, fp2, ch_start,
                                                       ch_len, ch_val, ndrift, mt,
                                                       partial, g);
@@ -941,6 +1256,11 @@ cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
 }
 
 #define VLS_INST(T)                                                            \
+  template cudaError_t launch_drift_tma<T>(                                     \
+      const CUtensorMap *, const T *, T *, const int32_t *, const T *, const T *, \
+      const uint2 *, const int64_t *, const int32_t *, const T *, int64_t,        \
+      const MomentTables &, double *, unsigned int *, const Geometry &,          \
+      cudaStream_t);                                                            \
   template cudaError_t launch_drift<T>(                                         \
       const T *, T *, const int32_t *, const T *, const T *, const uint2 *,      \
       const int64_t *, const int32_t *, const T *, int64_t,                     \

@@ -128,6 +128,18 @@ HostDirTables thomas_tables(int dim, double hi) {
   }
   t.L1 = -2.0 * t.hi2 - t.hi2 * t.q[M - 3];
   t.L2 = t.hi2 - t.L1 * t.q[M - 2];
+  // the forward coefficients converge (geometrically, ratio 0.268) to the
+  // fixed point of p = 4/6 - q/6, q = (1/6)/p; from row kc on they are
+  // constant in the given precision, so the solve can drop the table there
+  t.rp_inf = t.rp[M - 2];
+  t.q_inf = t.q[M - 2];
+  t.kc64 = M - 1;
+  while (t.kc64 > 2 && t.rp[t.kc64 - 1] == t.rp_inf && t.q[t.kc64 - 1] == t.q_inf)
+    t.kc64--;
+  t.kc32 = M - 1;
+  while (t.kc32 > 2 && (float)t.rp[t.kc32 - 1] == (float)t.rp_inf &&
+         (float)t.q[t.kc32 - 1] == (float)t.q_inf)
+    t.kc32--;
   return t;
 }
 

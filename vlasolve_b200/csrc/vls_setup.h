@@ -34,6 +34,8 @@ struct HostDirTables {
   std::vector<double> rp, q;
   double a01, a02, hi2, L1, L2;
   int M;
+  int kc64, kc32;  // first row of the constant-coefficient interior
+  double rp_inf, q_inf;
 };
 HostDirTables thomas_tables(int dim, double hi);
 
