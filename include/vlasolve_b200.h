@@ -201,6 +201,30 @@ int vls_write_ndfield(vls_handle *h, const char *path);
    vls_write_ndfield into f (dims and datatype are checked) */
 int vls_read_ndfield(vls_handle *h, const char *path);
 
+/* Radial moment of a grid that already lives in device memory, without any
+   allocation (no counterpart in the reference, whose grid is host memory).
+   For callers that own all device memory and must not let a library call
+   cudaMalloc (an application with its own memory pool or a fixed budget
+   reserved at start-up): the grid f_dev ([j][u][r], double for VLS_FP64,
+   float otherwise) and the outputs bins_dev, Mr_dev (N_r doubles each) and
+   mtot_dev (one double) are the caller's device buffers; the coordinates R
+   (N_r), U (N_u), J (N_J), JV (N_J+1) are host arrays, as vls_coords returns
+   them.  Results are those of vls_moments for the same grid.  Work is queued
+   on `stream` (a cudaStream_t, NULL for the legacy default stream) of
+   `device`.  Working space is a fixed 512 KiB device array inside the
+   library: grids above 2048 r vertices, 2048 u vertices or 2048 J cells are
+   rejected with VLS_EINVAL.  That array is shared by every call, so calls that
+   overlap on the GPU race and must be serialised by the caller; the first
+   call on a device looks up the array's device address with that device
+   current, so it should come before any stream capture on that device.
+   Errors are reported by vls_noalloc_last_error(). */
+int vls_radial_mass_noalloc(const void *f_dev, int32_t precision, int64_t nr,
+                            int64_t nu, int64_t nj, const double *R,
+                            const double *U, const double *J, const double *JV,
+                            double *bins_dev, double *Mr_dev, double *mtot_dev,
+                            void *stream, int32_t device);
+const char *vls_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in header_functions() if not hasattr(L, n)]
     assert not missing, missing
     # and the Python binding declares exactly the header's entry points
-    assert sorted(set(_lib.EXPORTED) | {"vls_last_error"}) == header_functions()
+    assert sorted(set(_lib.EXPORTED)) == header_functions()
 
 
 def test_library_is_sm100a_only():

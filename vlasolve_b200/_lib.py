@@ -28,7 +28,7 @@ EXPORTED = [
     "vls_set_chain_values", "vls_step", "vls_sync", "vls_kernel_launches",
     "vls_moments", "vls_last_mass", "vls_stats", "vls_get_time", "vls_set_time",
     "vls_write_ndfield", "vls_read_ndfield", "vls_stream", "vls_set_profiling",
-    "vls_profile_read",
+    "vls_profile_read", "vls_radial_mass_noalloc", "vls_noalloc_last_error",
 ]
 KERNEL_KINDS = ["ucol_kick", "ucol", "prer", "tails", "drift", "scan", "moment",
                 "stats", "convert"]
@@ -114,6 +114,9 @@ def load(path: str = LIB_PATH):
         "vls_stream": [H, P(ctypes.c_void_p)],
         "vls_set_profiling": [H, i32],
         "vls_profile_read": [H, P(d), P(i64), i32],
+        "vls_radial_mass_noalloc": [ctypes.c_void_p, i32, i64, i64, i64, P(d), P(d), P(d),
+                                    P(d), ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, i32],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -121,6 +124,8 @@ def load(path: str = LIB_PATH):
         fn.restype = ctypes.c_int
     L.vls_last_error.argtypes = [H]
     L.vls_last_error.restype = ctypes.c_char_p
+    L.vls_noalloc_last_error.argtypes = []
+    L.vls_noalloc_last_error.restype = ctypes.c_char_p
     _lib = L
     return L
 
