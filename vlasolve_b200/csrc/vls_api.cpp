@@ -65,8 +65,14 @@ struct vls_handle {
   double time = 0;
   int64_t step = 0;
   int64_t launches = 0;
-  // TMA descriptor of C for the drift's staged coefficient windows
-  CUtensorMap tmC{};
+  // slice batches: batch b covers slices [b*B, b*B+B) and runs on batch
+  // stream b mod NS with its own ring slot of G and C scratch
+  int B = 1, nbatch = 1, NS = 1;
+  cudaStream_t bst[8] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[8] = {};
+  std::vector<int64_t> chain_lo;  // first chain of slice j (size nj + 1)
+  // TMA descriptors of each slot of C for the drift's staged windows
+  CUtensorMap tmC[8];
   bool have_tma = false;
   // opt-in per-kernel event timing
   bool profiling = false;
@@ -132,8 +138,9 @@ static Geometry geometry(const vls_handle *h) {
   g.nu = h->co.nu;
   g.nj = h->co.nj;
   g.pc = h->pc;
+  g.j0 = 0;
+  g.nb = h->co.nj;
   g.U = h->dU_val;
-  g.Rsq = nullptr;
   g.u0 = h->co.U.front();
   g.umax = h->co.U.back();
   g.su = h->co.sstart[1];
@@ -181,17 +188,18 @@ static cudaEvent_t take_event(vls_handle *h) {
 
 // Runs one launch; counts it and, with profiling on, brackets it with events.
 template <typename F>
-static cudaError_t timed(vls_handle *h, int kind, F &&launch) {
+static cudaError_t timed(vls_handle *h, int kind, F &&launch, cudaStream_t st = nullptr) {
+  if (!st) st = h->st;
   cudaEvent_t a = nullptr, b = nullptr;
   if (h->profiling) {
     a = take_event(h);
     b = take_event(h);
-    cudaEventRecord(a, h->st);
+    cudaEventRecord(a, st);
   }
   const cudaError_t e = launch();
   h->launches++;
   if (h->profiling) {
-    cudaEventRecord(b, h->st);
+    cudaEventRecord(b, st);
     h->prof.push_back({kind, a, b});
   }
   return e;
@@ -326,6 +334,10 @@ static int setup_chain_device(vls_handle *h) {
     acc += h->ch_len_h[k];
   }
   h->nel = acc;
+  h->chain_lo.assign(c.nj + 1, nch);
+  for (int64_t k = nch - 1; k >= 0; k--)
+    h->chain_lo[h->ch_cell_h[k] / ((int64_t)c.nr * c.nu)] = k;
+  for (int j = c.nj - 1; j >= 0; j--) h->chain_lo[j] = std::min(h->chain_lo[j], h->chain_lo[j + 1]);
   std::vector<int32_t> tcode(2 * std::max<int64_t>(nch, 1), 0);
   std::vector<double> tx(std::max<int64_t>(nch, 1), 0), ty(std::max<int64_t>(nch, 1), 0);
   for (int64_t k = 0; k < nch; k++) {
@@ -385,18 +397,24 @@ static bool make_tensor_map(vls_handle *h) {
   }
   auto enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   const cuuint64_t es = h->esize;
-  const cuuint64_t dims[3] = {(cuuint64_t)h->pc, (cuuint64_t)h->co.nu + 3,
-                              (cuuint64_t)h->co.nj};
-  const cuuint64_t strides[2] = {(cuuint64_t)h->pc * es,
-                                 (cuuint64_t)h->pc * es * (cuuint64_t)(h->co.nu + 3)};
-  const cuuint32_t box[3] = {64, 40, 1};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = enc(&h->tmC,
-                         es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                         3, h->C, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS;
+  const size_t slot = (size_t)h->B * (h->co.nu + 3) * h->pc;  // elements per slot
+  for (int s = 0; s < h->NS; s++) {
+    const cuuint64_t dims[3] = {(cuuint64_t)h->pc, (cuuint64_t)h->co.nu + 3,
+                                (cuuint64_t)h->B};
+    const cuuint64_t strides[2] = {(cuuint64_t)h->pc * es,
+                                   (cuuint64_t)h->pc * es * (cuuint64_t)(h->co.nu + 3)};
+    const cuuint32_t box[3] = {64, 40, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    void *base = (char *)h->C + s * slot * es;
+    const CUresult r = enc(&h->tmC[s],
+                           es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                           3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+  }
+  return true;
 }
 
 // ------------------------------------------------------------- life cycle
@@ -432,6 +450,14 @@ static void free_all(vls_handle *h) {
   h->evpool.clear();
   for (void *p : h->allocs) cudaFree(p);
   h->allocs.clear();
+  for (int k = 0; k < 8; k++) {
+    if (h->bst[k]) cudaStreamDestroy(h->bst[k]);
+    if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
+    h->bst[k] = nullptr;
+    h->ev_join[k] = nullptr;
+  }
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  h->ev_fork = nullptr;
   if (h->st) cudaStreamDestroy(h->st);
   h->st = nullptr;
 }
@@ -481,9 +507,27 @@ extern "C" int vls_create(const vls_grid_desc *grid,
     if (s == VLS_OK) s = st;
   };
   const size_t es = h->esize, cells = h->cells;
+  {
+    // slice batching (VLS_BATCH slices per batch, VLS_STREAMS streams);
+    // default: one batch of every slice
+    const char *eb = std::getenv("VLS_BATCH");
+    const char *es_ = std::getenv("VLS_STREAMS");
+    h->B = eb ? std::max(1, std::min(c.nj, std::atoi(eb))) : c.nj;
+    h->nbatch = (c.nj + h->B - 1) / h->B;
+    h->NS = es_ ? std::max(1, std::min(8, std::atoi(es_))) : 1;
+    h->NS = std::min(h->NS, h->nbatch);
+    for (int k = 0; k < h->NS; k++)
+      if (cudaStreamCreateWithFlags(&h->bst[k], cudaStreamNonBlocking) != cudaSuccess)
+        return fail(nullptr, VLS_ECUDA, "cudaStreamCreate failed");
+    if (cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess)
+      return fail(nullptr, VLS_ECUDA, "cudaEventCreate failed");
+    for (int k = 0; k < h->NS; k++)
+      if (cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming) != cudaSuccess)
+        return fail(nullptr, VLS_ECUDA, "cudaEventCreate failed");
+  }
   A(dalloc(hp, &h->f, es * cells));
-  A(dalloc(hp, &h->G, es * (size_t)c.nj * (c.nu + 2) * c.nr));
-  A(dalloc(hp, &h->C, es * (size_t)c.nj * (c.nu + 3) * h->pc));
+  A(dalloc(hp, &h->G, es * (size_t)h->NS * h->B * (c.nu + 2) * c.nr));
+  A(dalloc(hp, &h->C, es * (size_t)h->NS * h->B * (c.nu + 3) * h->pc));
   if (h->prec == VLS_FP64) {
     A(dalloc(hp, &h->idx, sizeof(int32_t) * cells));
     A(dalloc(hp, &h->fx, es * cells));
@@ -529,7 +573,7 @@ extern "C" int vls_create(const vls_grid_desc *grid,
     }
     return st;
   };
-  if (cudaMemsetAsync(h->C, 0, es * (size_t)c.nj * (c.nu + 3) * h->pc, h->st) !=
+  if (cudaMemsetAsync(h->C, 0, es * (size_t)h->NS * h->B * (c.nu + 3) * h->pc, h->st) !=
           cudaSuccess ||
       cudaMemsetAsync(h->count, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess ||
       cudaMemsetAsync(h->flag, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess)
@@ -857,35 +901,58 @@ extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
 // ------------------------------------------------------------------ step
 template <typename T, typename R>
 static int drift_once(vls_handle *h, bool kick) {
-  const Geometry g = geometry(h);
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
   const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
-  CK(h, timed(h, kick ? VLS_K_UCOL_KICK : VLS_K_UCOL, [&] {
-       return launch_ucol<T, R>(kick, (const T *)h->f, (T *)h->G, h->shift, g, tu,
-                                h->st);
-     }));
-  CK(h, timed(h, VLS_K_PRER, [&] {
-       return launch_prer<T, R>((const T *)h->G, (T *)h->C, g, tr, h->st);
-     }));
-  if (h->nch) {
-    CK(h, timed(h, VLS_K_TAILS, [&] {
-         return launch_chain_tails<T>((const T *)h->C, (T *)h->ch_val, h->ch_start,
-                                      h->ch_len, h->t_idx, h->t_x, h->t_y, h->nch,
-                                      h->ndrift, g, h->st);
-       }));
+  const size_t gslot = (size_t)h->B * (h->co.nu + 2) * h->co.nr;
+  const size_t cslot = (size_t)h->B * (h->co.nu + 3) * h->pc;
+  CK(h, cudaEventRecord(h->ev_fork, h->st));
+  for (int k = 0; k < h->NS; k++) CK(h, cudaStreamWaitEvent(h->bst[k], h->ev_fork, 0));
+  for (int b = 0; b < h->nbatch; b++) {
+    const int sl = b % h->NS;
+    cudaStream_t bs = h->bst[sl];
+    Geometry g = geometry(h);
+    g.j0 = b * h->B;
+    g.nb = std::min(h->B, h->co.nj - g.j0);
+    T *G = (T *)h->G + sl * gslot;
+    T *C = (T *)h->C + sl * cslot;
+    CK(h, timed(
+              h, kick ? VLS_K_UCOL_KICK : VLS_K_UCOL,
+              [&] {
+                return launch_ucol<T, R>(kick, (const T *)h->f, G, h->shift, g, tu, bs);
+              },
+              bs));
+    CK(h, timed(h, VLS_K_PRER, [&] { return launch_prer<T, R>(G, C, g, tr, bs); }, bs));
+    const int64_t c_lo = h->chain_lo[g.j0], c_hi = h->chain_lo[g.j0 + g.nb];
+    if (c_hi > c_lo) {
+      CK(h, timed(
+                h, VLS_K_TAILS,
+                [&] {
+                  return launch_chain_tails<T>(C, (T *)h->ch_val, h->ch_start, h->ch_len,
+                                               h->t_idx, h->t_x, h->t_y, h->nch, c_lo,
+                                               c_hi, h->ndrift, g, bs);
+                },
+                bs));
+    }
+    CK(h, timed(
+              h, VLS_K_DRIFT,
+              [&] {
+                if (h->have_tma)
+                  return launch_drift_tma<T>(&h->tmC[sl], C, (T *)h->f, h->idx,
+                                             (const T *)h->fx, (const T *)h->fy, h->fp2,
+                                             h->ch_start, h->ch_len, (const T *)h->ch_val,
+                                             h->ndrift, moment_tables(h), h->partial,
+                                             h->flag + 1, g, bs);
+                return launch_drift<T>(C, (T *)h->f, h->idx, (const T *)h->fx,
+                                       (const T *)h->fy, h->fp2, h->ch_start, h->ch_len,
+                                       (const T *)h->ch_val, h->ndrift, moment_tables(h),
+                                       h->partial, g, bs);
+              },
+              bs));
   }
-  CK(h, timed(h, VLS_K_DRIFT, [&] {
-       if (h->have_tma)
-         return launch_drift_tma<T>(&h->tmC, (const T *)h->C, (T *)h->f, h->idx,
-                                    (const T *)h->fx, (const T *)h->fy, h->fp2,
-                                    h->ch_start, h->ch_len, (const T *)h->ch_val,
-                                    h->ndrift, moment_tables(h), h->partial,
-                                    h->flag + 1, g, h->st);
-       return launch_drift<T>((const T *)h->C, (T *)h->f, h->idx, (const T *)h->fx,
-                              (const T *)h->fy, h->fp2, h->ch_start, h->ch_len,
-                              (const T *)h->ch_val, h->ndrift, moment_tables(h),
-                              h->partial, g, h->st);
-     }));
+  for (int k = 0; k < h->NS; k++) {
+    CK(h, cudaEventRecord(h->ev_join[k], h->bst[k]));
+    CK(h, cudaStreamWaitEvent(h->st, h->ev_join[k], 0));
+  }
   h->ndrift++;
   h->moments_valid = true;
   return VLS_OK;

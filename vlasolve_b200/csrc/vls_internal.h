@@ -2,9 +2,10 @@
 //
 // Device layout (HBM), one GPU holds everything:
 //   f      [N_J][N_u][N_r]          T (float or double), r fastest
-//   G      [N_J][N_u+2][N_r]        T: u-direction spline coefficients of the
-//                                     kicked f (rows 0 and N_u+1 are ghosts)
-//   C      [N_J][N_u+3][Pc]         T: 2D coefficients, Pc >= N_r+3; row N_u+2
+//   G      [slot][B][N_u+2][N_r]    T: u-direction spline coefficients of the
+//                                     kicked f (rows 0 and N_u+1 are ghosts),
+//                                     for a batch of B slices per ring slot
+//   C      [slot][B][N_u+3][Pc]     T: 2D coefficients, Pc >= N_r+3; row N_u+2
 //                                     and columns >= N_r+2 stay zero (reads
 //                                     at index N exist for footpoints that
 //                                     land on the last vertex with weight 0)
@@ -42,8 +43,10 @@ struct DirTables {
 struct Geometry {
   int nr, nu, nj;
   int pc;  // row pitch of C
+  // slices [j0, j0 + nb) are processed by this launch (grid.y = nb); the
+  // scratch arrays G and C hold only those slices (local index j - j0)
+  int j0, nb;
   const double *U;      // U_Val (nu)
-  const double *Rsq;    // unused placeholder for alignment of future data
   double u0, umax;      // U_Val.front(), U_Val.back()
   double su, hu;        // spline start / step_inv of u (rescaled, linear)
 };
@@ -79,12 +82,13 @@ cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int
                              const T *ch_val, int64_t ndrift, const MomentTables &mt,
                              double *partial, unsigned int *err, const Geometry &g,
                              cudaStream_t st);
+// chains [c_lo, c_hi) (all of the launch's slices) of nchains in total
 template <typename T>
 cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
                                const int32_t *ch_len, const int32_t *t_idx,
                                const double *t_x, const double *t_y,
-                               int64_t nchains, int64_t ndrift,
-                               const Geometry &g, cudaStream_t st);
+                               int64_t nchains, int64_t c_lo, int64_t c_hi,
+                               int64_t ndrift, const Geometry &g, cudaStream_t st);
 template <typename T>
 cudaError_t launch_moment(const T *f, const MomentTables &mt, double *partial,
                           const Geometry &g, cudaStream_t st);

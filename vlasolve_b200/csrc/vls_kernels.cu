@@ -280,7 +280,8 @@ __global__ void __launch_bounds__(UC_THREADS)
   const int col = tid % TW;
   const int seg = tid / TW;
   const int r0 = blockIdx.x * TW;
-  const int j = blockIdx.y;
+  const int jl = blockIdx.y;        // slice within the batch (scratch index)
+  const int j = g.j0 + jl;          // global slice
   const int r = r0 + col;
 
   load_tables<R>(rp, qq, tu);
@@ -337,7 +338,7 @@ __global__ void __launch_bounds__(UC_THREADS)
     solve_lines<Prec<T>::K, R>(bufB + col, TW, k0, k1, tu, rp, qq);
     out = bufB;
   }
-  T *Gs = G + (size_t)j * M * g.nr;
+  T *Gs = G + (size_t)jl * M * g.nr;
   for (int e = tid; e < M * TW; e += UC_THREADS) {
     const int k = e / TW, c = e % TW;
     const int rr = r0 + c;
@@ -351,7 +352,7 @@ cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
   constexpr int TW = UcolCfg<R>::TW;
   const size_t smem =
       align16(2 * (size_t)(g.nu + 2) * sizeof(R)) + 2 * (size_t)(g.nu + 3) * TW * sizeof(R);
-  dim3 grid((g.nr + TW - 1) / TW, g.nj);
+  dim3 grid((g.nr + TW - 1) / TW, g.nb);
   cudaError_t e;
   if (kick) {
     e = cudaFuncSetAttribute(ucol_kernel<T, R, true>,
@@ -403,7 +404,7 @@ __global__ void __launch_bounds__(PrerCfg<R>::THREADS)
   const int tid = threadIdx.x;
   const int rho = tid % ROWS;
   const int seg = tid / ROWS;
-  const int j = blockIdx.y;
+  const int j = blockIdx.y;  // slice within the batch (G and C are batch scratch)
   const int kr0 = blockIdx.x * ROWS;
   const int nrows = g.nu + 2;
   const T *Gs = G + (size_t)j * nrows * g.nr;
@@ -445,7 +446,7 @@ cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr
   const int M = g.nr + 2;
   const size_t smem = align16(2 * (size_t)M * sizeof(R)) +
                       (size_t)ROWS * prer_pitch(M, sizeof(R)) * sizeof(R);
-  dim3 grid((g.nu + 2 + ROWS - 1) / ROWS, g.nj);
+  dim3 grid((g.nu + 2 + ROWS - 1) / ROWS, g.nb);
   cudaError_t e = cudaFuncSetAttribute(
       prer_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -606,8 +607,8 @@ __global__ void __launch_bounds__(32 * DR_W, 4)
                  double *__restrict__ partial, Geometry g) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int r = blockIdx.x * 32 + lane;
-  const int j = blockIdx.y;
-  const T *Cj = C + (size_t)j * (g.nu + 3) * g.pc;
+  const int j = g.j0 + blockIdx.y;
+  const T *Cj = C + (size_t)blockIdx.y * (g.nu + 3) * g.pc;
   // each warp walks a contiguous band of u rows: consecutive rows have
   // neighbouring footpoints, so their 4x4 patches overlap in L1
   const int band = (g.nu + DR_W - 1) / DR_W;
@@ -813,7 +814,8 @@ __global__ void __launch_bounds__(DT_THREADS)
   __shared__ double red[DT_THREADS / 32][32];
   constexpr uint32_t BYTES = DW_COLS * DW_ROWS * sizeof(T);
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int r0 = blockIdx.x * 32, r = r0 + lane, j = blockIdx.y;
+  const int r0 = blockIdx.x * 32, r = r0 + lane;
+  const int jl = blockIdx.y, j = g.j0 + jl;  // batch-local / global slice
   const int nch = (g.nu + DW_CH - 1) / DW_CH;
   const int x0 = r0 - DW_XOFF;
   if (tid == 0) {
@@ -822,11 +824,11 @@ __global__ void __launch_bounds__(DT_THREADS)
     mbar_fence_init();
     for (int c = 0; c < 2 && c < nch; ++c) {
       mbar_expect_tx(&bar[c], BYTES);
-      tma_load_3d(win + c * DW_COLS * DW_ROWS, &tmC, x0, c * DW_CH - DW_YOFF, j, &bar[c]);
+      tma_load_3d(win + c * DW_COLS * DW_ROWS, &tmC, x0, c * DW_CH - DW_YOFF, jl, &bar[c]);
     }
   }
   __syncthreads();
-  const T *Cj = C + (size_t)j * (g.nu + 3) * g.pc;
+  const T *Cj = C + (size_t)jl * (g.nu + 3) * g.pc;
   const size_t row0 = (size_t)j * g.nu * g.nr + r;
   const bool col_ok = r < g.nr;
   Cell<T> nxt[2];
@@ -887,7 +889,7 @@ __global__ void __launch_bounds__(DT_THREADS)
     if (tid == 0 && issuing && c + 2 < nch) {
       fence_proxy_async();
       mbar_expect_tx(&bar[b], BYTES);
-      tma_load_3d(win + b * DW_COLS * DW_ROWS, &tmC, x0, (c + 2) * DW_CH - DW_YOFF, j,
+      tma_load_3d(win + b * DW_COLS * DW_ROWS, &tmC, x0, (c + 2) * DW_CH - DW_YOFF, jl,
                   &bar[b]);
       last[b] = c + 2;
       pending[b] = true;
@@ -922,7 +924,7 @@ cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int
   cudaError_t e = cudaFuncSetAttribute(drift_tma_kernel<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((g.nr + 31) / 32, g.nj);
+  dim3 grid((g.nr + 31) / 32, g.nb);
   drift_tma_kernel<T><<<grid, DT_THREADS, smem, st>>>(*tmC, C, f, idx, fx, fy, fp2, ch_start,
                                                        ch_len, ch_val, ndrift, mt, partial,
                                                        err, g);
@@ -935,7 +937,7 @@ cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
                          const int32_t *ch_len, const T *ch_val,
                          int64_t ndrift, const MomentTables &mt, double *partial,
                          const Geometry &g, cudaStream_t st) {
-  dim3 grid((g.nr + 31) / 32, g.nj);
+  dim3 grid((g.nr + 31) / 32, g.nb);
   constexpr int CELLS = 2;
   drift_kernel<T, CELLS><<<grid, 32 * DR_W, 0, st>>>(C, f, idx, fx, fy, fp2, ch_start,
                                                       ch_len, ch_val, ndrift, mt,
@@ -952,15 +954,15 @@ __global__ void chain_tail_kernel(const T *__restrict__ C, T *__restrict__ ch_va
                                   const int32_t *__restrict__ t_idx,
                                   const double *__restrict__ t_x,
                                   const double *__restrict__ t_y,
-                                  const int32_t *__restrict__ t_j,
-                                  int64_t nchains, int64_t ndrift, Geometry g) {
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nchains) return;
+                                  const int32_t *__restrict__ t_j, int64_t c_lo,
+                                  int64_t c_hi, int64_t ndrift, Geometry g) {
+  const int64_t c = c_lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c_hi) return;
   const int L = ch_len[c];
   const int code = t_idx[c];
   T v = T(0);
   if (code >= 0) {
-    const T *Cj = C + (size_t)t_j[c] * (g.nu + 3) * g.pc;
+    const T *Cj = C + (size_t)(t_j[c] - g.j0) * (g.nu + 3) * g.pc;
     v = eval2d<T>(Cj, g.pc, code & 0xffff, (T)t_x[c], code >> 16, (T)t_y[c]);
   }
   ch_val[ch_start[c] + (ndrift + L - 1) % L] = v;
@@ -970,15 +972,15 @@ template <typename T>
 cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
                                const int32_t *ch_len, const int32_t *t_idx,
                                const double *t_x, const double *t_y,
-                               int64_t nchains, int64_t ndrift,
-                               const Geometry &g, cudaStream_t st) {
-  if (nchains == 0) return cudaSuccess;
+                               int64_t nchains, int64_t c_lo, int64_t c_hi,
+                               int64_t ndrift, const Geometry &g, cudaStream_t st) {
+  if (c_hi <= c_lo) return cudaSuccess;
   // t_j (slice of each chain) is stored right after t_idx
   const int32_t *t_j = t_idx + nchains;
   const int threads = 256;
-  const unsigned blocks = (unsigned)((nchains + threads - 1) / threads);
+  const unsigned blocks = (unsigned)((c_hi - c_lo + threads - 1) / threads);
   chain_tail_kernel<T><<<blocks, threads, 0, st>>>(C, ch_val, ch_start, ch_len, t_idx,
-                                                   t_x, t_y, t_j, nchains, ndrift, g);
+                                                   t_x, t_y, t_j, c_lo, c_hi, ndrift, g);
   return cudaGetLastError();
 }
 
@@ -1267,8 +1269,8 @@ cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
       const MomentTables &, double *, const Geometry &, cudaStream_t);          \
   template cudaError_t launch_chain_tails<T>(                                   \
       const T *, T *, const int64_t *, const int32_t *, const int32_t *,         \
-      const double *, const double *, int64_t, int64_t, const Geometry &,       \
-      cudaStream_t);                                                            \
+      const double *, const double *, int64_t, int64_t, int64_t, int64_t,       \
+      const Geometry &, cudaStream_t);                                          \
   template cudaError_t launch_moment<T>(const T *, const MomentTables &,        \
                                         double *, const Geometry &,             \
                                         cudaStream_t);                          \
