@@ -1,0 +1,208 @@
+// vlasolve_b200.hpp -- C++ adapter over the C-ABI of vlasolve_b200.h that
+// keeps the surface of the reference's solver classes for the spherical path:
+// vlasovSolver (vlasovSolver.hxx:13-317), vlasovSolver21
+// (vlasovSolver21.hxx:19-783) and vlasovSolver21_spline
+// (vlasovSolver21_spline.hxx:16-943): construct from grid/solver/init
+// parameters, makeOneStep(t), statistics(), snapshot(), moments and the
+// coordinate accessors.  Header-only; link with libvlasolve_b200.so.
+//
+// Errors become vls::error exceptions carrying the VLS_* status (the
+// reference prints and exits instead).
+#ifndef VLASOLVE_B200_HPP
+#define VLASOLVE_B200_HPP
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "vlasolve_b200.h"
+
+namespace vls {
+
+class error : public std::runtime_error {
+ public:
+  error(int code, const std::string &msg) : std::runtime_error(msg), code_(code) {}
+  int code() const { return code_; }
+
+ private:
+  int code_;
+};
+
+inline void check(int rc, const vls_handle *h) {
+  if (rc != VLS_OK) throw error(rc, vls_last_error(h));
+}
+
+// Parameter blocks with the reference's defaults for the UDF profile
+// (initGen_UniformDensitySphere.hxx:82-112); fill them from the -group.param
+// options as the reference's gridHandler / vlasovSolver::init do.
+inline vls_grid_desc default_grid() {
+  vls_grid_desc g{};
+  g.Pmin = 0.01;
+  g.Pmax = 25;
+  g.Pres = 200;
+  g.Pscale = VLS_SCALE_LOG;
+  g.Umin[0] = -2.0;
+  g.Umin[1] = 0.0;
+  g.Umax[0] = 2.0;
+  g.Umax[1] = 1.6;
+  g.Ures[0] = 200;
+  g.Ures[1] = 200;
+  g.Uscale[0] = VLS_SCALE_LINEAR;
+  g.Uscale[1] = VLS_SCALE_QUADRATIC;
+  return g;
+}
+
+inline vls_solver_desc default_solver() {
+  vls_solver_desc s{};
+  s.G = 1;
+  s.T0 = 0;
+  s.Tmax = 60;
+  s.dt = 0.005;
+  s.noLinking = 0;
+  s.kernelType = VLS_KERNEL_DELAYED;
+  s.kernelBufferSize = 0;
+  s.precision = VLS_FP64;
+  s.device = 0;
+  return s;
+}
+
+inline vls_init_desc default_init() {
+  vls_init_desc i{};
+  i.type = VLS_INIT_UDF;
+  i.M = 1;
+  i.R0 = 2;
+  i.alpha = 0.5;
+  i.smoothingRadius = 0.5;
+  i.eta = 0.1;
+  i.n = 1;
+  i.Ra = -1;
+  i.R0_given = 1;
+  return i;
+}
+
+// The spherical split semi-Lagrangian solver on one GPU.
+class vlasovSolver21_spline {
+ public:
+  vlasovSolver21_spline(const vls_grid_desc &g, const vls_solver_desc &s,
+                        const vls_init_desc &init)
+      : solver_(s) {
+    check(vls_create(&g, &s, &h_), nullptr);
+    try {
+      check(vls_init_profile(h_, &init, &mass_before_), h_);
+      int64_t nr, nu, nj;
+      check(vls_dims(h_, &nr, &nu, &nj), h_);
+      nr_ = nr;
+      nu_ = nu;
+      nj_ = nj;
+    } catch (...) {
+      vls_destroy(h_);
+      throw;
+    }
+  }
+  ~vlasovSolver21_spline() { vls_destroy(h_); }
+  vlasovSolver21_spline(const vlasovSolver21_spline &) = delete;
+  vlasovSolver21_spline &operator=(const vlasovSolver21_spline &) = delete;
+
+  // vlasovSolver21_spline::makeOneStep (vlasovSolver21_spline.hxx:680-801)
+  void makeOneStep(double /*t*/) { check(vls_step(h_, 1), h_); }
+  void steps(int n) { check(vls_step(h_, n), h_); }
+  void sync() { check(vls_sync(h_), h_); }
+
+  // vlasovSolver::run (vlasovSolver.hxx:134-190) without restart dumps:
+  // statistics every statsEvery steps (row appended to `stats`), snapshots
+  // every snapshotEvery steps (snapshot_%4.4f.ND)
+  void run(long statsEvery, long snapshotEvery, const char *stats = "statistics.txt") {
+    auto timer = [](long every, long n) { return every >= 0 && (n % every) == 0; };
+    auto checkTime = [&]() {
+      double t;
+      int64_t st;
+      vls_get_time(h_, &t, &st);
+      return solver_.Tmax <= 0 ||
+             (t < solver_.Tmax && std::abs(t - solver_.Tmax) > solver_.dt / 100);
+    };
+    if (!checkTime()) return;
+    do {
+      double t;
+      int64_t n;
+      vls_get_time(h_, &t, &n);
+      if (timer(snapshotEvery, n)) snapshot();
+      if (timer(statsEvery, n)) statistics(n == 0, stats);
+      makeOneStep(t);
+    } while (checkTime());
+  }
+
+  // vlasovSolver21::statistics (vlasovSolver21.hxx:644-690)
+  vls_stats_out statistics(bool reset = false, const char *fname = "statistics.txt") {
+    vls_stats_out o;
+    check(vls_stats(h_, &o), h_);
+    if (fname) {
+      FILE *f = std::fopen(fname, reset ? "w" : "a");
+      if (!f) throw error(VLS_EIO, std::string("cannot open ") + fname);
+      if (reset) std::fprintf(f, "# Time Step Mass E Ek Ep S L1 L2\n");
+      std::fprintf(f, "%.10g %ld %10.10g %10.10g %10.10g %10.10g %10.10g %10.10g %10.10g\n",
+                   o.time, (long)o.step, o.Mass, o.E, o.Ek, o.Ep, o.S, o.L1, o.L2);
+      std::fclose(f);
+    }
+    return o;
+  }
+
+  // vlasovSolver21::snapshot (vlasovSolver21.hxx:585-598)
+  std::string snapshot(const char *name = nullptr) {
+    char buf[1024];
+    double t;
+    int64_t n;
+    vls_get_time(h_, &t, &n);
+    if (!name) {
+      std::snprintf(buf, sizeof(buf), "snapshot_%4.4f.ND", t);
+      name = buf;
+    }
+    check(vls_write_ndfield(h_, name), h_);
+    return name;
+  }
+
+  // quadrature21::integrate1D_acc (vlasovSolver21_spline.hxx:736)
+  double enclosedMass(std::vector<double> &bins, std::vector<double> &Mr) {
+    bins.resize(nr_);
+    Mr.resize(nr_);
+    double tot = 0;
+    check(vls_moments(h_, bins.data(), Mr.data(), &tot), h_);
+    return tot;
+  }
+
+  // gridBase::getDataPtr equivalents (host copies, [j][u][r])
+  std::vector<double> data() {
+    std::vector<double> f(nr_ * nu_ * nj_);
+    check(vls_get_f(h_, f.data(), f.size()), h_);
+    return f;
+  }
+  void setData(const std::vector<double> &f) { check(vls_set_f(h_, f.data(), f.size()), h_); }
+
+  // grid_21.hxx:150-158
+  std::vector<double> getValCoord21_R() const { return coord(0); }
+  std::vector<double> getValCoord21_U() const { return coord(1); }
+  std::vector<double> getValCoord21_J() const { return coord(2); }
+
+  double massBeforeRenormalisation() const { return mass_before_; }
+  size_t nr() const { return nr_; }
+  size_t nu() const { return nu_; }
+  size_t nj() const { return nj_; }
+  vls_handle *handle() { return h_; }
+
+ private:
+  std::vector<double> coord(int which) const {
+    std::vector<double> R(nr_), U(nu_), J(nj_), JV(nj_ + 1);
+    check(vls_coords(h_, R.data(), U.data(), J.data(), JV.data()), h_);
+    return which == 0 ? R : which == 1 ? U : J;
+  }
+  vls_handle *h_ = nullptr;
+  vls_solver_desc solver_;
+  double mass_before_ = 0;
+  size_t nr_ = 0, nu_ = 0, nj_ = 0;
+};
+
+}  // namespace vls
+
+#endif

@@ -57,3 +57,34 @@ def test_create_without_gpu_fails_loudly():
     rc = L.vls_create(ctypes.byref(g), ctypes.byref(s), ctypes.byref(h))
     assert rc == _lib.VLS_ECUDA
     assert b"CUDA" in L.vls_last_error(None) or b"device" in L.vls_last_error(None)
+
+
+def _driver():
+    from vlasolve_b200.build import DRIVER, build
+    build()
+    return DRIVER
+
+
+def test_driver_rejects_bad_options(tmp_path):
+    """The command-line driver parses the reference's -group.param options and
+    parameter files before touching the GPU."""
+    import subprocess
+    d = _driver()
+    r = subprocess.run([d, "-solver.kernelType", "foo"], cwd=tmp_path,
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "invalid kernel type" in r.stderr
+    r = subprocess.run([d, "missing.ini"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "could not read parameter file" in r.stderr
+    r = subprocess.run([d, "-init.type", "King"], cwd=tmp_path, capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and "unknown initial conditions" in r.stderr
+
+
+def test_driver_without_gpu_fails_loudly(tmp_path):
+    import subprocess
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    (tmp_path / "p.ini").write_text("init.type Plummer\ngrid.Pres 16\n")
+    r = subprocess.run([_driver(), "p.ini"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 2 and "device" in r.stderr

@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvlasolve_b200.so")
+DRIVER = os.path.join(HERE, "vlasolve_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["vls_kernels.cu", "vls_noalloc.cu", "vls_api.cpp", "vls_setup.cpp"]
@@ -33,7 +34,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(CSRC, s) for s in SOURCES]
     deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
     deps.append(os.path.join(REPO, "include", "vlasolve_b200.h"))
-    if not force and not _stale(LIB, deps):
+    deps.append(os.path.join(REPO, "include", "vlasolve_b200.hpp"))
+    deps.append(os.path.join(CSRC, "vls_main.cpp"))
+    if not force and not _stale(LIB, deps) and os.path.exists(DRIVER):
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -53,6 +56,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cmd = [NVCC, "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fopenmp",
                                                           "-lgomp", "-lcudart"]
     subprocess.check_call(cmd)
+    # command-line driver with the reference's options (links the library)
+    subprocess.check_call([
+        "g++", "-O2", "-std=c++17", "-I" + os.path.join(REPO, "include"),
+        os.path.join(CSRC, "vls_main.cpp"), "-L" + HERE, "-lvlasolve_b200",
+        "-Wl,-rpath,$ORIGIN", "-o", DRIVER])
     return LIB
 
 
