@@ -202,9 +202,16 @@ def gpu_arm(args):
         # timing only (used under ncu): no FP64 arm, statistics or end-to-end run
         s = VlasovSolver21Spline(w, precision=args.precision, device=local)
         ms, launches = time_steps(s, K, W, torch, dist)
+        out = {"workload": args.workload, "precision": args.precision,
+               "ms_per_step": ms / K, "launches": launches}
+        if args.kernels:
+            s.set_profiling(True)
+            s.step(min(K, 20))
+            prof = s.profile_read()
+            s.set_profiling(False)
+            out["kernels_ms_per_step"] = {k: v[0] / max(v[1], 1) for k, v in prof.items()}
         if rank == 0:
-            print(json.dumps({"workload": args.workload, "precision": args.precision,
-                              "ms_per_step": ms / K, "launches": launches}), flush=True)
+            print(json.dumps(out), flush=True)
         s.close()
         if dist is not None:
             dist.destroy_process_group()
@@ -360,6 +367,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-max-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels", action="store_true",
+                    help="with --quick: also report per-kernel event times")
     ap.add_argument("--quick", action="store_true",
                     help="timing of the chosen precision only (for profiler runs)")
     ap.add_argument("--workload", default=WORKLOAD_NAME, choices=sorted(WORKLOADS))

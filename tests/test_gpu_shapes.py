@@ -1,0 +1,72 @@
+"""Grid shapes that exercise the chunking of the register-resident prefilter
+(one chunk, a last chunk of one row, exactly full chunks, odd sizes) and the
+drift's strip boxes against the oracle, for every prefilter / drift layout
+and all three precisions."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.vls_oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+# (grid.Pres, grid.Ures[0]) -> N_r = Pres + 1 r vertices, N_u = Ures0 + 1 u
+# vertices; chunks of 31 rows: 4 -> 1 chunk, 32 -> 2 chunks with a last
+# chunk of one row, 62 -> 2 full chunks, 63 -> 3 chunks, 94 -> 4 chunks
+SHAPES = [(3, 31), (31, 32), (32, 61), (61, 62), (62, 93), (93, 3), (150, 40)]
+
+FP64_TOL = 1e-12
+FP32_L2 = 2e-6
+FP32_MAX = 1e-5
+
+
+def cfg_for(pres, ures0):
+    return {"type": "UDF", "Pmin": 0.01, "Pmax": 25.0, "Pres": pres,
+            "Pscale": "logarithmic", "Umin": (-2.0, 0.0), "Umax": (2.0, 1.6),
+            "Ures": (ures0, 6), "Uscale": ("linear", "quadratic"), "dt": 0.02}
+
+
+# environment of each implementation choice: the defaults, the shared-memory
+# segment prefilter with the windowed drift, each register chunk layout, and
+# each whole-strip drift layout
+IMPLS = {
+    "default": {},
+    "segment-window": {"VLS_PREFILTER": "segment", "VLS_DRIFT": "window"},
+    "rcA": {"VLS_RC": "A"},
+    "rcB": {"VLS_RC": "B"},
+    "rcC": {"VLS_RC": "C"},
+    "strip48": {"VLS_DRIFT": "48"},
+    "strip64": {"VLS_DRIFT": "64"},
+    "strip-48": {"VLS_DRIFT": "-48"},
+}
+
+
+@pytest.fixture(params=sorted(IMPLS))
+def impl(request, monkeypatch):
+    for k in ("VLS_PREFILTER", "VLS_DRIFT", "VLS_RC"):
+        monkeypatch.delenv(k, raising=False)
+    for k, v in IMPLS[request.param].items():
+        monkeypatch.setenv(k, v)
+    return request.param
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "%dx%d" % (s[0] + 1, s[1] + 1))
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32all"])
+def test_shape_steps_match_oracle(shape, precision, impl):
+    from vlasolve_b200 import VlasovSolver21Spline
+    cfg = cfg_for(*shape)
+    s = VlasovSolver21Spline(cfg, precision=precision)
+    o = Oracle(cfg)
+    for _ in range(3):
+        s.step(1)
+        o.step(1)
+        ref = o.f
+        got = s.f
+        scale = np.max(np.abs(ref))
+        if precision == "fp64":
+            assert np.max(np.abs(got - ref)) <= FP64_TOL * scale
+        else:
+            l2 = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+            assert l2 <= FP32_L2, l2
+            assert np.max(np.abs(got - ref)) <= FP32_MAX * scale

@@ -71,8 +71,17 @@ struct vls_handle {
   cudaStream_t bst[8] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[8] = {};
   std::vector<int64_t> chain_lo;  // first chain of slice j (size nj + 1)
-  // TMA descriptors of each slot of C for the drift's staged windows
+  // register-resident prefilter tables (per direction and recursion type)
+  // and whether its kernels take this grid; VLS_PREFILTER=segment selects
+  // the shared-memory segment kernels instead
+  RcDir<double> rcu_d{}, rcr_d{};
+  RcDir<float> rcu_f{}, rcr_f{};
+  int rcu_cfg = -1, rcr_cfg = -1;
+  // TMA descriptors of each slot of C for the drift's staged windows (tmC)
+  // and strips (tmS, when strip_w != 0: the strip layout in use)
   CUtensorMap tmC[8];
+  CUtensorMap tmS[8];
+  int strip_w = 0;
   bool have_tma = false;
   // opt-in per-kernel event timing
   bool profiling = false;
@@ -413,6 +422,15 @@ static bool make_tensor_map(vls_handle *h) {
                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
+    if (h->strip_w != 0) {
+      const cuuint32_t sbox[3] = {(cuuint32_t)std::abs(h->strip_w), 64, 1};
+      if (enc(&h->tmS[s],
+              es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+              base, dims, strides, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        h->strip_w = 0;
+    }
   }
   return true;
 }
@@ -496,6 +514,22 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   h->pc = ((c.nr + 3) + 3) / 4 * 4;
   h->tr = thomas_tables(c.nr, c.sstep_inv[0]);
   h->tu = thomas_tables(c.nu, c.sstep_inv[1]);
+  {
+    // prefilter kernels: register chunks (VLS_PREFILTER=segment selects the
+    // shared-memory segment kernels; VLS_RC=A|B|C a chunk layout)
+    const char *pf = std::getenv("VLS_PREFILTER");
+    const bool seg = pf && std::string(pf) == "segment";
+    const char *lay = std::getenv("VLS_RC");
+    const bool r64 = h->prec == VLS_FP64 || h->prec == VLS_FP32_BULK;
+    if (!seg) {
+      h->rcu_cfg = r64 ? rc_config<double>(h->tu, lay, true) : rc_config<float>(h->tu, lay, true);
+      h->rcr_cfg = r64 ? rc_config<double>(h->tr, lay, false) : rc_config<float>(h->tr, lay, false);
+    }
+    h->rcu_d = rc_dir<double>(h->tu, h->rcu_cfg);
+    h->rcr_d = rc_dir<double>(h->tr, h->rcr_cfg);
+    h->rcu_f = rc_dir<float>(h->tu, h->rcu_cfg);
+    h->rcr_f = rc_dir<float>(h->tr, h->rcr_cfg);
+  }
   if (cudaSetDevice(solver->device) != cudaSuccess)
     return fail(nullptr, VLS_ECUDA, "cudaSetDevice failed");
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess)
@@ -578,6 +612,16 @@ extern "C" int vls_create(const vls_grid_desc *grid,
       cudaMemsetAsync(h->count, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess ||
       cudaMemsetAsync(h->flag, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess)
     return fin(fail(hp, VLS_ECUDA, "cudaMemsetAsync failed"));
+  {
+    // drift layout: whole-strip staging where it fits (VLS_DRIFT=window, 48,
+    // 64 or -48 selects one for measurements)
+    const char *dv = std::getenv("VLS_DRIFT");
+    const std::string d = dv ? dv : "";
+    const int want = d == "48" ? 48 : d == "64" ? 64 : d == "-48" ? -48 : 0;
+    h->strip_w = d == "window" ? 0
+                 : h->esize == 4 ? drift_strip_width<float>(c.nu, want)
+                                 : drift_strip_width<double>(c.nu, want);
+  }
   h->have_tma = make_tensor_map(hp);
   // tables
   std::vector<double> dR(c.nr), dU(c.nu), Ct1(c.nj), bu(c.nu), wj(c.nj), dR4(c.nr),
@@ -899,6 +943,17 @@ extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
 }
 
 // ------------------------------------------------------------------ step
+template <typename R>
+static const RcDir<R> &rcdir(const vls_handle *h, bool u);
+template <>
+const RcDir<double> &rcdir<double>(const vls_handle *h, bool u) {
+  return u ? h->rcu_d : h->rcr_d;
+}
+template <>
+const RcDir<float> &rcdir<float>(const vls_handle *h, bool u) {
+  return u ? h->rcu_f : h->rcr_f;
+}
+
 template <typename T, typename R>
 static int drift_once(vls_handle *h, bool kick) {
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
@@ -918,10 +973,20 @@ static int drift_once(vls_handle *h, bool kick) {
     CK(h, timed(
               h, kick ? VLS_K_UCOL_KICK : VLS_K_UCOL,
               [&] {
+                if (h->rcu_cfg >= 0)
+                  return launch_ucol_rc<T, R>(h->rcu_cfg, kick, (const T *)h->f, G, h->shift,
+                                              g, rcdir<R>(h, true), bs);
                 return launch_ucol<T, R>(kick, (const T *)h->f, G, h->shift, g, tu, bs);
               },
               bs));
-    CK(h, timed(h, VLS_K_PRER, [&] { return launch_prer<T, R>(G, C, g, tr, bs); }, bs));
+    CK(h, timed(
+              h, VLS_K_PRER,
+              [&] {
+                if (h->rcr_cfg >= 0)
+                  return launch_prer_rc<T, R>(h->rcr_cfg, G, C, g, rcdir<R>(h, false), bs);
+                return launch_prer<T, R>(G, C, g, tr, bs);
+              },
+              bs));
     const int64_t c_lo = h->chain_lo[g.j0], c_hi = h->chain_lo[g.j0 + g.nb];
     if (c_hi > c_lo) {
       CK(h, timed(
@@ -936,6 +1001,12 @@ static int drift_once(vls_handle *h, bool kick) {
     CK(h, timed(
               h, VLS_K_DRIFT,
               [&] {
+                if (h->have_tma && h->strip_w != 0)
+                  return launch_drift_strip<T>(&h->tmS[sl], h->strip_w, C, (T *)h->f, h->idx,
+                                               (const T *)h->fx, (const T *)h->fy, h->fp2,
+                                               h->ch_start, h->ch_len, (const T *)h->ch_val,
+                                               h->ndrift, moment_tables(h), h->partial,
+                                               h->flag + 1, g, bs);
                 if (h->have_tma)
                   return launch_drift_tma<T>(&h->tmC[sl], C, (T *)h->f, h->idx,
                                              (const T *)h->fx, (const T *)h->fy, h->fp2,

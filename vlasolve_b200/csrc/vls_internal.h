@@ -58,6 +58,18 @@ struct MomentTables {
   const double *Rcoef;  // G/(R_r^2) * dt
 };
 
+// Register-resident prefilter (vls_rc.cu): L rows of a line per thread,
+// chunk layouts chosen per direction by rc_config.  RcDir is passed by value
+// as a kernel parameter, so its tables are read as constant-bank operands.
+template <typename R>
+struct RcDir {
+  R rp0[32], m0[32], q0[32];  // rp_k, -rp_k/6, q_k for rows k = 0..31
+  R mpow[33], qpow[33];       // (-rp_inf/6)^i and (-q_inf)^i, i = 0..32
+  R rp_inf, m_inf, q_inf;
+  R a01, a02, hi2, L1, L2;
+  int N, L, S;                // data rows, rows per chunk, chunks
+};
+
 // launchers (vls_kernels.cu); all asynchronous on `st`
 // T: storage type of f and the coefficients; R: arithmetic of the recursions
 template <typename T, typename R>
@@ -82,6 +94,19 @@ cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int
                              const T *ch_val, int64_t ndrift, const MomentTables &mt,
                              double *partial, unsigned int *err, const Geometry &g,
                              cudaStream_t st);
+// drift with the block's whole coefficient strip staged by TMA (tmS: 3D map
+// of C with box |width| columns x 64 rows x 1 slice); width from
+// drift_strip_width (48: two blocks per SM; 64, -48: one), 0 = unsupported;
+// want != 0 requests one layout
+template <typename T>
+int drift_strip_width(int nu, int want);
+template <typename T>
+cudaError_t launch_drift_strip(const CUtensorMap *tmS, int width, const T *C, T *f,
+                               const int32_t *idx, const T *fx, const T *fy, const uint2 *fp2,
+                               const int64_t *ch_start, const int32_t *ch_len,
+                               const T *ch_val, int64_t ndrift, const MomentTables &mt,
+                               double *partial, unsigned int *err, const Geometry &g,
+                               cudaStream_t st);
 // chains [c_lo, c_hi) (all of the launch's slices) of nchains in total
 template <typename T>
 cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
@@ -89,6 +114,20 @@ cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
                                const double *t_x, const double *t_y,
                                int64_t nchains, int64_t c_lo, int64_t c_hi,
                                int64_t ndrift, const Geometry &g, cudaStream_t st);
+struct HostDirTables;
+// chunk layout of the register kernels for a direction (-1: none takes it;
+// pref "A", "B", "C" or null for the default; u_lines for the ucol kernel)
+// and its tables
+template <typename R>
+int rc_config(const HostDirTables &t, const char *pref, bool u_lines);
+template <typename R>
+RcDir<R> rc_dir(const HostDirTables &t, int cfg);
+template <typename T, typename R>
+cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *shift,
+                           const Geometry &g, const RcDir<R> &tu, cudaStream_t st);
+template <typename T, typename R>
+cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
+                           cudaStream_t st);
 template <typename T>
 cudaError_t launch_moment(const T *f, const MomentTables &mt, double *partial,
                           const Geometry &g, cudaStream_t st);

@@ -760,6 +760,60 @@ __device__ __forceinline__ Cell<float> load_cell(const int32_t *, const float *,
   return c;
 }
 
+// Footpoint words as loaded (decoded only where the cell is computed, so that
+// prefetched loads stay in flight)
+template <typename T>
+struct RawCell;
+template <>
+struct RawCell<float> {
+  uint2 w;
+};
+template <>
+struct RawCell<double> {
+  int code;
+  double x, y;
+};
+__device__ __forceinline__ RawCell<float> load_raw(const int32_t *, const float *,
+                                                   const float *,
+                                                   const uint2 *__restrict__ fp2, size_t i) {
+  RawCell<float> c;
+  c.w = __ldg(fp2 + i);
+  return c;
+}
+__device__ __forceinline__ RawCell<double> load_raw(const int32_t *__restrict__ idx,
+                                                    const double *__restrict__ fx,
+                                                    const double *__restrict__ fy,
+                                                    const uint2 *, size_t i) {
+  RawCell<double> c;
+  c.code = __ldg(idx + i);
+  c.x = __ldg(fx + i);
+  c.y = __ldg(fy + i);
+  return c;
+}
+__device__ __forceinline__ Cell<float> decode(const RawCell<float> &r) {
+  Cell<float> c;
+  const uint2 w = r.w;
+  const bool ok = w.x < FP_CHAIN;
+  c.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
+  c.ch = w.y;
+  c.rI = ok ? (int)(w.x >> FP_FBITS) : 0;
+  c.uI = ok ? (int)(w.y >> FP_FBITS) : 0;
+  c.x = frac21(w.x);
+  c.y = frac21(w.y);
+  return c;
+}
+__device__ __forceinline__ Cell<double> decode(const RawCell<double> &r) {
+  Cell<double> c;
+  const int code = r.code;
+  c.kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
+  c.ch = (uint32_t)(-2 - code);
+  c.rI = code >= 0 ? (code & 0xffff) : 0;
+  c.uI = code >= 0 ? (code >> 16) : 0;
+  c.x = code >= 0 ? r.x : 0.0;
+  c.y = code >= 0 ? r.y : 0.0;
+  return c;
+}
+
 // 4x4 gather from a shared window row-pitched DW_COLS (immediate offsets)
 template <typename T>
 __device__ __forceinline__ T eval_window(const T *p, T x, T y) {
@@ -831,32 +885,31 @@ __global__ void __launch_bounds__(DT_THREADS)
   const T *Cj = C + (size_t)jl * (g.nu + 3) * g.pc;
   const size_t row0 = (size_t)j * g.nu * g.nr + r;
   const bool col_ok = r < g.nr;
-  Cell<T> nxt[2];
+  RawCell<T> nxt[2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const int u = w + 8 * q;
-    nxt[q] = load_cell(idx, fx, fy, fp2, row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
+    nxt[q] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
   }
   double acc = 0.0;
   // copy bookkeeping (meaningful in thread 0, which issues every copy): the
   // chunk last sent to each buffer and whether its completion was observed
-  int last[2] = {0, 1};
-  bool pending[2] = {true, nch > 1};
+  int last0 = 0, last1 = 1;                   // chunk last sent to buffer 0 / 1
+  unsigned pending = 1u | (nch > 1 ? 2u : 0u);  // bit b: buffer b's copy not yet seen
   bool issuing = true;
   for (int c = 0; c < nch; ++c) {
-    Cell<T> cur[2] = {nxt[0], nxt[1]};
+    const RawCell<T> cur[2] = {nxt[0], nxt[1]};
     if (c + 1 < nch) {
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int u = (c + 1) * DW_CH + w + 8 * q;
-        nxt[q] = load_cell(idx, fx, fy, fp2,
-                           row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
+        nxt[q] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
       }
     }
     const int b = c & 1;
     // after one failed wait this thread waits no more (it reads C globally)
     const bool have = issuing && mbar_wait_bounded(&bar[b], (uint32_t)((c >> 1) & 1));
-    if (have) pending[b] = false;
+    if (have) pending &= ~(1u << b);
     if (!have && issuing) {
       issuing = false;  // never stack a second copy onto an unfinished one
       atomicOr(err, 1u);
@@ -868,7 +921,7 @@ __global__ void __launch_bounds__(DT_THREADS)
     for (int q = 0; q < 2; ++q) {
       const int u = c * DW_CH + w + 8 * q;
       if (u < g.nu && col_ok) {
-        const Cell<T> &cl = cur[q];
+        const Cell<T> cl = decode(cur[q]);
         T v = T(0);
         if (cl.kind == 0) {
           const int wr = cl.uI - y0, wc = cl.rI - x0;
@@ -891,17 +944,19 @@ __global__ void __launch_bounds__(DT_THREADS)
       mbar_expect_tx(&bar[b], BYTES);
       tma_load_3d(win + b * DW_COLS * DW_ROWS, &tmC, x0, (c + 2) * DW_CH - DW_YOFF, jl,
                   &bar[b]);
-      last[b] = c + 2;
-      pending[b] = true;
+      if (b) last1 = c + 2; else last0 = c + 2;
+      pending |= 1u << b;
     }
   }
   // a copy whose wait timed out may still be in flight: wait for it (bounded)
   // before the block's shared memory is released
   if (tid == 0) {
-    for (int b = 0; b < 2; ++b)
-      if (pending[b] && last[b] < nch &&
-          !mbar_wait_bounded(&bar[b], (uint32_t)((last[b] >> 1) & 1)))
+    for (int b = 0; b < 2; ++b) {
+      const int lb = b ? last1 : last0;
+      if (((pending >> b) & 1u) && lb < nch &&
+          !mbar_wait_bounded(&bar[b], (uint32_t)((lb >> 1) & 1)))
         atomicOr(err, 2u);
+    }
   }
   red[w][lane] = acc;
   __syncthreads();
@@ -943,6 +998,222 @@ cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
                                                       ch_len, ch_val, ndrift, mt,
                                                       partial, g);
   return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ strip drift
+// Block: 32 output columns x every row of one J slice.  The block's whole
+// coefficient strip (WC columns starting (WC-32)/2 columns to the left, all
+// N_u+3 rows) is staged once by TMA in DS_ROWS-row boxes, one mbarrier per
+// box, so a cell can read any row of the strip: the footpoints' u
+// displacements reach hundreds of rows while their r displacements stay
+// within a few columns.  A cell waits only for the boxes its taps lie in
+// (bounded; after a timeout the thread reads C in global memory).  No block
+// barrier is taken inside the row loop.  Cells whose taps leave the strip's
+// columns gather from global memory.
+constexpr int DS_ROWS = 64;
+
+template <typename T, int PITCH>
+__device__ __forceinline__ T eval_pitch(const T *p, T x, T y) {
+  const T b2xI = bv2<T>(T(1) - x), b1xI = bv1<T>(T(1) - x);
+  const T b1x = bv1<T>(x), b2x = bv2<T>(x);
+  const T s0 = p[0] * b2xI + p[1] * b1xI + p[2] * b1x + p[3] * b2x;
+  const T s1 = p[PITCH] * b2xI + p[PITCH + 1] * b1xI + p[PITCH + 2] * b1x + p[PITCH + 3] * b2x;
+  const T s2 = p[2 * PITCH] * b2xI + p[2 * PITCH + 1] * b1xI + p[2 * PITCH + 2] * b1x +
+               p[2 * PITCH + 3] * b2x;
+  const T s3 = p[3 * PITCH] * b2xI + p[3 * PITCH + 1] * b1xI + p[3 * PITCH + 2] * b1x +
+               p[3 * PITCH + 3] * b2x;
+  return (T(1) / T(36)) * (bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
+                           bv1<T>(y) * s2 + bv2<T>(y) * s3);
+}
+template <int PITCH>
+__device__ __forceinline__ float eval_pitch_f32x2(const float *p, float x, float y) {
+  const float2 t = f2(x, y);
+  const float2 one = f2(1.f, 1.f), three = f2(3.f, 3.f), m3 = f2(-3.f, -3.f);
+  const float2 sv = __fadd2_rn(one, f2(-t.x, -t.y));
+  const float2 t2 = __fmul2_rn(t, t), t3 = __fmul2_rn(t2, t);
+  const float2 s2 = __fmul2_rn(sv, sv), s3 = __fmul2_rn(s2, sv);
+  const float2 a1 = __ffma2_rn(m3, s3, __ffma2_rn(three, s2, __ffma2_rn(three, sv, one)));
+  const float2 b1 = __ffma2_rn(m3, t3, __ffma2_rn(three, t2, __ffma2_rn(three, t, one)));
+  const float2 wx0 = f2(s3.x, s3.x), wx1 = f2(a1.x, a1.x), wx2 = f2(b1.x, b1.x),
+               wx3 = f2(t3.x, t3.x);
+  float2 r01 = __fmul2_rn(f2(p[0], p[PITCH]), wx0);
+  r01 = __ffma2_rn(f2(p[1], p[PITCH + 1]), wx1, r01);
+  r01 = __ffma2_rn(f2(p[2], p[PITCH + 2]), wx2, r01);
+  r01 = __ffma2_rn(f2(p[3], p[PITCH + 3]), wx3, r01);
+  const float *q = p + 2 * PITCH;
+  float2 r23 = __fmul2_rn(f2(q[0], q[PITCH]), wx0);
+  r23 = __ffma2_rn(f2(q[1], q[PITCH + 1]), wx1, r23);
+  r23 = __ffma2_rn(f2(q[2], q[PITCH + 2]), wx2, r23);
+  r23 = __ffma2_rn(f2(q[3], q[PITCH + 3]), wx3, r23);
+  const float2 acc = __ffma2_rn(r23, f2(b1.y, t3.y), __fmul2_rn(r01, f2(s3.y, a1.y)));
+  return (acc.x + acc.y) * (1.f / 36.f);
+}
+template <typename T, int PITCH>
+__device__ __forceinline__ T eval_strip(const T *p, T x, T y) {
+  if constexpr (sizeof(T) == 4)
+    return eval_pitch_f32x2<PITCH>(p, x, y);
+  else
+    return eval_pitch<T, PITCH>(p, x, y);
+}
+
+template <typename T, int WC, int NW, int MINB>
+__global__ void __launch_bounds__(32 * NW, MINB)
+    drift_strip_kernel(const __grid_constant__ CUtensorMap tmS, const T *__restrict__ C,
+                       T *__restrict__ f, const int32_t *__restrict__ idx,
+                       const T *__restrict__ fx, const T *__restrict__ fy,
+                       const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
+                       const int32_t *__restrict__ ch_len, const T *__restrict__ ch_val,
+                       int64_t ndrift, MomentTables mt, double *__restrict__ partial,
+                       unsigned int *err, Geometry g) {
+  constexpr int XL = (WC - 32) / 2;
+  constexpr int PF = 4;  // rows of footpoints in flight per thread
+  constexpr uint32_t BYTES = DS_ROWS * WC * sizeof(T);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ double red[NW][32];
+  const int rows = g.nu + 3;
+  const int nch = (rows + DS_ROWS - 1) / DS_ROWS;
+  T *win = reinterpret_cast<T *>(smem_raw);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + (size_t)nch * BYTES);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int r0 = blockIdx.x * 32, r = r0 + lane;
+  const int jl = blockIdx.y, j = g.j0 + jl;
+  const int x0 = r0 - XL;
+  if (tid == 0) {
+    for (int c = 0; c < nch; ++c) mbar_init(&bar[c], 1);
+    mbar_fence_init();
+    for (int c = 0; c < nch; ++c) {
+      mbar_expect_tx(&bar[c], BYTES);
+      tma_load_3d(win + (size_t)c * DS_ROWS * WC, &tmS, x0, c * DS_ROWS, jl, &bar[c]);
+    }
+  }
+  __syncthreads();
+  const T *Cj = C + (size_t)jl * rows * g.pc;
+  const size_t row0 = (size_t)j * g.nu * g.nr + r;
+  const bool col_ok = r < g.nr;
+  int ready = 0;  // boxes [0, ready) seen complete by this thread
+  bool waits_ok = true;
+  double acc = 0.0;
+  RawCell<T> q[PF];
+#pragma unroll
+  for (int k = 0; k < PF; ++k) {
+    const int u = w + NW * k;
+    q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
+  }
+  for (int ub = w; ub < g.nu; ub += NW * PF) {
+    T part = T(0);
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      const int u = ub + NW * k;
+      const Cell<T> cl = decode(q[k]);
+      const int un = u + NW * PF;
+      q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(un < g.nu && col_ok ? un : 0) * g.nr);
+      if (u < g.nu && col_ok) {
+        T v = T(0);
+        if (cl.kind == 0) {
+          const int wc = cl.rI - x0;
+          bool inwin = waits_ok && wc >= 0 && wc <= WC - 4;
+          if (inwin) {
+            // boxes complete in issue order; wait up to the one holding the last tap row
+            const int cb = (cl.uI + 3) / DS_ROWS;
+            while (ready <= cb) {
+              if (!mbar_wait_bounded(&bar[ready], 0u)) {
+                waits_ok = false;
+                inwin = false;
+                atomicOr(err, 1u);
+                break;
+              }
+              ++ready;
+            }
+          }
+          if (inwin)
+            v = eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y);
+          else
+            v = eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
+        } else if (cl.kind == 2) {
+          const int L = __ldg(ch_len + cl.ch);
+          v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
+        }
+        f[row0 + (size_t)u * g.nr] = v;
+        part += (T)__ldg(mt.bu + u) * v;
+      }
+    }
+    acc += (double)part;
+  }
+  // every box must have landed before the block's shared memory is released
+  if (tid == 0) {
+    for (int c = 0; c < nch; ++c)
+      if (!mbar_wait_bounded(&bar[c], 0u)) atomicOr(err, 2u);
+  }
+  red[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && col_ok) {
+    double sum = 0.0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) sum += red[k][lane];
+    partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * sum;
+  }
+}
+
+// strip layouts: 48 (48 columns, 8 warps, two blocks per SM), 64 (64
+// columns, 16 warps, one block per SM), -48 (48 columns, 16 warps, two blocks
+// per SM); 0: none, the windowed kernel is used.  `want` != 0 asks for one
+// layout, returned only if it fits.  The default is -48 for FP32 storage
+// where two blocks fit, else the windowed kernel (FP64 strips fit one block
+// per SM only, which measured slower than the windowed kernel).
+template <typename T>
+int drift_strip_width(int nu, int want) {
+  const int nch = (nu + 3 + DS_ROWS - 1) / DS_ROWS;
+  if (nch > 32) return 0;
+  auto dyn = [&](int wc) { return (size_t)nch * (DS_ROWS * wc * sizeof(T) + sizeof(uint64_t)); };
+  // 228 KB of shared memory per SM, 1 KB of it reserved per block; at most
+  // 227 KB per block; static reduction array NW x 32 doubles
+  const bool fit48x8 = 2 * (dyn(48) + 8 * 32 * 8 + 1024) <= 233472;
+  const bool fit48x16 = 2 * (dyn(48) + 16 * 32 * 8 + 1024) <= 233472;
+  const bool fit64 = dyn(64) + 16 * 32 * 8 <= 232448;
+  if (want == 48) return fit48x8 ? 48 : 0;
+  if (want == 64) return fit64 ? 64 : 0;
+  if (want == -48) return fit48x16 ? -48 : 0;
+  return (sizeof(T) == 4 && fit48x16) ? -48 : 0;
+}
+
+template <typename T, int WC, int NW, int MINB>
+static cudaError_t drift_strip_go(const CUtensorMap *tmS, const T *C, T *f, const int32_t *idx,
+                                  const T *fx, const T *fy, const uint2 *fp2,
+                                  const int64_t *ch_start, const int32_t *ch_len,
+                                  const T *ch_val, int64_t ndrift, const MomentTables &mt,
+                                  double *partial, unsigned int *err, const Geometry &g,
+                                  cudaStream_t st) {
+  const int nch = (g.nu + 3 + DS_ROWS - 1) / DS_ROWS;
+  const size_t smem = (size_t)nch * DS_ROWS * WC * sizeof(T) + nch * sizeof(uint64_t);
+  cudaError_t e = cudaFuncSetAttribute(drift_strip_kernel<T, WC, NW, MINB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((g.nr + 31) / 32, g.nb);
+  drift_strip_kernel<T, WC, NW, MINB><<<grid, 32 * NW, smem, st>>>(
+      *tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val, ndrift, mt, partial, err, g);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_drift_strip(const CUtensorMap *tmS, int width, const T *C, T *f,
+                               const int32_t *idx, const T *fx, const T *fy, const uint2 *fp2,
+                               const int64_t *ch_start, const int32_t *ch_len,
+                               const T *ch_val, int64_t ndrift, const MomentTables &mt,
+                               double *partial, unsigned int *err, const Geometry &g,
+                               cudaStream_t st) {
+  switch (width) {
+    case 64:
+      return drift_strip_go<T, 64, 16, 1>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
+                                          ndrift, mt, partial, err, g, st);
+    case 48:
+      return drift_strip_go<T, 48, 8, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
+                                         ndrift, mt, partial, err, g, st);
+    case -48:
+      return drift_strip_go<T, 48, 16, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
+                                          ndrift, mt, partial, err, g, st);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
 // tails: chains are independent; the tail slot (ndrift+L-1) mod L differs
@@ -1258,6 +1529,11 @@ cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
 }
 
 #define VLS_INST(T)                                                            \
+  template int drift_strip_width<T>(int, int);                                  \
+  template cudaError_t launch_drift_strip<T>(                                   \
+      const CUtensorMap *, int, const T *, T *, const int32_t *, const T *, const T *, \
+      const uint2 *, const int64_t *, const int32_t *, const T *, int64_t,       \
+      const MomentTables &, double *, unsigned int *, const Geometry &, cudaStream_t); \
   template cudaError_t launch_drift_tma<T>(                                     \
       const CUtensorMap *, const T *, T *, const int32_t *, const T *, const T *, \
       const uint2 *, const int64_t *, const int32_t *, const T *, int64_t,        \

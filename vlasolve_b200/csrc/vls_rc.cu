@@ -1,0 +1,576 @@
+// vls_rc.cu -- the cubic B-spline prefilter with register-resident lines.
+//
+// A line of the natural-BC system (localSpline::create_1D,
+// localSpline.hxx:953-1182) has N data rows k = 1..N and M = N + 2
+// coefficients.  It is cut into S = ceil(N / L) chunks of L rows; each
+// thread holds one chunk of one line in registers and runs the Thomas
+// recurrences there:
+//
+//   forward   d_k = (x_k - d_{k-1}/6) rp_k          (written d = d m_k + x rp_k)
+//   last row  c_{M-1} = ((0 - hi2 d_{N-1}) - L1 d_N) / L2
+//   backward  c_k = d_k - q_k c_{k+1},  c_0 = (0 - a01 c_1) - a02 c_2
+//
+// Chunks other than the first start their recurrence from zero and are
+// corrected afterwards: the true d_k differs from the local one by
+// m^(k - k_first + 1) times the true d at the row before the chunk (the
+// "carry"), and likewise backward with (-q)^(...).  From row L+1 on the
+// coefficients are constant (rp_inf, q_inf) in the recursion's precision, so
+// the correction factors are powers of one constant, held in the kernel
+// parameters.  A carry is the neighbour chunk's local end value plus m^L (or
+// (-q)^L) times the next one's; the remaining term is below m^(2L) (7e-18
+// for L = 15) of the values and is dropped.  The first chunk (rows 1..L, where the
+// coefficients still vary) runs the exact recurrences with the per-row
+// tables; the last chunk computes c_{M-1} and starts the backward pass from
+// it.
+//
+// Block layout (RcCfg): LN lines per block, 32/LN chunks per warp.  Warp 0
+// holds the first chunk (lanes 0..LN-1) and the last chunk (lanes LN..2LN-1),
+// the two chunks with their own code paths; every other warp holds 32/LN
+// middle chunks.  L is odd so that the chunks of a warp, whose rows differ by
+// multiples of L, fall on distinct shared-memory banks.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+
+#include "vls_internal.h"
+#include "vls_setup.h"
+
+namespace vls {
+
+namespace {
+
+template <int L_, int LN_, int NT_, int MINB_>
+struct RcCfg {
+  static constexpr int L = L_, LN = LN_, CPW = 32 / LN_, NT = NT_, MINB = MINB_;
+  // most chunks one block holds: warp 0 + (NT/32 - 1) warps of CPW chunks
+  static constexpr int MAXS = 2 + (NT_ / 32 - 1) * (32 / LN_);
+};
+// configuration ids (host and device agree on the order)
+using CfgA = RcCfg<31, 16, 320, 2>;   // 31-row chunks, 16 lines, two blocks per SM
+using CfgA1 = RcCfg<31, 16, 576, 1>;  // the same for up to 35 chunks
+using CfgB = RcCfg<15, 8, 320, 3>;    // 15-row chunks, 8 lines, three blocks per SM
+using CfgB1 = RcCfg<15, 8, 640, 1>;   // the same for up to 78 chunks
+using CfgC = RcCfg<15, 16, 576, 2>;   // 15-row chunks, 16 lines, two blocks per SM
+
+template <typename R>
+struct Dev;
+template <>
+struct Dev<double> {
+  static __device__ __forceinline__ double fma_(double a, double b, double c) {
+    return __fma_rn(a, b, c);
+  }
+};
+template <>
+struct Dev<float> {
+  static __device__ __forceinline__ float fma_(float a, float b, float c) {
+    return __fmaf_rn(a, b, c);
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ R rfma(R a, R b, R c) {
+  return Dev<R>::fma_(a, b, c);
+}
+
+// cubic B-spline weights (localSpline.hxx:381-441): BV2(x) = x^3,
+// BV1(x) = 1 + 3x + 3x^2 - 3x^3
+template <typename T>
+__device__ __forceinline__ T w_bv2(T x) {
+  return x * x * x;
+}
+template <typename T>
+__device__ __forceinline__ T w_bv1(T x) {
+  return T(1) + T(3) * x + T(3) * x * x - T(3) * x * x * x;
+}
+
+__host__ __device__ constexpr size_t al16(size_t b) { return (b + 15) / 16 * 16; }
+
+// chunk index, role and activity of this thread
+struct Role {
+  int s;        // chunk
+  bool active;  // holds a chunk
+  int ln;       // line within the block
+  int warp, grp;  // warp, chunk slot within the warp
+};
+
+template <class C>
+__device__ __forceinline__ Role rc_role(int S) {
+  Role o;
+  const int lane = threadIdx.x & 31;
+  o.warp = threadIdx.x >> 5;
+  o.grp = lane / C::LN;
+  o.ln = lane % C::LN;
+  if (o.warp == 0) {
+    o.s = o.grp == 0 ? 0 : S - 1;
+    o.active = o.grp == 0 || (o.grp == 1 && S >= 2);
+  } else {
+    o.s = 1 + (o.warp - 1) * C::CPW + o.grp;
+    o.active = o.s <= S - 2;
+  }
+  return o;
+}
+
+// The solve of one chunk per thread; v holds x on entry and c on exit.
+// dend, cst: shared [S][LN] carry slots.  c0 (first chunk) and cM (last
+// chunk) receive the two boundary coefficients.
+template <typename R, class C>
+__device__ __forceinline__ void rc_solve(R (&v)[C::L], const Role &ro, R *dend, R *cst,
+                                         const RcDir<R> &t, R &c0, R &cM) {
+  constexpr int L = C::L, LN = C::LN;
+  const int S = t.S, N = t.N;
+  const int s = ro.s;
+  const int kfirst = 1 + s * L;
+  const int slot = s * LN + ro.ln;
+  // ---------------------------------------------------------- phase A
+  if (s == 0) {
+    // first chunk: per-row tables (this code path diverges within warp 0)
+    R d = R(0);
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      d = rfma(d, t.m0[1 + i], v[i] * t.rp0[1 + i]);
+      v[i] = d;
+    }
+    if (ro.active && S >= 2) dend[slot] = d;
+  } else {
+    R d = R(0);
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      d = rfma(d, t.m_inf, v[i] * t.rp_inf);
+      v[i] = d;
+    }
+    if (ro.active) dend[slot] = d;
+  }
+  __syncthreads();
+  // ---------------------------------------------------------- phase B
+  if (ro.active) {
+    if (S == 1) {
+      // the only chunk is first and last: exact recurrences throughout
+      const int iN = N - 1;
+      R dl = v[0], dp = R(0);
+#pragma unroll
+      for (int i = 1; i < L; ++i)
+        if (i == iN) {
+          dl = v[i];
+          dp = v[i - 1];
+        }
+      cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+      R c = cM;
+#pragma unroll
+      for (int i = L - 1; i >= 0; --i)
+        if (i <= iN) {
+          c = rfma(-t.q0[1 + i], c, v[i]);
+          v[i] = c;
+        }
+      c0 = (R(0) - t.a01 * v[0]) - t.a02 * (N >= 2 ? v[1] : cM);
+    } else if (s > 0) {
+      R carry = dend[slot - LN];
+      if (s >= 2) carry = rfma(t.mpow[L], dend[slot - 2 * LN], carry);
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = rfma(t.mpow[i + 1], carry, v[i]);
+      R c;
+      if (s == S - 1) {
+        const int iN = N - kfirst;  // 0 .. L-1
+        R dl = v[0], dp = carry;
+#pragma unroll
+        for (int i = 1; i < L; ++i)
+          if (i == iN) {
+            dl = v[i];
+            dp = v[i - 1];
+          }
+        cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+        c = cM;
+#pragma unroll
+        for (int i = L - 1; i >= 0; --i)
+          if (i <= iN) {
+            c = rfma(-t.q_inf, c, v[i]);
+            v[i] = c;
+          }
+      } else {
+        c = R(0);
+#pragma unroll
+        for (int i = L - 1; i >= 0; --i) {
+          c = rfma(-t.q_inf, c, v[i]);
+          v[i] = c;
+        }
+      }
+      cst[slot] = c;
+    }
+  }
+  __syncthreads();
+  // ---------------------------------------------------------- phase C
+  if (ro.active && S >= 2 && s <= S - 2) {
+    R carry = cst[slot + LN];
+    if (s + 2 <= S - 1) carry = rfma(t.qpow[L], cst[slot + 2 * LN], carry);
+    if (s == 0) {
+      R c = carry;
+#pragma unroll
+      for (int i = L - 1; i >= 0; --i) {
+        c = rfma(-t.q0[1 + i], c, v[i]);
+        v[i] = c;
+      }
+      c0 = (R(0) - t.a01 * v[0]) - t.a02 * v[1];
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = rfma(t.qpow[L - i], carry, v[i]);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ ucol
+// Block: LN r columns of one J slice; a column is a u line.  With KICK: the
+// u-solve of f, the kick gather (vlasovSolver21_spline.hxx:752-770 with the
+// r-direction (1,4,1)/6 weights folded into the u-only coefficients) from a
+// shared copy of the column's coefficients, and the u-solve of the kicked
+// values; G receives the u-coefficients.
+template <typename T, typename R, bool KICK, class CF>
+__global__ void __launch_bounds__(CF::NT, CF::MINB)
+    ucol_rc_kernel(const T *__restrict__ f, T *__restrict__ G,
+                   const double *__restrict__ shift, Geometry g,
+                   const __grid_constant__ RcDir<R> t) {
+  constexpr int L = CF::L, LN = CF::LN;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int S = t.S, N = t.N;  // N == g.nu
+  const int M = N + 2;
+  R *dend = reinterpret_cast<R *>(smem_raw);
+  R *cst = dend + S * LN;
+  T *kb = reinterpret_cast<T *>(smem_raw + al16(2 * (size_t)S * LN * sizeof(R)));
+  const Role ro = rc_role<CF>(S);
+  const int r = blockIdx.x * LN + ro.ln;
+  const bool colok = r < g.nr;
+  const int jl = blockIdx.y, j = g.j0 + jl;
+  const int kfirst = 1 + ro.s * L;
+  R v[L];
+  {
+    // unpredicated loads kept inside the slice (rows clamped to N, columns
+    // to N_r - 1): values of rows beyond N and of idle threads are never used
+    const T *fc = f + (size_t)j * g.nu * g.nr + (colok ? r : g.nr - 1);
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const int k = min(kfirst + i, N);
+      v[i] = (R)__ldg(fc + (size_t)(k - 1) * g.nr);
+    }
+  }
+  R c0 = R(0), cM = R(0);
+  rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
+  if (KICK) {
+    if (ro.active) {
+#pragma unroll
+      for (int i = 0; i < L; ++i) {
+        const int k = kfirst + i;
+        if (k <= N) kb[k * LN + ro.ln] = (T)v[i];
+      }
+      if (ro.s == 0) kb[ro.ln] = (T)c0;
+      if (ro.s == S - 1) {
+        kb[(M - 1) * LN + ro.ln] = (T)cM;
+        kb[M * LN + ro.ln] = T(0);
+      }
+    }
+    __syncthreads();
+    // The shift is constant along the column and the u grid is uniform, so
+    // y_u = u + s*hu: one fraction and one integer offset serve every row,
+    // unless that fraction is within 1e-9 of a node (then every row takes
+    // the exact per-cell path).  Rows with 0 < u + s*hu < N-1 are inside
+    // (strictly, vlasovSolver21_spline.hxx:761); outside rows get 0.
+    const double sft = colok ? __ldg(shift + r) : 0.0;
+    const double qf = sft * g.hu;
+    const double fl = floor(qf);
+    const double frd = qf - fl;
+    const bool fast = frd > 1e-9 && frd < 1.0 - 1e-9 && fabs(qf) < 1e6;
+    if (ro.active) {
+      if (fast) {
+        const int o = (int)fl;
+        const T fr = (T)frd;
+        const T w0 = w_bv2<T>(T(1) - fr) * (T(1) / T(6)), w1 = w_bv1<T>(T(1) - fr) * (T(1) / T(6));
+        const T w2 = w_bv1<T>(fr) * (T(1) / T(6)), w3 = w_bv2<T>(fr) * (T(1) / T(6));
+        const int ulo = (int)floor(-qf) + 1;
+        const int uhi = (int)ceil((double)(N - 1) - qf) - 1;
+        // row k = kfirst + i (u = k - 1) reads coefficient rows k+o-1 .. k+o+2
+        const int ilo = ulo - kfirst + 1, ihi = min(uhi, N - 1) - kfirst + 1;
+        const T *base = kb + (ptrdiff_t)(kfirst + o - 1) * LN + ro.ln;
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+          T x = T(0);
+          if (i >= ilo && i <= ihi) {
+            const T *p = base + i * LN;
+            x = w0 * p[0] + w1 * p[LN] + w2 * p[2 * LN] + w3 * p[3 * LN];
+          }
+          v[i] = (R)x;
+        }
+      } else {
+        // exact per-cell path (localSpline.hxx:426-429)
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+          const int k = kfirst + i, u = k - 1;
+          R x = R(0);
+          if (k <= N) {
+            const double newU = __ldg(g.U + u) + sft;
+            if (newU > g.u0 && newU < g.umax) {
+              const double y = (newU - g.su) * g.hu;
+              const double yf = floor(y);
+              const T fr = (T)(y - yf);
+              const int Ny = 1 + (int)yf;
+              const T *p = kb + (ptrdiff_t)(Ny - 1) * LN + ro.ln;
+              x = (R)((T(1) / T(6)) * (w_bv2<T>(T(1) - fr) * p[0] + w_bv1<T>(T(1) - fr) * p[LN] +
+                                       w_bv1<T>(fr) * p[2 * LN] + w_bv2<T>(fr) * p[3 * LN]));
+            }
+          }
+          v[i] = x;
+        }
+      }
+    }
+    rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
+  }
+  if (ro.active && colok) {
+    T *Gc = G + (size_t)jl * M * g.nr + r;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const int k = kfirst + i;
+      if (k <= N) Gc[(size_t)k * g.nr] = (T)v[i];
+    }
+    if (ro.s == 0) Gc[0] = (T)c0;
+    if (ro.s == S - 1) Gc[(size_t)(M - 1) * g.nr] = (T)cM;
+  }
+}
+
+// ------------------------------------------------------------------ prer
+// Block: LN rows of G (u lines of the padded grid) of one J slice; a row is
+// an r line.  The rows are staged in shared memory (coalesced cp.async), each
+// thread moves its chunk into registers, solves, and writes it back; the
+// block then stores the tile to C with coalesced rows.
+//
+// Tile row pitch P: the lanes of a warp read (line ln, chunk slot m) at
+// ln*P + m*L + const.  FP32 words: P = LN/... chosen so that 32/LN lines
+// times the chunk slots cover the 32 banks (L odd): P = 2 mod 32 for 16
+// lines, 4 mod 32 for 8 lines.  FP64 words (16 lanes per wavefront): odd P
+// for 16 lines, 2 mod 16 for 8 lines.
+__host__ __device__ inline int rc_tile_pitch(int M, int elem, int LN) {
+  if (elem == 4) return (M + 31) / 32 * 32 + (LN == 16 ? 2 : 4);
+  if (LN == 16) return M | 1;
+  return (M + 15) / 16 * 16 + 2;
+}
+
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T *smem, const T *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem),
+               "n"(sizeof(T))
+               : "memory");
+}
+
+template <typename T, typename R, class CF>
+__global__ void __launch_bounds__(CF::NT, CF::MINB)
+    prer_rc_kernel(const T *__restrict__ G, T *__restrict__ C, Geometry g,
+                   const __grid_constant__ RcDir<R> t) {
+  constexpr int L = CF::L, LN = CF::LN;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int S = t.S, N = t.N;  // N == g.nr
+  const int M = N + 2;
+  const int P = rc_tile_pitch(M, sizeof(T), LN);
+  R *dend = reinterpret_cast<R *>(smem_raw);
+  R *cst = dend + S * LN;
+  T *tile = reinterpret_cast<T *>(smem_raw + al16(2 * (size_t)S * LN * sizeof(R)));
+  const Role ro = rc_role<CF>(S);
+  const int jl = blockIdx.y;
+  const int rows = g.nu + 2;
+  const int kr0 = blockIdx.x * LN;
+  const int nrow = min(LN, rows - kr0);
+  const T *Gs = G + ((size_t)jl * rows + kr0) * g.nr;
+  for (int p = 0; p < nrow; ++p) {
+    const T *src = Gs + (size_t)p * g.nr;
+    T *dst = tile + p * P + 1;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) cp_async_el(dst + k, src + k);
+  }
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  const bool lineok = ro.ln < nrow;
+  const int kfirst = 1 + ro.s * L;
+  R v[L];
+  {
+    // rows clamped to N; rows beyond N and lines beyond the tile's last
+    // row are computed but never stored
+    const T *row = tile + ro.ln * P;
+#pragma unroll
+    for (int i = 0; i < L; ++i) v[i] = (R)row[min(kfirst + i, N)];
+  }
+  R c0 = R(0), cM = R(0);
+  rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
+  if (ro.active && lineok) {
+    T *row = tile + ro.ln * P;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const int k = kfirst + i;
+      if (k <= N) row[k] = (T)v[i];
+    }
+    if (ro.s == 0) row[0] = (T)c0;
+    if (ro.s == S - 1) row[M - 1] = (T)cM;
+  }
+  __syncthreads();
+  T *Cs = C + ((size_t)jl * (g.nu + 3) + kr0) * g.pc;
+  for (int p = 0; p < nrow; ++p) {
+    const T *src = tile + p * P;
+    T *dst = Cs + (size_t)p * g.pc;
+    for (int k = threadIdx.x; k < M; k += blockDim.x) dst[k] = src[k];
+  }
+}
+
+template <class CF>
+int rc_threads(int S) {
+  const int warps = S == 1 ? 1 : 1 + (S - 2 + CF::CPW - 1) / CF::CPW;
+  return 32 * warps;
+}
+
+template <class CF>
+bool cfg_fits(int N, int kc) {
+  const int S = (N + CF::L - 1) / CF::L;
+  return N >= 2 && kc <= 1 + CF::L && S <= CF::MAXS;
+}
+
+template <typename K>
+cudaError_t rc_attr(K kern, size_t smem) {
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <typename T, typename R, bool KICK, class CF>
+cudaError_t ucol_rc_go(const T *f, T *G, const double *shift, const Geometry &g,
+                       const RcDir<R> &tu, cudaStream_t st) {
+  const int nt = rc_threads<CF>(tu.S);
+  if (tu.N != g.nu || nt > CF::NT || tu.L != CF::L) return cudaErrorInvalidValue;
+  const size_t smem = al16(2 * (size_t)tu.S * CF::LN * sizeof(R)) +
+                      (size_t)(tu.N + 3) * CF::LN * sizeof(T);
+  const dim3 grid((g.nr + CF::LN - 1) / CF::LN, g.nb);
+  auto k = ucol_rc_kernel<T, R, KICK, CF>;
+  cudaError_t e = rc_attr(k, smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, nt, smem, st>>>(f, G, shift, g, tu);
+  return cudaGetLastError();
+}
+
+template <typename T, typename R, class CF>
+cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
+                       cudaStream_t st) {
+  const int nt = rc_threads<CF>(tr.S);
+  if (tr.N != g.nr || nt > CF::NT || tr.L != CF::L) return cudaErrorInvalidValue;
+  const int M = tr.N + 2;
+  const size_t smem = al16(2 * (size_t)tr.S * CF::LN * sizeof(R)) +
+                      (size_t)CF::LN * rc_tile_pitch(M, sizeof(T), CF::LN) * sizeof(T);
+  const dim3 grid((g.nu + 2 + CF::LN - 1) / CF::LN, g.nb);
+  auto k = prer_rc_kernel<T, R, CF>;
+  cudaError_t e = rc_attr(k, smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, nt, smem, st>>>(G, C, g, tr);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- host side
+// configuration for one direction (u_lines: the ucol kernel's columns, else
+// the prer kernel's rows): `pref` "A", "B" or "C" (31-row chunks of 16
+// lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines) or empty for
+// the default; -1 when no configuration takes the shape
+template <typename R>
+int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
+  const int N = t.M - 2;
+  const int kc = sizeof(R) == 8 ? t.kc64 : t.kc32;
+  const std::string p = pref ? pref : "";
+  const int b = cfg_fits<CfgB>(N, kc) ? 2 : cfg_fits<CfgB1>(N, kc) ? 3 : -1;
+  if (p == "A") return cfg_fits<CfgA>(N, kc) ? 0 : cfg_fits<CfgA1>(N, kc) ? 1 : -1;
+  if (p == "B") return b;
+  if (p == "C") return cfg_fits<CfgC>(N, kc) ? 4 : -1;
+  // default (fastest measured on 513 x 513 x 256): 16-line blocks for the u
+  // lines, 8-line blocks for the r lines
+  if (u_lines && cfg_fits<CfgC>(N, kc)) return 4;
+  return b;
+}
+
+static int cfg_L(int cfg) { return cfg <= 1 ? CfgA::L : CfgB::L; }
+
+template <typename R>
+RcDir<R> rc_dir(const HostDirTables &t, int cfg) {
+  RcDir<R> o{};
+  const int M = t.M, N = M - 2;
+  const int L = cfg_L(cfg < 0 ? 0 : cfg);
+  const double sixth = 1.0 / 6.0;
+  for (int k = 0; k < 32; ++k) {
+    const double rp = (k >= 1 && k <= M - 2) ? t.rp[k] : t.rp_inf;
+    const double q = (k >= 1 && k <= M - 2) ? t.q[k] : t.q_inf;
+    o.rp0[k] = (R)rp;
+    o.m0[k] = (R)(-(sixth * rp));
+    o.q0[k] = (R)q;
+  }
+  o.rp_inf = (R)t.rp_inf;
+  o.m_inf = (R)(-(sixth * t.rp_inf));
+  o.q_inf = (R)t.q_inf;
+  const double m = -(sixth * t.rp_inf);
+  double pm = 1.0, pq = 1.0;
+  for (int i = 0; i <= 32; ++i) {
+    o.mpow[i] = (R)pm;
+    o.qpow[i] = (R)pq;
+    pm *= m;
+    pq *= -t.q_inf;
+  }
+  o.a01 = (R)t.a01;
+  o.a02 = (R)t.a02;
+  o.hi2 = (R)t.hi2;
+  o.L1 = (R)t.L1;
+  o.L2 = (R)t.L2;
+  o.N = N;
+  o.L = L;
+  o.S = (N + L - 1) / L;
+  return o;
+}
+
+template <typename T, typename R>
+cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *shift,
+                           const Geometry &g, const RcDir<R> &tu, cudaStream_t st) {
+#define VLS_UCOL_CFG(ID, CF)                                                    \
+  case ID:                                                                      \
+    return kick ? ucol_rc_go<T, R, true, CF>(f, G, shift, g, tu, st)            \
+                : ucol_rc_go<T, R, false, CF>(f, G, shift, g, tu, st);
+  switch (cfg) {
+    VLS_UCOL_CFG(0, CfgA)
+    VLS_UCOL_CFG(1, CfgA1)
+    VLS_UCOL_CFG(2, CfgB)
+    VLS_UCOL_CFG(3, CfgB1)
+    VLS_UCOL_CFG(4, CfgC)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef VLS_UCOL_CFG
+}
+
+template <typename T, typename R>
+cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
+                           cudaStream_t st) {
+  switch (cfg) {
+    case 0:
+      return prer_rc_go<T, R, CfgA>(G, C, g, tr, st);
+    case 1:
+      return prer_rc_go<T, R, CfgA1>(G, C, g, tr, st);
+    case 2:
+      return prer_rc_go<T, R, CfgB>(G, C, g, tr, st);
+    case 3:
+      return prer_rc_go<T, R, CfgB1>(G, C, g, tr, st);
+    case 4:
+      return prer_rc_go<T, R, CfgC>(G, C, g, tr, st);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+#define VLS_RC_INST(T, R)                                                                 \
+  template cudaError_t launch_ucol_rc<T, R>(int, bool, const T *, T *, const double *,   \
+                                            const Geometry &, const RcDir<R> &,          \
+                                            cudaStream_t);                               \
+  template cudaError_t launch_prer_rc<T, R>(int, const T *, T *, const Geometry &,       \
+                                            const RcDir<R> &, cudaStream_t);
+VLS_RC_INST(double, double)
+VLS_RC_INST(float, double)
+VLS_RC_INST(float, float)
+template int rc_config<double>(const HostDirTables &, const char *, bool);
+template int rc_config<float>(const HostDirTables &, const char *, bool);
+template RcDir<double> rc_dir<double>(const HostDirTables &, int);
+template RcDir<float> rc_dir<float>(const HostDirTables &, int);
+
+}  // namespace vls
