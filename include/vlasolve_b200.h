@@ -201,6 +201,26 @@ int vls_write_ndfield(vls_handle *h, const char *path);
    vls_write_ndfield into f (dims and datatype are checked) */
 int vls_read_ndfield(vls_handle *h, const char *path);
 
+/* Adjoint of the linked step (the reference has no derivative code).
+   vls_adjoint_forward runs nsteps steps from the current state (as vls_step)
+   and keeps a device copy of the state every checkpoint_every steps.
+   vls_adjoint_backward then takes dL/dbins of a loss L of the final radial
+   bins (nbins = N_r, the bins vls_moments returns for the final grid) and
+   returns dL/df of the initial grid (df0, N_r*N_u*N_J doubles, [j][u][r]) and
+   of the initial delayed-kernel chain values (dchain0, n_elems doubles in
+   vls_get_chains order; may be NULL).  The backward pass recomputes each
+   segment of checkpoint_every steps from its checkpoint and applies the
+   transposed step: drift and chain-tail gathers as scatter-adds, the
+   natural-BC prefilter transposed, the kick's gather transposed plus its
+   derivative with respect to the shift, and the transposed enclosed-mass
+   scan and moment.  The derivative is of the step as computed in the
+   handle's precision, evaluated in FP64.  Afterwards the handle holds the
+   final state again; vls_adjoint_backward may be called again with another
+   seed.  Linked step only (noLinking = 0). */
+int vls_adjoint_forward(vls_handle *h, int32_t nsteps, int32_t checkpoint_every);
+int vls_adjoint_backward(vls_handle *h, const double *dbins, int64_t nbins, double *df0,
+                         size_t ncells, double *dchain0, int64_t nelems);
+
 /* Radial moment of a grid that already lives in device memory, without any
    allocation (no counterpart in the reference, whose grid is host memory).
    For callers that own all device memory and must not let a library call

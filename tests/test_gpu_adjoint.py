@@ -1,0 +1,103 @@
+"""The hand-written adjoint of the step against central finite differences of
+full forward runs (FP64), against the FP64 adjoint (FP32 modes), and its
+checkpointing invariances.
+
+Loss: L(theta) = sum_r (rho_r(theta) - rho*_r)^2, rho the radial density of
+the final state and rho* the same forward run at theta + (0.05, -0.02, 0.03),
+theta = (R0, alpha, smoothingRadius) of the UDF profile."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+THETA = np.array([2.0, 0.5, 0.5])
+DTHETA = np.array([0.05, -0.02, 0.03])
+FD_STEP = 1e-4
+FD_RTOL = 1e-5       # adjoint vs central differences, FP64
+FP32_RTOL = 1e-3     # FP32-storage adjoints vs the FP64 adjoint
+
+
+def cfg(pres=32, ures=(24, 8), dt=0.02):
+    return {"type": "UDF", "Pmin": 0.01, "Pmax": 25.0, "Pres": pres,
+            "Pscale": "logarithmic", "Umin": (-2.0, 0.0), "Umax": (2.0, 1.6),
+            "Ures": ures, "Uscale": ("linear", "quadratic"), "dt": dt}
+
+
+def problem(precision="fp64", nsteps=12, K=5, **kw):
+    from vlasolve_b200.adjoint import DensityProblem
+    return DensityProblem(cfg(**kw), precision=precision, nsteps=nsteps, checkpoint_every=K)
+
+
+def loss_and_grad(p, target):
+    from vlasolve_b200.adjoint import final_density
+    th = torch.tensor(THETA, dtype=torch.float64, requires_grad=True)
+    rho = final_density(th, p)
+    L = ((rho - torch.as_tensor(target)) ** 2).sum()
+    L.backward()
+    return float(L.detach()), th.grad.numpy().copy()
+
+
+def test_adjoint_matches_central_differences():
+    p = problem()
+    target = p.run(THETA + DTHETA)
+    L0, g = loss_and_grad(p, target)
+    assert L0 > 0
+    fd = np.zeros(3)
+    for k in range(3):
+        tp, tm = THETA.copy(), THETA.copy()
+        tp[k] += FD_STEP
+        tm[k] -= FD_STEP
+        Lp = np.sum((p.run(tp) - target) ** 2)
+        Lm = np.sum((p.run(tm) - target) ** 2)
+        fd[k] = (Lp - Lm) / (2 * FD_STEP)
+    err = np.abs(g - fd) / np.max(np.abs(fd))
+    assert np.all(err <= FD_RTOL), (g, fd, err)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp32all"])
+def test_fp32_adjoint_matches_fp64_adjoint(precision):
+    p64 = problem("fp64")
+    target = p64.run(THETA + DTHETA)
+    _, g64 = loss_and_grad(p64, target)
+    p32 = problem(precision)
+    _, g32 = loss_and_grad(p32, target)
+    err = np.abs(g32 - g64) / np.max(np.abs(g64))
+    assert np.all(err <= FP32_RTOL), (g32, g64, err)
+
+
+@pytest.mark.parametrize("K", [1, 4, 12])
+def test_checkpoint_interval_does_not_change_gradient(K):
+    p_ref = problem(K=5)
+    target = p_ref.run(THETA + DTHETA)
+    _, g_ref = loss_and_grad(p_ref, target)
+    _, g = loss_and_grad(problem(K=K), target)
+    np.testing.assert_allclose(g, g_ref, rtol=1e-10, atol=1e-14 * np.max(np.abs(g_ref)))
+
+
+def test_backward_restores_final_state_and_repeats():
+    p = problem()
+    p.run(THETA)
+    s = p.solver
+    f_final = s.f
+    dbins = np.linspace(0.0, 1.0, s.nr)
+    a, ca = s.adjoint_backward(dbins)
+    np.testing.assert_array_equal(s.f, f_final)
+    b, cb = s.adjoint_backward(dbins)
+    np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-14 * np.max(np.abs(a)))
+    np.testing.assert_allclose(ca, cb, rtol=1e-12, atol=1e-14 * max(np.max(np.abs(ca), initial=0), 1e-300))
+    # linear in the seed
+    c, _ = s.adjoint_backward(2.0 * dbins)
+    np.testing.assert_allclose(c, 2.0 * a, rtol=1e-12, atol=1e-14 * np.max(np.abs(a)))
+
+
+def test_adjoint_rejects_nolinking_and_missing_forward():
+    from vlasolve_b200 import VlasovSolver21Spline
+    from vlasolve_b200._lib import VlsError
+    c = dict(cfg(), noLinking=1)
+    s = VlasovSolver21Spline(c)
+    with pytest.raises(VlsError):
+        s.adjoint_forward(3, 1)
+    s2 = VlasovSolver21Spline(cfg())
+    with pytest.raises(VlsError):
+        s2.adjoint_backward(np.zeros(s2.nr))

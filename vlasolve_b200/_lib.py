@@ -29,6 +29,7 @@ EXPORTED = [
     "vls_moments", "vls_last_mass", "vls_stats", "vls_get_time", "vls_set_time",
     "vls_write_ndfield", "vls_read_ndfield", "vls_stream", "vls_set_profiling",
     "vls_profile_read", "vls_radial_mass_noalloc", "vls_noalloc_last_error",
+    "vls_adjoint_forward", "vls_adjoint_backward",
 ]
 KERNEL_KINDS = ["ucol_kick", "ucol", "prer", "tails", "drift", "scan", "moment",
                 "stats", "convert"]
@@ -114,6 +115,8 @@ def load(path: str = LIB_PATH):
         "vls_stream": [H, P(ctypes.c_void_p)],
         "vls_set_profiling": [H, i32],
         "vls_profile_read": [H, P(d), P(i64), i32],
+        "vls_adjoint_forward": [H, i32, i32],
+        "vls_adjoint_backward": [H, P(d), i64, P(d), ctypes.c_size_t, P(d), i64],
         "vls_radial_mass_noalloc": [ctypes.c_void_p, i32, i64, i64, i64, P(d), P(d), P(d),
                                     P(d), ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, i32],

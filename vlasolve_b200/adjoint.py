@@ -1,0 +1,94 @@
+"""Gradients of a final radial-density loss with respect to initial-condition
+parameters, through the hand-written adjoint of the step.
+
+The reference has no derivative code.  The adjoint of the N linked steps runs
+in the CUDA library (vls_adjoint_forward / vls_adjoint_backward: transposed
+drift and chain-tail gathers, transposed natural-BC prefilter, transposed
+kick with its shift derivative, transposed enclosed-mass scan and moment),
+with checkpoints every K steps and recomputation of each segment.  It yields
+dL/df0 and dL/d(initial chain values).  The map from the parameters theta to
+the initial state (the analytic distribution function and its
+renormalisation, vlasovSolver21::renormalize) is differentiated by central
+differences of that map alone, evaluated in FP64, which costs two
+initial-state evaluations per parameter and no time steps.
+
+FinalDensity wraps this as a torch.autograd.Function: forward(theta) returns
+the radial density of the final state, backward(grad) returns grad_theta.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .solver import VlasovSolver21Spline
+
+
+class DensityProblem:
+    """A forward run of `nsteps` linked steps from the initial state generated
+    with parameters `params` (init.* names) = theta."""
+
+    def __init__(self, cfg, precision: str = "fp64", nsteps: int = 1,
+                 checkpoint_every: int = 1, params=("R0", "alpha", "smoothingRadius"),
+                 ic_step: float = 1e-6, device: int = 0):
+        self.solver = VlasovSolver21Spline(cfg, precision=precision, device=device, init=False)
+        # the initial-state map is differenced in FP64 whatever the storage
+        # precision (differences of FP32-rounded grids would lose the digits)
+        self.ic = (self.solver if precision == "fp64" else
+                   VlasovSolver21Spline(cfg, precision="fp64", device=device, init=False))
+        self.nsteps, self.K = int(nsteps), int(checkpoint_every)
+        self.params = tuple(params)
+        self.ic_step = ic_step
+        self.vol = None
+        self.theta = None
+
+    def initial_state(self, theta):
+        """FP64 initial grid and chain values for parameters theta."""
+        self.ic.set_init_params(**dict(zip(self.params, map(float, theta))))
+        return self.ic.f, self.ic.chains()["val"]
+
+    def run(self, theta) -> np.ndarray:
+        """Radial density of the final state for parameters theta."""
+        self.theta = np.asarray(theta, dtype=np.float64).copy()
+        self.solver.set_init_params(**dict(zip(self.params, map(float, self.theta))))
+        self.solver.set_time(0.0, 0)
+        self.solver.adjoint_forward(self.nsteps, self.K)
+        if self.vol is None:
+            self.vol = self.solver.shell_volumes()
+        return self.solver.radial_density()
+
+    def vjp(self, grad_rho) -> np.ndarray:
+        """grad_theta = (d rho / d theta)^T grad_rho at the last run's theta."""
+        g = np.asarray(grad_rho, dtype=np.float64)
+        dbins = np.zeros(self.solver.nr)
+        dbins[:-1] = g / self.vol
+        df0, dch0 = self.solver.adjoint_backward(dbins)
+        out = np.zeros(len(self.params))
+        for k in range(len(self.params)):
+            h = self.ic_step * max(1.0, abs(self.theta[k]))
+            tp, tm = self.theta.copy(), self.theta.copy()
+            tp[k] += h
+            tm[k] -= h
+            fp, cp = self.initial_state(tp)
+            fm, cm = self.initial_state(tm)
+            out[k] = (np.vdot(df0, fp - fm) + np.vdot(dch0, cp - cm)) / (2 * h)
+        return out
+
+
+class FinalDensity(torch.autograd.Function):
+    """theta (float64 tensor of the problem's parameters) -> final radial
+    density (float64 tensor of N_r - 1 shells)."""
+
+    @staticmethod
+    def forward(ctx, theta, problem: DensityProblem):
+        rho = problem.run(theta.detach().cpu().numpy())
+        ctx.problem = problem
+        return torch.as_tensor(rho, dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx, grad_rho):
+        g = ctx.problem.vjp(grad_rho.detach().cpu().numpy())
+        return torch.as_tensor(g, dtype=torch.float64), None
+
+
+def final_density(theta: torch.Tensor, problem: DensityProblem) -> torch.Tensor:
+    return FinalDensity.apply(theta, problem)

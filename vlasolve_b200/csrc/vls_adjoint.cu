@@ -1,0 +1,373 @@
+// vls_adjoint.cu -- kernels of the adjoint (reverse-mode derivative) of the
+// linked step f_{n+1} = D P_r P_u Kick(P_u f_n; s(f_n)) + chains.
+//
+// The reference has no derivative code; this is the transpose of the step as
+// the forward kernels compute it (vls_kernels.cu, vls_rc.cu):
+//   drift D       f(cell) = sum_ab wy_a wx_b C[uI+a][rI+b] / 36   -> scatter-add
+//   tails E       ring[tail] = same gather at the chain's end    -> scatter-add
+//   prefilter P   natural-BC Thomas solve of each line           -> transposed
+//                 recurrences (localSpline.hxx:953-1182 read backwards)
+//   kick          per column: gather at y = u + s_r hu           -> transposed
+//                 gather, plus d/ds_r of the interpolant
+//   shift s       s_r = Rcoef_r sum_{r' < r} bins_r'             -> reverse scan
+//   moment        bins_r = dR_r/4 (T_r + T_{r+1}), T_r = sum_j w_j sum_u b_u f
+// Adjoint values are FP64 in every precision mode; the forward state they
+// linearise around is read in the handle's storage type.  Scatter-adds use
+// FP64 atomics (their summation order is not deterministic).
+#include <cuda_runtime.h>
+
+#include "vls_internal.h"
+
+namespace vls {
+
+namespace {
+
+__device__ __forceinline__ double bv2d(double x) { return x * x * x; }
+__device__ __forceinline__ double bv1d(double x) {
+  return 1.0 + 3.0 * x + 3.0 * x * x - 3.0 * x * x * x;
+}
+// derivatives of the kick weights w_m(fr)/6 with respect to fr
+__device__ __forceinline__ void kick_weights(double fr, double w[4], double dw[4]) {
+  const double a = 1.0 - fr;
+  w[0] = bv2d(a) / 6.0;
+  w[1] = bv1d(a) / 6.0;
+  w[2] = bv1d(fr) / 6.0;
+  w[3] = bv2d(fr) / 6.0;
+  dw[0] = -3.0 * a * a / 6.0;
+  dw[1] = -(3.0 + 6.0 * a - 9.0 * a * a) / 6.0;
+  dw[2] = (3.0 + 6.0 * fr - 9.0 * fr * fr) / 6.0;
+  dw[3] = 3.0 * fr * fr / 6.0;
+}
+
+// forward natural-BC solve of a line (FP64): x at xs[(k-1)*xst], k = 1..N;
+// coefficients c_0..c_{M-1} to cs[k*cst] (may not alias xs)
+__device__ void solve_line_fwd(const double *x, int xst, double *c, int cst,
+                               const DirTables &t) {
+  const int M = t.M, N = M - 2;
+  double d = 0.0, dprev = 0.0;
+  for (int k = 1; k <= N; ++k) {
+    dprev = d;
+    d = (x[(size_t)(k - 1) * xst] - d * (1.0 / 6.0)) * t.rp[k];
+    c[(size_t)k * cst] = d;
+  }
+  double cc = ((0.0 - t.hi2 * dprev) - t.L1 * d) / t.L2;
+  c[(size_t)(M - 1) * cst] = cc;
+  double cn = cc;
+  for (int k = N; k >= 1; --k) {
+    const double v = c[(size_t)k * cst] - t.q[k] * cn;
+    c[(size_t)k * cst] = v;
+    cc = cn;
+    cn = v;
+  }
+  // cn = c_1, cc = c_2
+  c[0] = (0.0 - t.a01 * cn) - t.a02 * cc;
+}
+
+// transposed solve: cbar[k*cst] (k = 0..M-1) -> xbar[(k-1)*xst] (k = 1..N);
+// xbar may alias neither cbar's storage nor overlap it
+__device__ void solve_line_adj(const double *cb, int cst, double *xb, int xst,
+                               const DirTables &t) {
+  const int M = t.M, N = M - 2;
+  const double c0b = cb[0];
+  // back-substitution and first row, transposed (ascending): e_k = cbar_k
+  // complete, dbar_k = e_k
+  double e = cb[(size_t)1 * cst] - t.a01 * c0b;
+  xb[0] = e;
+  for (int k = 2; k <= N; ++k) {
+    double ck = cb[(size_t)k * cst];
+    if (k == 2) ck -= t.a02 * c0b;
+    e = ck - t.q[k - 1] * e;
+    xb[(size_t)(k - 1) * xst] = e;
+  }
+  double cMb = cb[(size_t)(M - 1) * cst] - t.q[N] * e;
+  if (N == 1) cMb -= t.a02 * c0b;  // c_2 is then the last coefficient
+  // last row, transposed
+  if (N >= 2) xb[(size_t)(N - 2) * xst] += -(t.hi2 / t.L2) * cMb;
+  xb[(size_t)(N - 1) * xst] += -(t.L1 / t.L2) * cMb;
+  // forward elimination, transposed (descending)
+  double fk = xb[(size_t)(N - 1) * xst];
+  xb[(size_t)(N - 1) * xst] = t.rp[N] * fk;
+  for (int k = N - 1; k >= 1; --k) {
+    fk = xb[(size_t)(k - 1) * xst] - (1.0 / 6.0) * t.rp[k + 1] * fk;
+    xb[(size_t)(k - 1) * xst] = t.rp[k] * fk;
+  }
+}
+
+__device__ __forceinline__ void scatter16(double *Cbj, int pc, int rI, double x, int uI,
+                                          double y, double v) {
+  const double wx[4] = {bv2d(1.0 - x), bv1d(1.0 - x), bv1d(x), bv2d(x)};
+  const double wy[4] = {bv2d(1.0 - y), bv1d(1.0 - y), bv1d(y), bv2d(y)};
+  const double s = v * (1.0 / 36.0);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    double *row = Cbj + (size_t)(uI + a) * pc + rI;
+    const double sa = s * wy[a];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) atomicAdd(row + b, sa * wx[b]);
+  }
+}
+
+constexpr uint32_t AFP_OUT = 0xFFFFFFFFu, AFP_CHAIN = 0xFFFFFFFEu;
+constexpr int AFP_FBITS = 21;
+
+// drift, transposed: lam (cells) -> Cb (C layout, all slices), chain fronts
+// -> ring adjoint
+template <typename T>
+__global__ void drift_adj_kernel(const double *__restrict__ lam, double *__restrict__ Cb,
+                                 const int32_t *__restrict__ idx, const T *__restrict__ fx,
+                                 const T *__restrict__ fy, const uint2 *__restrict__ fp2,
+                                 const int64_t *__restrict__ ch_start,
+                                 const int32_t *__restrict__ ch_len, double *__restrict__ ringb,
+                                 int64_t ndrift, Geometry g) {
+  const size_t n = (size_t)g.nr * g.nu * g.nj;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double v = lam[i];
+    if (v == 0.0) continue;
+    const int j = (int)(i / ((size_t)g.nr * g.nu));
+    int kind, rI = 0, uI = 0;
+    uint32_t ch = 0;
+    double x = 0, y = 0;
+    if (sizeof(T) == 8) {
+      const int code = idx[i];
+      kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
+      ch = (uint32_t)(-2 - code);
+      if (code >= 0) {
+        rI = code & 0xffff;
+        uI = code >> 16;
+        x = (double)fx[i];
+        y = (double)fy[i];
+      }
+    } else {
+      const uint2 w = fp2[i];
+      kind = w.x < AFP_CHAIN ? 0 : (w.x == AFP_OUT ? 1 : 2);
+      ch = w.y;
+      if (kind == 0) {
+        rI = (int)(w.x >> AFP_FBITS);
+        uI = (int)(w.y >> AFP_FBITS);
+        const uint32_t m = (1u << AFP_FBITS) - 1u;
+        // the forward decodes the fraction to float exactly (21 bits)
+        x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
+        y = (double)(__uint_as_float(0x3F800000u | ((w.y & m) << 2)) - 1.0f);
+      }
+    }
+    if (kind == 0) {
+      scatter16(Cb + (size_t)j * (g.nu + 3) * g.pc, g.pc, rI, x, uI, y, v);
+    } else if (kind == 2) {
+      const int L = ch_len[ch];
+      atomicAdd(ringb + ch_start[ch] + ndrift % L, v);
+    }
+  }
+}
+
+// chain tails, transposed: ring adjoint of each chain's tail slot -> Cb
+// (the slot's value was written by this step's tails, so its adjoint is
+// consumed and cleared)
+__global__ void tails_adj_kernel(double *__restrict__ Cb, double *__restrict__ ringb,
+                                 const int64_t *__restrict__ ch_start,
+                                 const int32_t *__restrict__ ch_len,
+                                 const int32_t *__restrict__ t_idx, const double *__restrict__ t_x,
+                                 const double *__restrict__ t_y, const int32_t *__restrict__ t_j,
+                                 int64_t nch, int64_t ndrift, Geometry g) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  const int L = ch_len[c];
+  double *slot = ringb + ch_start[c] + (ndrift + L - 1) % L;
+  const double v = *slot;
+  *slot = 0.0;
+  const int code = t_idx[c];
+  if (code >= 0 && v != 0.0)
+    scatter16(Cb + (size_t)t_j[c] * (g.nu + 3) * g.pc, g.pc, code & 0xffff, t_x[c], code >> 16,
+              t_y[c], v);
+}
+
+// r-solve, transposed: each row k of every slice, Cb[j][k][0..M_r-1] ->
+// Gb[j][k][0..N_r-1]
+__global__ void prer_adj_kernel(const double *__restrict__ Cb, double *__restrict__ Gb,
+                                Geometry g, DirTables tr) {
+  const int rows = g.nu + 2;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)rows * g.nj) return;
+  const int j = (int)(i / rows), k = (int)(i % rows);
+  const double *cb = Cb + ((size_t)j * (g.nu + 3) + k) * g.pc;
+  double *gb = Gb + ((size_t)j * rows + k) * g.nr;
+  solve_line_adj(cb, 1, gb, 1, tr);
+}
+
+// u-solves and kick, transposed, one thread per (slice, column):
+//   g    = P_u f_n                      (scratch A, G layout)
+//   fbar = P_u^T Gb                     (in place in Gb rows 1..N_u)
+//   gbar = Kick^T fbar, sbar partial    (scratch B, G layout)
+//   lam  = P_u^T gbar                   (cells)
+template <typename T>
+__global__ void ucol_adj_kernel(const T *__restrict__ f, double *__restrict__ Gb,
+                                double *__restrict__ A, double *__restrict__ B,
+                                double *__restrict__ lam, double *__restrict__ sbar,
+                                const double *__restrict__ shift, Geometry g, DirTables tu) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)g.nr * g.nj) return;
+  const int j = (int)(i / g.nr), r = (int)(i % g.nr);
+  const int N = g.nu, M = N + 2;
+  const size_t gofs = (size_t)j * M * g.nr + r;
+  double *gcol = A + gofs;     // g = P_u f_n, rows 0..M-1
+  double *bcol = B + gofs;     // gbar
+  double *Gcol = Gb + gofs;    // Gbar -> fbar (rows 1..N hold fbar_u at row u+1)
+  const size_t fofs = (size_t)j * N * g.nr + r;
+  // g = P_u f_n (f read as FP64)
+  {
+    // solve_line_fwd reads x from a double array: stage f into bcol rows 1..N
+    for (int u = 0; u < N; ++u) bcol[(size_t)(u + 1) * g.nr] = (double)f[fofs + (size_t)u * g.nr];
+    solve_line_fwd(bcol + g.nr, g.nr, gcol, g.nr, tu);
+  }
+  // fbar = P_u^T Gbar, written to bcol rows 1..N (then moved back to Gcol)
+  solve_line_adj(Gcol, g.nr, bcol + g.nr, g.nr, tu);
+  for (int u = 0; u < N; ++u) Gcol[(size_t)(u + 1) * g.nr] = bcol[(size_t)(u + 1) * g.nr];
+  for (int k = 0; k < M; ++k) bcol[(size_t)k * g.nr] = 0.0;
+  // kick, transposed (vlasovSolver21_spline.hxx:752-770 as the forward
+  // kernels compute it: fast path with one fraction per column, or the exact
+  // per-cell path when the fraction is within 1e-9 of a node)
+  const double sft = shift[r];
+  const double qf = sft * g.hu;
+  const double fl = floor(qf);
+  const double frd = qf - fl;
+  const bool fast = frd > 1e-9 && frd < 1.0 - 1e-9 && fabs(qf) < 1e6;
+  double sb = 0.0;
+  double w[4], dw[4];
+  if (fast) kick_weights(frd, w, dw);
+  const int o = fast ? (int)fl : 0;
+  const int ulo = fast ? (int)floor(-qf) + 1 : 0;
+  const int uhi = fast ? (int)ceil((double)(N - 1) - qf) - 1 : -1;
+  for (int u = 0; u < N; ++u) {
+    const double fb = Gcol[(size_t)(u + 1) * g.nr];
+    int Ny;
+    if (fast) {
+      if (u < ulo || u > uhi) continue;
+      Ny = 1 + u + o;
+    } else {
+      const double newU = g.U[u] + sft;
+      if (!(newU > g.u0 && newU < g.umax)) continue;
+      const double y = (newU - g.su) * g.hu;
+      const double yf = floor(y);
+      kick_weights(y - yf, w, dw);
+      Ny = 1 + (int)yf;
+    }
+    double dv = 0.0;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      // a tap on row M is the forward's always-zero guard row
+      if (Ny - 1 + m >= M) continue;
+      const size_t row = (size_t)(Ny - 1 + m) * g.nr;
+      bcol[row] += w[m] * fb;
+      dv += dw[m] * gcol[row];
+    }
+    sb += fb * dv * g.hu;
+  }
+  sbar[(size_t)j * g.nr + r] = sb;
+  // lam = P_u^T gbar
+  solve_line_adj(bcol, g.nr, lam + fofs, g.nr, tu);
+}
+
+// shift, transposed: sbar (per slice) -> beta_r' = sum_{r > r'} Rcoef_r sum_j sbar[j][r]
+__global__ void shift_adj_kernel(const double *__restrict__ sbar, double *__restrict__ beta,
+                                 MomentTables mt, Geometry g) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double acc = 0.0;
+  for (int r = g.nr - 1; r >= 0; --r) {
+    beta[r] = acc;  // exclusive: bins_r' enters s_r for r > r'
+    double s = 0.0;
+    for (int j = 0; j < g.nj; ++j) s += sbar[(size_t)j * g.nr + r];
+    acc += s * mt.Rcoef[r];
+  }
+}
+
+// moment, transposed: lam += w_j b_u (beta_r dR_r/4 + beta_{r-1} dR_{r-1}/4)
+__global__ void moment_adj_kernel(double *__restrict__ lam, const double *__restrict__ beta,
+                                  MomentTables mt, Geometry g) {
+  const size_t n = (size_t)g.nr * g.nu * g.nj;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i % g.nr);
+    const size_t ju = i / g.nr;
+    const int u = (int)(ju % g.nu), j = (int)(ju / g.nu);
+    double b = beta[r] * mt.dR4[r];
+    if (r > 0) b += beta[r - 1] * mt.dR4[r - 1];
+    lam[i] += mt.wj[j] * mt.bu[u] * b;
+  }
+}
+
+unsigned grid_for(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  if (b > 148 * 64) b = 148 * 64;
+  return (unsigned)(b ? b : 1);
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_drift_adj(const double *lam, double *Cb, const int32_t *idx, const T *fx,
+                             const T *fy, const uint2 *fp2, const int64_t *ch_start,
+                             const int32_t *ch_len, double *ringb, int64_t ndrift,
+                             const Geometry &g, cudaStream_t st) {
+  const size_t n = (size_t)g.nr * g.nu * g.nj;
+  drift_adj_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(lam, Cb, idx, fx, fy, fp2, ch_start,
+                                                         ch_len, ringb, ndrift, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tails_adj(double *Cb, double *ringb, const int64_t *ch_start,
+                             const int32_t *ch_len, const int32_t *t_idx, const double *t_x,
+                             const double *t_y, int64_t nch, int64_t ndrift, const Geometry &g,
+                             cudaStream_t st) {
+  if (nch <= 0) return cudaSuccess;
+  const int threads = 256;
+  tails_adj_kernel<<<(unsigned)((nch + threads - 1) / threads), threads, 0, st>>>(
+      Cb, ringb, ch_start, ch_len, t_idx, t_x, t_y, t_idx + nch, nch, ndrift, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prer_adj(const double *Cb, double *Gb, const Geometry &g,
+                            const DirTables &tr, cudaStream_t st) {
+  const int64_t n = (int64_t)(g.nu + 2) * g.nj;
+  prer_adj_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(Cb, Gb, g, tr);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_ucol_adj(const T *f, double *Gb, double *A, double *B, double *lam,
+                            double *sbar, const double *shift, const Geometry &g,
+                            const DirTables &tu, cudaStream_t st) {
+  const int64_t n = (int64_t)g.nr * g.nj;
+  ucol_adj_kernel<T><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(f, Gb, A, B, lam, sbar,
+                                                                   shift, g, tu);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTables &mt,
+                             const Geometry &g, cudaStream_t st) {
+  shift_adj_kernel<<<1, 32, 0, st>>>(sbar, beta, mt, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_moment_adj(double *lam, const double *beta, const MomentTables &mt,
+                              const Geometry &g, cudaStream_t st) {
+  const size_t n = (size_t)g.nr * g.nu * g.nj;
+  moment_adj_kernel<<<grid_for(n, 256), 256, 0, st>>>(lam, beta, mt, g);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_drift_adj<float>(const double *, double *, const int32_t *,
+                                             const float *, const float *, const uint2 *,
+                                             const int64_t *, const int32_t *, double *,
+                                             int64_t, const Geometry &, cudaStream_t);
+template cudaError_t launch_drift_adj<double>(const double *, double *, const int32_t *,
+                                              const double *, const double *, const uint2 *,
+                                              const int64_t *, const int32_t *, double *,
+                                              int64_t, const Geometry &, cudaStream_t);
+template cudaError_t launch_ucol_adj<float>(const float *, double *, double *, double *,
+                                            double *, double *, const double *,
+                                            const Geometry &, const DirTables &, cudaStream_t);
+template cudaError_t launch_ucol_adj<double>(const double *, double *, double *, double *,
+                                             double *, double *, const double *,
+                                             const Geometry &, const DirTables &, cudaStream_t);
+
+}  // namespace vls

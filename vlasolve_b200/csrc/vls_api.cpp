@@ -93,6 +93,20 @@ struct vls_handle {
   std::vector<cudaEvent_t> evpool;
   std::string err;
   std::vector<void *> allocs;
+  // adjoint: checkpoints of the forward run (state before steps 0, K, 2K, ...),
+  // the final state, and the FP64 adjoint arrays; freed by the next forward
+  // run or by vls_destroy
+  struct Ckpt {
+    void *f = nullptr, *ch = nullptr;
+    int64_t ndrift = 0, step = 0;
+    double time = 0;
+  };
+  std::vector<Ckpt> adj_ck;
+  Ckpt adj_final;
+  int64_t adj_n = 0;
+  int adj_K = 0;
+  bool adj_ready = false;
+  std::vector<void *> adj_allocs;
 };
 
 static std::string g_create_error;
@@ -468,6 +482,8 @@ static void free_all(vls_handle *h) {
   h->evpool.clear();
   for (void *p : h->allocs) cudaFree(p);
   h->allocs.clear();
+  for (void *p : h->adj_allocs) cudaFree(p);
+  h->adj_allocs.clear();
   for (int k = 0; k < 8; k++) {
     if (h->bst[k]) cudaStreamDestroy(h->bst[k]);
     if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
@@ -1346,4 +1362,195 @@ extern "C" int vls_read_ndfield(vls_handle *h, const char *path) {
     return fail(h, VLS_EIO, "truncated NDfield data");
   CK(h, cudaSetDevice(h->solver.device));
   return put_f(h, f.data());
+}
+
+// ------------------------------------------------------------------ adjoint
+// Reverse-mode derivative of N linked steps (vls_adjoint.cu holds the
+// transposed kernels).  vls_adjoint_forward runs the steps and keeps a copy
+// of the state every K steps; vls_adjoint_backward walks the segments
+// backwards, recomputes each segment's states from its checkpoint, and
+// applies the transposed step to the adjoint field from the last step to the
+// first.  Memory: ceil(N/K) + 1 checkpoints and K states of f, plus six FP64
+// arrays of about one grid each.
+static void adj_release(vls_handle *h) {
+  for (void *p : h->adj_allocs) cudaFree(p);
+  h->adj_allocs.clear();
+  h->adj_ck.clear();
+  h->adj_final = vls_handle::Ckpt();
+  h->adj_ready = false;
+}
+
+template <typename P>
+static int adj_alloc(vls_handle *h, P **p, size_t bytes) {
+  void *q = nullptr;
+  if (bytes == 0) bytes = 16;
+  const cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, VLS_ECUDA,
+                "adjoint: cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                    cudaGetErrorString(e));
+  }
+  h->adj_allocs.push_back(q);
+  *p = reinterpret_cast<P *>(q);
+  return VLS_OK;
+}
+
+static int ckpt_save(vls_handle *h, vls_handle::Ckpt &c) {
+  const size_t fb = h->esize * h->cells, cb = h->esize * (size_t)h->nel;
+  if (!c.f) {
+    TRY(adj_alloc(h, &c.f, fb));
+    TRY(adj_alloc(h, &c.ch, cb));
+  }
+  CK(h, cudaMemcpyAsync(c.f, h->f, fb, cudaMemcpyDeviceToDevice, h->st));
+  if (cb) CK(h, cudaMemcpyAsync(c.ch, h->ch_val, cb, cudaMemcpyDeviceToDevice, h->st));
+  c.ndrift = h->ndrift;
+  c.time = h->time;
+  c.step = h->step;
+  return VLS_OK;
+}
+
+static int ckpt_load(vls_handle *h, const vls_handle::Ckpt &c) {
+  const size_t fb = h->esize * h->cells, cb = h->esize * (size_t)h->nel;
+  CK(h, cudaMemcpyAsync(h->f, c.f, fb, cudaMemcpyDeviceToDevice, h->st));
+  if (cb) CK(h, cudaMemcpyAsync(h->ch_val, c.ch, cb, cudaMemcpyDeviceToDevice, h->st));
+  h->ndrift = c.ndrift;
+  h->time = c.time;
+  h->step = c.step;
+  h->moments_valid = false;
+  return VLS_OK;
+}
+
+extern "C" int vls_adjoint_forward(vls_handle *h, int32_t nsteps, int32_t checkpoint_every) {
+  if (!h) return VLS_EINVAL;
+  if (nsteps < 1 || checkpoint_every < 1)
+    return fail(h, VLS_EINVAL, "adjoint: nsteps and checkpoint_every must be >= 1");
+  if (h->solver.noLinking)
+    return fail(h, VLS_EINVAL, "adjoint: only the linked step (noLinking = false) is supported");
+  if (!h->have_f) return fail(h, VLS_ESTATE, "adjoint: the grid was not set");
+  CK(h, cudaSetDevice(h->solver.device));
+  CK(h, cudaStreamSynchronize(h->st));
+  adj_release(h);
+  const int ncp = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  h->adj_ck.assign(ncp, vls_handle::Ckpt());
+  for (int s = 0; s < nsteps; ++s) {
+    if (s % checkpoint_every == 0) TRY(ckpt_save(h, h->adj_ck[s / checkpoint_every]));
+    TRY(vls_step(h, 1));
+  }
+  TRY(ckpt_save(h, h->adj_final));
+  h->adj_n = nsteps;
+  h->adj_K = checkpoint_every;
+  h->adj_ready = true;
+  return VLS_OK;
+}
+
+namespace {
+struct AdjBufs {
+  double *lam, *Cb, *Gb, *A, *B, *ringb, *sbar, *beta;
+  std::vector<void *> stash;
+  std::vector<int64_t> ndrift;
+};
+}  // namespace
+
+template <typename T>
+static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift) {
+  const Geometry g = geometry(h);
+  const MomentTables mt = moment_tables(h);
+  const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
+  const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
+  // the shift of this step, from f_n
+  CK(h, launch_moment<T>((const T *)fn, mt, h->partial, g, h->st));
+  CK(h, launch_scan(h->partial, mt, h->T2, h->bins, h->Mr, h->shift, h->mtot, h->count, g,
+                    h->st));
+  const size_t cbn = (size_t)g.nj * (g.nu + 3) * g.pc;
+  CK(h, cudaMemsetAsync(b.Cb, 0, cbn * sizeof(double), h->st));
+  CK(h, launch_drift_adj<T>(b.lam, b.Cb, h->idx, (const T *)h->fx, (const T *)h->fy, h->fp2,
+                            h->ch_start, h->ch_len, b.ringb, ndrift, g, h->st));
+  CK(h, launch_tails_adj(b.Cb, b.ringb, h->ch_start, h->ch_len, h->t_idx, h->t_x, h->t_y,
+                         h->nch, ndrift, g, h->st));
+  CK(h, launch_prer_adj(b.Cb, b.Gb, g, tr, h->st));
+  CK(h, launch_ucol_adj<T>((const T *)fn, b.Gb, b.A, b.B, b.lam, b.sbar, h->shift, g, tu,
+                           h->st));
+  CK(h, launch_shift_adj(b.sbar, b.beta, mt, g, h->st));
+  CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
+  h->launches += 9;
+  return VLS_OK;
+}
+
+template <typename T>
+static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0,
+                                 double *dchain0) {
+  const Geometry g = geometry(h);
+  const MomentTables mt = moment_tables(h);
+  const size_t cells = h->cells;
+  const size_t gn = (size_t)g.nj * (g.nu + 2) * g.nr;
+  AdjBufs b{};
+  TRY(adj_alloc(h, &b.lam, cells * sizeof(double)));
+  TRY(adj_alloc(h, &b.Cb, (size_t)g.nj * (g.nu + 3) * g.pc * sizeof(double)));
+  TRY(adj_alloc(h, &b.Gb, gn * sizeof(double)));
+  TRY(adj_alloc(h, &b.A, gn * sizeof(double)));
+  TRY(adj_alloc(h, &b.B, gn * sizeof(double)));
+  TRY(adj_alloc(h, &b.ringb, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double)));
+  TRY(adj_alloc(h, &b.sbar, (size_t)g.nj * g.nr * sizeof(double)));
+  TRY(adj_alloc(h, &b.beta, (size_t)g.nr * sizeof(double)));
+  const int K = h->adj_K;
+  b.stash.assign(K, nullptr);
+  for (int k = 0; k < K; ++k) TRY(adj_alloc(h, &b.stash[k], h->esize * cells));
+  b.ndrift.assign(K, 0);
+  // seed: the derivative of the loss with respect to the final radial bins
+  TRY(upload(h, b.beta, dbins, (size_t)g.nr * sizeof(double)));
+  CK(h, cudaMemsetAsync(b.lam, 0, cells * sizeof(double), h->st));
+  CK(h, cudaMemsetAsync(b.ringb, 0, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double), h->st));
+  CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
+  const int ncp = (int)h->adj_ck.size();
+  for (int seg = ncp - 1; seg >= 0; --seg) {
+    const int64_t n0 = (int64_t)seg * K;
+    const int64_t n1 = std::min<int64_t>(n0 + K, h->adj_n);
+    TRY(ckpt_load(h, h->adj_ck[seg]));
+    for (int64_t n = n0; n < n1; ++n) {
+      CK(h, cudaMemcpyAsync(b.stash[n - n0], h->f, h->esize * cells, cudaMemcpyDeviceToDevice,
+                            h->st));
+      b.ndrift[n - n0] = h->ndrift;
+      if (n + 1 < n1) TRY(vls_step(h, 1));
+    }
+    for (int64_t n = n1 - 1; n >= n0; --n) TRY(adj_step<T>(h, b, b.stash[n - n0], b.ndrift[n - n0]));
+  }
+  // results: the derivative with respect to the initial grid and the initial
+  // chain values (logical ring order at the first step)
+  CK(h, cudaMemcpyAsync(df0, b.lam, cells * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  std::vector<double> rb((size_t)h->nel);
+  if (h->nel)
+    CK(h, cudaMemcpyAsync(rb.data(), b.ringb, rb.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  if (dchain0) {
+    const int64_t nd0 = h->adj_ck[0].ndrift;
+    for (int64_t c = 0; c < h->nch; ++c) {
+      const int64_t s0 = h->ch_start_h[c];
+      const int32_t L = h->ch_len_h[c];
+      for (int32_t e = 0; e < L; e++) dchain0[s0 + e] = rb[s0 + (nd0 + e) % L];
+    }
+  }
+  // back to the final state of the forward run
+  TRY(ckpt_load(h, h->adj_final));
+  // the stash and adjoint arrays go; the checkpoints stay for another seed
+  const size_t keep = 2 * (h->adj_ck.size() + 1);
+  for (size_t i = keep; i < h->adj_allocs.size(); ++i) cudaFree(h->adj_allocs[i]);
+  h->adj_allocs.resize(keep);
+  CK(h, cudaGetLastError());
+  return VLS_OK;
+}
+
+extern "C" int vls_adjoint_backward(vls_handle *h, const double *dbins, int64_t nbins,
+                                    double *df0, size_t ncells, double *dchain0,
+                                    int64_t nelems) {
+  if (!h || !dbins || !df0) return VLS_EINVAL;
+  if (!h->adj_ready) return fail(h, VLS_ESTATE, "adjoint: run vls_adjoint_forward first");
+  if (nbins != h->co.nr || ncells != h->cells || (dchain0 && nelems != h->nel))
+    return fail(h, VLS_EINVAL, "adjoint: buffer sizes do not match the grid");
+  CK(h, cudaSetDevice(h->solver.device));
+  const int rc = h->esize == 8 ? adjoint_backward_impl<double>(h, dbins, df0, dchain0)
+                               : adjoint_backward_impl<float>(h, dbins, df0, dchain0);
+  if (rc != VLS_OK) return rc;
+  return check_device_flags(h);
 }

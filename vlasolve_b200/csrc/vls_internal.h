@@ -128,6 +128,27 @@ cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *s
 template <typename T, typename R>
 cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
                            cudaStream_t st);
+// adjoint of the step (vls_adjoint.cu); all adjoint arrays FP64: Cb in C
+// layout and Gb, A, B in G layout, each over all J slices
+template <typename T>
+cudaError_t launch_drift_adj(const double *lam, double *Cb, const int32_t *idx, const T *fx,
+                             const T *fy, const uint2 *fp2, const int64_t *ch_start,
+                             const int32_t *ch_len, double *ringb, int64_t ndrift,
+                             const Geometry &g, cudaStream_t st);
+cudaError_t launch_tails_adj(double *Cb, double *ringb, const int64_t *ch_start,
+                             const int32_t *ch_len, const int32_t *t_idx, const double *t_x,
+                             const double *t_y, int64_t nch, int64_t ndrift, const Geometry &g,
+                             cudaStream_t st);
+cudaError_t launch_prer_adj(const double *Cb, double *Gb, const Geometry &g,
+                            const DirTables &tr, cudaStream_t st);
+template <typename T>
+cudaError_t launch_ucol_adj(const T *f, double *Gb, double *A, double *B, double *lam,
+                            double *sbar, const double *shift, const Geometry &g,
+                            const DirTables &tu, cudaStream_t st);
+cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTables &mt,
+                             const Geometry &g, cudaStream_t st);
+cudaError_t launch_moment_adj(double *lam, const double *beta, const MomentTables &mt,
+                              const Geometry &g, cudaStream_t st);
 template <typename T>
 cudaError_t launch_moment(const T *f, const MomentTables &mt, double *partial,
                           const Geometry &g, cudaStream_t st);

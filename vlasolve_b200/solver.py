@@ -338,11 +338,56 @@ class VlasovSolver21Spline:
         self._ck(self._L.vls_get_time(self._h, ctypes.byref(t), ctypes.byref(s)))
         return t.value
 
+    def set_time(self, time: float, step: int = 0):
+        self._ck(self._L.vls_set_time(self._h, float(time), int(step)))
+
     @property
     def stepCount(self):
         t, s = ctypes.c_double(), ctypes.c_int64()
         self._ck(self._L.vls_get_time(self._h, ctypes.byref(t), ctypes.byref(s)))
         return s.value
+
+    def shell_volumes(self) -> np.ndarray:
+        """(4 pi / 3)(R_{r+1}^3 - R_r^3) for the N_r - 1 radial shells."""
+        R = self.coords()[0]
+        return (4.0 * np.pi / 3.0) * (R[1:] ** 3 - R[:-1] ** 3)
+
+    def radial_density(self) -> np.ndarray:
+        """Mass of each radial shell (the moment's bins) over its volume; the
+        last bin, of zero width, is dropped."""
+        bins = self.moments()[0]
+        return bins[:-1] / self.shell_volumes()
+
+    # -- adjoint --------------------------------------------------------------
+    def adjoint_forward(self, nsteps: int, checkpoint_every: int):
+        """Runs nsteps steps keeping a state every checkpoint_every steps
+        (vls_adjoint_forward)."""
+        self._ck(self._L.vls_adjoint_forward(self._h, int(nsteps), int(checkpoint_every)))
+
+    def adjoint_backward(self, dbins):
+        """dL/dbins of the final radial bins -> (dL/df0 [j][u][r], dL/dchain0)
+        for the initial grid and initial chain values (vls_adjoint_backward)."""
+        db = np.ascontiguousarray(dbins, dtype=np.float64)
+        df0 = np.empty(self.shape)
+        nc, ne = ctypes.c_int64(), ctypes.c_int64()
+        self._ck(self._L.vls_get_chains(self._h, ctypes.byref(nc), ctypes.byref(ne),
+                                        None, None, None, None, None, None))
+        dch = np.empty(ne.value)
+        self._ck(self._L.vls_adjoint_backward(
+            self._h, _dptr(db), db.size, _dptr(df0), df0.size,
+            _dptr(dch) if ne.value else None, ne.value))
+        return df0, dch
+
+    def set_init_params(self, **kw):
+        """Changes init.* parameters (R0, alpha, smoothingRadius, M, eta, n, Ra)
+        and regenerates the initial state."""
+        for k, v in kw.items():
+            if not hasattr(self._init_desc, k):
+                raise KeyError(k)
+            setattr(self._init_desc, k, v)
+            if k == "R0":
+                self._init_desc.R0_given = 1
+        self.init_profile()
 
     # -- output ---------------------------------------------------------------
     def snapshot(self, fname: str | None = None):
