@@ -324,9 +324,110 @@ def gpu_arm(args):
                                            for k, x in res[p]["prof"].items()}}
     if "fp64" in line:
         line["fp32_over_fp64"] = value / line["fp64"]["value"]
+    if world == 1 and not args.no_accuracy:
+        line["accuracy"] = accuracy_block(args.accuracy_steps)
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_block(args.adjoint_steps, args.adjoint_every)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# accuracy run: Plummer M=1, a=1 on 257 x 257 x 128, dt = 0.005, 2000 steps
+ACCURACY = dict(type="Plummer", Pmin=0.01, Pmax=25.0, Pres=256, Pscale="logarithmic",
+                Umin=(-3.0, 0.0), Umax=(3.0, 2.0), Ures=(256, 128),
+                Uscale=("linear", "quadratic"), dt=0.005)
+# adjoint run: UDF theta = (R0, alpha, smoothingRadius) = (2, 0.5, 0.5) on
+# 257 x 257 x 128, 500 steps at dt = 0.005, a checkpoint every 50 steps
+ADJOINT = dict(type="UDF", Pmin=0.01, Pmax=25.0, Pres=256, Pscale="logarithmic",
+               Umin=(-2.0, 0.0), Umax=(2.0, 1.6), Ures=(256, 128),
+               Uscale=("linear", "quadratic"), dt=0.005)
+
+
+def accuracy_block(steps):
+    """Mass and energy drift of each precision over `steps` steps, and the L2
+    distance of the FP32 modes' final f from the FP64 path's (the FP64 path
+    matches the oracle to 1e-12 per step)."""
+    import numpy as np
+    from vlasolve_b200 import VlasovSolver21Spline
+    out, f64 = {}, None
+    t0 = time.perf_counter()
+    for prec in ("fp64", "fp32", "fp32all"):
+        s = VlasovSolver21Spline(ACCURACY, precision=prec)
+        a = s.stats()
+        s.step(steps)
+        b = s.stats()
+        f = s.f
+        if prec == "fp64":
+            f64 = f
+        out[prec] = {"mass_drift": (b["Mass"] - a["Mass"]) / a["Mass"],
+                     "energy_drift": (b["E"] - a["E"]) / abs(a["E"])}
+        if prec != "fp64":
+            out[prec]["l2_vs_fp64"] = float(np.linalg.norm(f - f64) / np.linalg.norm(f64))
+            out[prec]["energy_drift_minus_fp64"] = (out[prec]["energy_drift"]
+                                                    - out["fp64"]["energy_drift"])
+        s.close()
+    return {"workload": "plummer_257x257x128", "steps": steps, "dt": ACCURACY["dt"],
+            "reference": "FP64 GPU path", "seconds": time.perf_counter() - t0, **out}
+
+
+def adjoint_block(nsteps, K):
+    """Config of the adjoint: loss ||rho(theta) - rho(theta + dtheta)||_2 of the
+    final radial density; gradient by the adjoint (FP64 and FP32 storage)
+    against central differences of full FP64 runs (h = 1e-4); backward time
+    over the plain forward time of the same steps."""
+    import numpy as np
+    import torch
+    from vlasolve_b200 import VlasovSolver21Spline
+    from vlasolve_b200.adjoint import DensityProblem, final_density
+    theta = np.array([2.0, 0.5, 0.5])
+    dtheta = np.array([0.05, -0.02, 0.03])
+    out = {"workload": "udf_257x257x128", "steps": nsteps, "checkpoint_every": K,
+           "theta": theta.tolist(), "loss": "||rho - rho_target||_2, rho_target at theta + "
+           + str(dtheta.tolist())}
+    t_all = time.perf_counter()
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        p = DensityProblem(ADJOINT, precision=prec, nsteps=nsteps, checkpoint_every=K)
+        target = p.run(theta + dtheta) if prec == "fp64" else target
+        th = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rho = final_density(th, p)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        L = torch.linalg.norm(rho - torch.as_tensor(target))
+        L.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        grads[prec] = th.grad.numpy().copy()
+        # plain forward of the same steps
+        s = p.solver
+        s.set_init_params(**dict(zip(p.params, map(float, theta))))
+        s.sync()
+        t3 = time.perf_counter()
+        s.step(nsteps)
+        s.sync()
+        t4 = time.perf_counter()
+        out[prec] = {"grad": grads[prec].tolist(), "loss": float(L.detach()),
+                     "forward_checkpointed_s": t1 - t0, "backward_s": t2 - t1,
+                     "forward_s": t4 - t3, "adjoint_over_forward": (t2 - t1) / (t4 - t3)}
+        if prec == "fp64":
+            fd = np.zeros(3)
+            h = 1e-4
+            for k in range(3):
+                tp, tm = theta.copy(), theta.copy()
+                tp[k] += h
+                tm[k] -= h
+                fd[k] = (np.linalg.norm(p.run(tp) - target)
+                         - np.linalg.norm(p.run(tm) - target)) / (2 * h)
+            out["fd_grad"] = fd.tolist()
+            out["fp64_vs_fd_rel"] = float(np.max(np.abs(grads["fp64"] - fd)) / np.max(np.abs(fd)))
+        p.solver.close()
+    out["fp32_vs_fp64_rel"] = float(np.max(np.abs(grads["fp32"] - grads["fp64"]))
+                                    / np.max(np.abs(grads["fp64"])))
+    out["seconds"] = time.perf_counter() - t_all
+    return out
 
 
 def reference_arm(args):
@@ -367,6 +468,13 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-max-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the 2000-step drift comparison of the precisions")
+    ap.add_argument("--accuracy-steps", type=int, default=2000)
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint gradient check and timing")
+    ap.add_argument("--adjoint-steps", type=int, default=500)
+    ap.add_argument("--adjoint-every", type=int, default=50)
     ap.add_argument("--kernels", action="store_true",
                     help="with --quick: also report per-kernel event times")
     ap.add_argument("--quick", action="store_true",

@@ -101,3 +101,18 @@ def test_adjoint_rejects_nolinking_and_missing_forward():
     s2 = VlasovSolver21Spline(cfg())
     with pytest.raises(VlsError):
         s2.adjoint_backward(np.zeros(s2.nr))
+
+
+def test_reinitialising_a_stepped_handle_restores_the_initial_state():
+    """vls_init_profile after steps gives the same grid and chain values as
+    on a fresh handle (the ring position restarts first)."""
+    from vlasolve_b200 import VlasovSolver21Spline
+    fresh = VlasovSolver21Spline(cfg())
+    s = VlasovSolver21Spline(cfg())
+    s.step(7)
+    s.init_profile()
+    np.testing.assert_array_equal(s.f, fresh.f)
+    np.testing.assert_array_equal(s.chains()["val"], fresh.chains()["val"])
+    s.step(3)
+    fresh.step(3)
+    np.testing.assert_array_equal(s.f, fresh.f)

@@ -41,10 +41,11 @@ __device__ __forceinline__ void kick_weights(double fr, double w[4], double dw[4
 
 // forward natural-BC solve of a line (FP64): x at xs[(k-1)*xst], k = 1..N;
 // coefficients c_0..c_{M-1} to cs[k*cst] (may not alias xs)
-__device__ void solve_line_fwd(const double *x, int xst, double *c, int cst,
-                               const DirTables &t) {
+__device__ void solve_line_fwd(const double *__restrict__ x, int xst, double *__restrict__ c,
+                               int cst, const DirTables &t) {
   const int M = t.M, N = M - 2;
   double d = 0.0, dprev = 0.0;
+#pragma unroll 8
   for (int k = 1; k <= N; ++k) {
     dprev = d;
     d = (x[(size_t)(k - 1) * xst] - d * (1.0 / 6.0)) * t.rp[k];
@@ -53,6 +54,7 @@ __device__ void solve_line_fwd(const double *x, int xst, double *c, int cst,
   double cc = ((0.0 - t.hi2 * dprev) - t.L1 * d) / t.L2;
   c[(size_t)(M - 1) * cst] = cc;
   double cn = cc;
+#pragma unroll 8
   for (int k = N; k >= 1; --k) {
     const double v = c[(size_t)k * cst] - t.q[k] * cn;
     c[(size_t)k * cst] = v;
@@ -65,14 +67,15 @@ __device__ void solve_line_fwd(const double *x, int xst, double *c, int cst,
 
 // transposed solve: cbar[k*cst] (k = 0..M-1) -> xbar[(k-1)*xst] (k = 1..N);
 // xbar may alias neither cbar's storage nor overlap it
-__device__ void solve_line_adj(const double *cb, int cst, double *xb, int xst,
-                               const DirTables &t) {
+__device__ void solve_line_adj(const double *__restrict__ cb, int cst, double *__restrict__ xb,
+                               int xst, const DirTables &t) {
   const int M = t.M, N = M - 2;
   const double c0b = cb[0];
   // back-substitution and first row, transposed (ascending): e_k = cbar_k
   // complete, dbar_k = e_k
   double e = cb[(size_t)1 * cst] - t.a01 * c0b;
   xb[0] = e;
+#pragma unroll 8
   for (int k = 2; k <= N; ++k) {
     double ck = cb[(size_t)k * cst];
     if (k == 2) ck -= t.a02 * c0b;
@@ -87,6 +90,7 @@ __device__ void solve_line_adj(const double *cb, int cst, double *xb, int xst,
   // forward elimination, transposed (descending)
   double fk = xb[(size_t)(N - 1) * xst];
   xb[(size_t)(N - 1) * xst] = t.rp[N] * fk;
+#pragma unroll 8
   for (int k = N - 1; k >= 1; --k) {
     fk = xb[(size_t)(k - 1) * xst] - (1.0 / 6.0) * t.rp[k + 1] * fk;
     xb[(size_t)(k - 1) * xst] = t.rp[k] * fk;
@@ -268,15 +272,23 @@ __global__ void ucol_adj_kernel(const T *__restrict__ f, double *__restrict__ Gb
 }
 
 // shift, transposed: sbar (per slice) -> beta_r' = sum_{r > r'} Rcoef_r sum_j sbar[j][r]
+// (one block: the slice sums in parallel, the N_r-long reverse scan in one
+// thread)
 __global__ void shift_adj_kernel(const double *__restrict__ sbar, double *__restrict__ beta,
                                  MomentTables mt, Geometry g) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double acc = 0.0;
-  for (int r = g.nr - 1; r >= 0; --r) {
-    beta[r] = acc;  // exclusive: bins_r' enters s_r for r > r'
+  extern __shared__ double ssum[];
+  for (int r = threadIdx.x; r < g.nr; r += blockDim.x) {
     double s = 0.0;
     for (int j = 0; j < g.nj; ++j) s += sbar[(size_t)j * g.nr + r];
-    acc += s * mt.Rcoef[r];
+    ssum[r] = s * mt.Rcoef[r];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double acc = 0.0;
+    for (int r = g.nr - 1; r >= 0; --r) {
+      beta[r] = acc;  // exclusive: bins_r' enters s_r for r > r'
+      acc += ssum[r];
+    }
   }
 }
 
@@ -344,7 +356,7 @@ cudaError_t launch_ucol_adj(const T *f, double *Gb, double *A, double *B, double
 
 cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTables &mt,
                              const Geometry &g, cudaStream_t st) {
-  shift_adj_kernel<<<1, 32, 0, st>>>(sbar, beta, mt, g);
+  shift_adj_kernel<<<1, 256, (size_t)g.nr * sizeof(double), st>>>(sbar, beta, mt, g);
   return cudaGetLastError();
 }
 

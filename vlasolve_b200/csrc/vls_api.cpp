@@ -825,8 +825,10 @@ extern "C" int vls_init_profile(vls_handle *h, const vls_init_desc *init,
     for (auto &v : vals) v *= fac;
   }
   TRY(put_f(h, f.data()));
-  TRY(vls_set_chain_values(h, vals.data(), h->nel));
+  // the ring position restarts before the values are placed (they are given
+  // in logical order, front first)
   h->ndrift = 0;
+  TRY(vls_set_chain_values(h, vals.data(), h->nel));
   return VLS_OK;
 }
 

@@ -49,6 +49,19 @@ __device__ __forceinline__ T bv1(T x) {
   return T(1) + T(3) * x + T(3) * x * x - T(3) * x * x * x;
 }
 
+// s / 36 without the bias of a rounded 1/36 factor: in FP32 the constant is
+// split in two floats (hi + lo = 1/36 to 1e-17), so the product carries only
+// the final rounding.  A biased factor would scale every drifted value the
+// same way in every step and show up as a steady mass drift.
+template <typename T>
+__device__ __forceinline__ T over36(T s) {
+  return s * (T(1) / T(36));
+}
+template <>
+__device__ __forceinline__ float over36<float>(float s) {
+  return __fmaf_rn(s, 0.02777777798473835f, s * -2.0696057367874943e-10f);
+}
+
 // ----------------------------------------------------------- async copies
 // cp.async (LDGSTS): element-wise global -> shared copies that stay in flight
 // together; the tiles' global rows are only 4-byte aligned (r-pitch N_r).
@@ -259,9 +272,9 @@ __device__ __forceinline__ R kick_exact(const R *cb, const Geometry &g, int u,
   const double fl = floor(y);
   const R fr = (R)(y - fl);
   const int Ny = 1 + (int)fl;
-  return (R(1) / R(6)) *
-         (bv2<R>(R(1) - fr) * cb[(Ny - 1) * TW] + bv1<R>(R(1) - fr) * cb[Ny * TW] +
-          bv1<R>(fr) * cb[(Ny + 1) * TW] + bv2<R>(fr) * cb[(Ny + 2) * TW]);
+  return (bv2<R>(R(1) - fr) * cb[(Ny - 1) * TW] + bv1<R>(R(1) - fr) * cb[Ny * TW] +
+          bv1<R>(fr) * cb[(Ny + 1) * TW] + bv2<R>(fr) * cb[(Ny + 2) * TW]) /
+         R(6);
 }
 
 template <typename T, typename R, bool KICK>
@@ -314,8 +327,8 @@ __global__ void __launch_bounds__(UC_THREADS)
     const bool fast = frd > 1e-9 && frd < 1.0 - 1e-9 && fabs(qf) < 1e6;
     const int o = fast ? (int)fl : 0;
     const R fr = (R)frd;
-    const R w0 = bv2<R>(R(1) - fr) * (R(1) / R(6)), w1 = bv1<R>(R(1) - fr) * (R(1) / R(6));
-    const R w2 = bv1<R>(fr) * (R(1) / R(6)), w3 = bv2<R>(fr) * (R(1) / R(6));
+    const R w0 = bv2<R>(R(1) - fr) / R(6), w1 = bv1<R>(R(1) - fr) / R(6);
+    const R w2 = bv1<R>(fr) / R(6), w3 = bv2<R>(fr) / R(6);
     // rows with 0 < u + qf < nu - 1 are inside (strictly, as :761)
     const int ulo = fast ? (int)floor(-qf) + 1 : 0;
     const int uhi = fast ? (int)ceil((double)(g.nu - 1) - qf) - 1 : -1;
@@ -474,7 +487,7 @@ __device__ __forceinline__ T eval2d(const T *__restrict__ Cj, int pc, int rI,
   p += pc;
   const T s3 = __ldg(p) * b2xI + __ldg(p + 1) * b1xI + __ldg(p + 2) * b1x +
                __ldg(p + 3) * b2x;
-  return (T(1) / T(36)) * (bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
+  return over36<T>(bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
                            bv1<T>(y) * s2 + bv2<T>(y) * s3);
 }
 
@@ -507,7 +520,7 @@ __device__ __forceinline__ float eval2d_f32x2(const float *__restrict__ Cj, int 
   r23 = __ffma2_rn(f2(__ldg(p2 + 3), __ldg(p2 + pc + 3)), wx3, r23);
   // y weights (rows 0..3) applied pairwise, times 1/36
   const float2 acc = __ffma2_rn(r23, f2(b1.y, t3.y), __fmul2_rn(r01, f2(s3.y, a1.y)));
-  return (acc.x + acc.y) * (1.f / 36.f);
+  return over36<float>(acc.x + acc.y);
 }
 
 constexpr int DR_W = 8;  // warps per drift block
@@ -826,7 +839,7 @@ __device__ __forceinline__ T eval_window(const T *p, T x, T y) {
                p[2 * DW_COLS + 2] * b1x + p[2 * DW_COLS + 3] * b2x;
   const T s3 = p[3 * DW_COLS] * b2xI + p[3 * DW_COLS + 1] * b1xI +
                p[3 * DW_COLS + 2] * b1x + p[3 * DW_COLS + 3] * b2x;
-  return (T(1) / T(36)) * (bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
+  return over36<T>(bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
                            bv1<T>(y) * s2 + bv2<T>(y) * s3);
 }
 template <>
@@ -850,7 +863,7 @@ __device__ __forceinline__ float eval_window<float>(const float *p, float x, flo
   r23 = __ffma2_rn(f2(q[2], q[DW_COLS + 2]), wx2, r23);
   r23 = __ffma2_rn(f2(q[3], q[DW_COLS + 3]), wx3, r23);
   const float2 acc = __ffma2_rn(r23, f2(b1.y, t3.y), __fmul2_rn(r01, f2(s3.y, a1.y)));
-  return (acc.x + acc.y) * (1.f / 36.f);
+  return over36<float>(acc.x + acc.y);
 }
 
 template <typename T>
@@ -1022,7 +1035,7 @@ __device__ __forceinline__ T eval_pitch(const T *p, T x, T y) {
                p[2 * PITCH + 3] * b2x;
   const T s3 = p[3 * PITCH] * b2xI + p[3 * PITCH + 1] * b1xI + p[3 * PITCH + 2] * b1x +
                p[3 * PITCH + 3] * b2x;
-  return (T(1) / T(36)) * (bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
+  return over36<T>(bv2<T>(T(1) - y) * s0 + bv1<T>(T(1) - y) * s1 +
                            bv1<T>(y) * s2 + bv2<T>(y) * s3);
 }
 template <int PITCH>
@@ -1046,7 +1059,7 @@ __device__ __forceinline__ float eval_pitch_f32x2(const float *p, float x, float
   r23 = __ffma2_rn(f2(q[2], q[PITCH + 2]), wx2, r23);
   r23 = __ffma2_rn(f2(q[3], q[PITCH + 3]), wx3, r23);
   const float2 acc = __ffma2_rn(r23, f2(b1.y, t3.y), __fmul2_rn(r01, f2(s3.y, a1.y)));
-  return (acc.x + acc.y) * (1.f / 36.f);
+  return over36<float>(acc.x + acc.y);
 }
 template <typename T, int PITCH>
 __device__ __forceinline__ T eval_strip(const T *p, T x, T y) {

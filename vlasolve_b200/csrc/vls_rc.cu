@@ -281,8 +281,10 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
       if (fast) {
         const int o = (int)fl;
         const T fr = (T)frd;
-        const T w0 = w_bv2<T>(T(1) - fr) * (T(1) / T(6)), w1 = w_bv1<T>(T(1) - fr) * (T(1) / T(6));
-        const T w2 = w_bv1<T>(fr) * (T(1) / T(6)), w3 = w_bv2<T>(fr) * (T(1) / T(6));
+        // weights divided by 6 (a rounded 1/6 factor would bias every kick
+        // the same way, a steady mass drift in FP32)
+        const T w0 = w_bv2<T>(T(1) - fr) / T(6), w1 = w_bv1<T>(T(1) - fr) / T(6);
+        const T w2 = w_bv1<T>(fr) / T(6), w3 = w_bv2<T>(fr) / T(6);
         const int ulo = (int)floor(-qf) + 1;
         const int uhi = (int)ceil((double)(N - 1) - qf) - 1;
         // row k = kfirst + i (u = k - 1) reads coefficient rows k+o-1 .. k+o+2
@@ -311,8 +313,9 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
               const T fr = (T)(y - yf);
               const int Ny = 1 + (int)yf;
               const T *p = kb + (ptrdiff_t)(Ny - 1) * LN + ro.ln;
-              x = (R)((T(1) / T(6)) * (w_bv2<T>(T(1) - fr) * p[0] + w_bv1<T>(T(1) - fr) * p[LN] +
-                                       w_bv1<T>(fr) * p[2 * LN] + w_bv2<T>(fr) * p[3 * LN]));
+              x = (R)((w_bv2<T>(T(1) - fr) * p[0] + w_bv1<T>(T(1) - fr) * p[LN] +
+                       w_bv1<T>(fr) * p[2 * LN] + w_bv2<T>(fr) * p[3 * LN]) /
+                      T(6));
             }
           }
           v[i] = x;
