@@ -201,6 +201,26 @@ int vls_write_ndfield(vls_handle *h, const char *path);
    vls_write_ndfield into f (dims and datatype are checked) */
 int vls_read_ndfield(vls_handle *h, const char *path);
 
+/* .vls restart files in the reference's layout (vlasovSolver::write and the
+   sections it calls: vlasovSolver.hxx:272-287, grid_handler.hxx:325-347,
+   grid_base.hxx:123-153 and :492-497, grid_21.hxx:85-91,
+   vlasovSolver21.hxx:568-583, sphericalKernel.hxx:88-106,
+   vlasovSolver21_spline.hxx:437-444), so that the reference's -reload reads
+   ours and vls_read_restart reads the reference's.  The grid is written in
+   FP64 whatever the precision.  snapshot_every, restart_every and
+   stats_every are the solverParam fields the file carries.
+   vls_restart_info reads a file's grid and solver parameters (so a caller can
+   create a matching handle first; the J minimum is not stored in the file
+   and is returned as 0), the three intervals, the time and the step count.
+   vls_read_restart loads the grid, the chain values, the time and the step
+   count into a handle whose grid, dt, G, noLinking, kernel type and kernel
+   buffer size match the file's. */
+int vls_write_restart(vls_handle *h, const char *path, int64_t snapshot_every,
+                      int64_t restart_every, int64_t stats_every);
+int vls_restart_info(const char *path, vls_grid_desc *grid, vls_solver_desc *solver,
+                     int64_t *every, double *time, int64_t *step);
+int vls_read_restart(vls_handle *h, const char *path);
+
 /* Adjoint of the linked step (the reference has no derivative code).
    vls_adjoint_forward runs nsteps steps from the current state (as vls_step)
    and keeps a device copy of the state every checkpoint_every steps.

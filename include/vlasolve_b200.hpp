@@ -86,12 +86,13 @@ inline vls_init_desc default_init() {
 // The spherical split semi-Lagrangian solver on one GPU.
 class vlasovSolver21_spline {
  public:
+  // init == nullptr leaves the grid unset (for readRestart)
   vlasovSolver21_spline(const vls_grid_desc &g, const vls_solver_desc &s,
-                        const vls_init_desc &init)
+                        const vls_init_desc *init)
       : solver_(s) {
     check(vls_create(&g, &s, &h_), nullptr);
     try {
-      check(vls_init_profile(h_, &init, &mass_before_), h_);
+      if (init) check(vls_init_profile(h_, init, &mass_before_), h_);
       int64_t nr, nu, nj;
       check(vls_dims(h_, &nr, &nu, &nj), h_);
       nr_ = nr;
@@ -103,6 +104,9 @@ class vlasovSolver21_spline {
     }
   }
   ~vlasovSolver21_spline() { vls_destroy(h_); }
+  vlasovSolver21_spline(const vls_grid_desc &g, const vls_solver_desc &s,
+                        const vls_init_desc &init)
+      : vlasovSolver21_spline(g, s, &init) {}
   vlasovSolver21_spline(const vlasovSolver21_spline &) = delete;
   vlasovSolver21_spline &operator=(const vlasovSolver21_spline &) = delete;
 
@@ -111,10 +115,13 @@ class vlasovSolver21_spline {
   void steps(int n) { check(vls_step(h_, n), h_); }
   void sync() { check(vls_sync(h_), h_); }
 
-  // vlasovSolver::run (vlasovSolver.hxx:134-190) without restart dumps:
-  // statistics every statsEvery steps (row appended to `stats`), snapshots
-  // every snapshotEvery steps (snapshot_%4.4f.ND)
-  void run(long statsEvery, long snapshotEvery, const char *stats = "statistics.txt") {
+  // vlasovSolver::run (vlasovSolver.hxx:134-190): restart files every
+  // restartEvery steps (restart_%.4f.vls), statistics every statsEvery steps
+  // (row appended to `stats`), snapshots every snapshotEvery steps
+  // (snapshot_%4.4f.ND); afterRunning (:235-246): a last snapshot when the
+  // step count is a multiple of snapshotEvery, and final_%.4f.vls
+  void run(long statsEvery, long snapshotEvery, const char *stats = "statistics.txt",
+           long restartEvery = -1, bool finalDump = false) {
     auto timer = [](long every, long n) { return every >= 0 && (n % every) == 0; };
     auto checkTime = [&]() {
       double t;
@@ -124,15 +131,36 @@ class vlasovSolver21_spline {
              (t < solver_.Tmax && std::abs(t - solver_.Tmax) > solver_.dt / 100);
     };
     if (!checkTime()) return;
+    char buf[64];
     do {
       double t;
       int64_t n;
       vls_get_time(h_, &t, &n);
+      if (timer(restartEvery, n)) {
+        std::snprintf(buf, sizeof(buf), "restart_%.4f.vls", t);
+        writeRestart(buf, snapshotEvery, restartEvery, statsEvery);
+      }
       if (timer(snapshotEvery, n)) snapshot();
       if (timer(statsEvery, n)) statistics(n == 0, stats);
       makeOneStep(t);
     } while (checkTime());
+    if (finalDump) {
+      double t;
+      int64_t n;
+      vls_get_time(h_, &t, &n);
+      if (timer(snapshotEvery, n)) snapshot();
+      std::snprintf(buf, sizeof(buf), "final_%.4f.vls", t);
+      writeRestart(buf, snapshotEvery, restartEvery, statsEvery);
+    }
   }
+
+  // vlasovSolver::write(fname) (vlasovSolver.hxx:248-269): the .vls file
+  void writeRestart(const char *name, long snapshotEvery, long restartEvery, long statsEvery) {
+    check(vls_write_restart(h_, name, snapshotEvery, restartEvery, statsEvery), h_);
+  }
+  // vlasovSolver::init(params, fname) (vlasovSolver.hxx:104-131): the state of
+  // a .vls file, into a solver created with the file's parameters
+  void readRestart(const char *name) { check(vls_read_restart(h_, name), h_); }
 
   // vlasovSolver21::statistics (vlasovSolver21.hxx:644-690)
   vls_stats_out statistics(bool reset = false, const char *fname = "statistics.txt") {

@@ -11,7 +11,8 @@ order) and records:
   full-size configurations, whose grids are too large to commit);
 * the ``statistics.txt`` rows;
 * the delayed-kernel chains (cell, R, U, values) from the restart file written
-  at step 0 and from the final restart file.
+  at step 0 and from the final restart file;
+* two .vls restart files of the smallest case, byte for byte (``restart``).
 
 Usage:  python tests/golden/make_golden.py [case ...]
 """
@@ -193,10 +194,36 @@ def run_case(c):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+# .vls restart files of the reference, kept byte for byte: the udf_tiny case
+# dumped after step 2 (restartEvery 2) and its final dump after step 3
+RESTART_FILES = {"restart_0.0100.vls": "udf_tiny_restart_step2.vls",
+                 "final_0.0150.vls": "udf_tiny_final_step3.vls"}
+
+
+def make_restart_fixtures():
+    tmp = tempfile.mkdtemp(prefix="vls_golden_")
+    try:
+        c = CASES[0]
+        args = [REF_BIN, "-threads_per_node", "1", "-verbose", "0"] + c["args"] + [
+            "-solver.dt", "0.005", "-solver.Tmax", "0.0125", "-solver.restartEvery", "2",
+            "-solver.statsEvery", "-1", "-solver.snapshotEvery", "-1"]
+        with open(os.path.join(tmp, "log.txt"), "w") as log:
+            subprocess.check_call(args, cwd=tmp, stdout=log, stderr=subprocess.STDOUT)
+        for src, dst in RESTART_FILES.items():
+            shutil.copyfile(os.path.join(tmp, src), os.path.join(HERE, dst))
+        return "restart", "ok"
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main(names):
     if not os.path.exists(REF_BIN):
         sys.exit("reference binary missing: run oracle/build_ref.sh first")
+    if not names or "restart" in names:
+        print(*make_restart_fixtures(), flush=True)
     todo = [c for c in CASES if not names or c["name"] in names]
+    if not todo:
+        return
     with cf.ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 1)) as ex:
         for name, st in ex.map(run_case, todo):
             print(name, st, flush=True)

@@ -34,3 +34,24 @@ def test_driver_statistics_match_reference(name, tmp_path):
     np.testing.assert_allclose(rows[:, 2:], ref[:, 2:], rtol=2e-9, atol=1e-14)
     snaps = sorted(f for f in os.listdir(tmp_path) if f.startswith("snapshot_"))
     assert snaps and snaps[0] == "snapshot_0.0000.ND"
+
+
+def test_driver_reload_continues_reference_restart(tmp_path):
+    """-reload of the reference's step-2 restart file runs to its Tmax and
+    writes final_0.0150.vls matching the reference's final dump."""
+    from conftest import GOLDEN
+    from test_gpu_restart import read_vls
+    from vlasolve_b200.build import DRIVER, build
+    build()
+    stem = os.path.join(GOLDEN, "udf_tiny_restart_step2")
+    r = subprocess.run([DRIVER, "-reload", stem], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "Reloaded" in r.stdout
+    ours = tmp_path / "final_0.0150.vls"
+    assert ours.exists()
+    f, ch = read_vls(str(ours))
+    f3, ch3 = read_vls(os.path.join(GOLDEN, "udf_tiny_final_step3.vls"))
+    scale = np.max(np.abs(f3))
+    assert np.max(np.abs(f - f3)) <= 1e-12 * scale
+    assert np.max(np.abs(ch - ch3)) <= 1e-12 * scale

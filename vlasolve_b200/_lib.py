@@ -29,7 +29,8 @@ EXPORTED = [
     "vls_moments", "vls_last_mass", "vls_stats", "vls_get_time", "vls_set_time",
     "vls_write_ndfield", "vls_read_ndfield", "vls_stream", "vls_set_profiling",
     "vls_profile_read", "vls_radial_mass_noalloc", "vls_noalloc_last_error",
-    "vls_adjoint_forward", "vls_adjoint_backward",
+    "vls_adjoint_forward", "vls_adjoint_backward", "vls_write_restart",
+    "vls_restart_info", "vls_read_restart",
 ]
 KERNEL_KINDS = ["ucol_kick", "ucol", "prer", "tails", "drift", "scan", "moment",
                 "stats", "convert"]
@@ -115,6 +116,10 @@ def load(path: str = LIB_PATH):
         "vls_stream": [H, P(ctypes.c_void_p)],
         "vls_set_profiling": [H, i32],
         "vls_profile_read": [H, P(d), P(i64), i32],
+        "vls_write_restart": [H, ctypes.c_char_p, i64, i64, i64],
+        "vls_restart_info": [ctypes.c_char_p, P(GridDesc), P(SolverDesc), P(i64), P(d),
+                             P(i64)],
+        "vls_read_restart": [H, ctypes.c_char_p],
         "vls_adjoint_forward": [H, i32, i32],
         "vls_adjoint_backward": [H, P(d), i64, P(d), ctypes.c_size_t, P(d), i64],
         "vls_radial_mass_noalloc": [ctypes.c_void_p, i32, i64, i64, i64, P(d), P(d), P(d),

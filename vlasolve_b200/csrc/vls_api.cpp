@@ -1556,3 +1556,386 @@ extern "C" int vls_adjoint_backward(vls_handle *h, const double *dbins, int64_t 
   if (rc != VLS_OK) return rc;
   return check_device_flags(h);
 }
+
+// ------------------------------------------------------------------ restart
+// .vls restart files in the reference's layout (vlasovSolver::write,
+// vlasovSolver.hxx:272-287 and the chain it calls): endianness word, tagged
+// sections (int length + characters) with 2048-byte spares, the FP64 grid
+// [j][u][r], and the delayed-kernel chains per J slice in ascending cell
+// order (its std::map order), each as length + (R, U, nVal = 1, value) per
+// element, front first.  gridBase::paramT::write writes Pmax with the count of
+// U and Umin with the count of P (grid_base.hxx:129-130), so the six doubles
+// are Pmin, Pmax, Umin[0], Umin[0], Umax[0], Umax[1]; Umin[1] (the J minimum)
+// is not in the file.
+namespace {
+const char *const TAG_SOLVER = "VLASOV_SOLVER v0.13";
+const char *const TAG_GH = "GRID_HANDLER v0.11";
+const char *const TAG_GB = "GRID_BASE v0.12";
+const char *const TAG_G21 = "GRID_21 v0.11";
+const char *const TAG_S21 = "VLASOV_SOLVER21 v0.12";
+const char *const TAG_KERNEL = "KERNEL_CELLS v0.10";
+const char *const TAG_SPLINE = "VLASOV_SOLVER21_SPLINE v0.11";
+constexpr size_t SPARE = 256 * 8;
+constexpr size_t PARAM_SPARE = SPARE - sizeof(int32_t) * (3 + 3) - sizeof(int64_t);
+
+struct Out {
+  std::vector<char> b;
+  template <typename V>
+  void put(V v) {
+    const char *p = reinterpret_cast<const char *>(&v);
+    b.insert(b.end(), p, p + sizeof(V));
+  }
+  void tag(const char *s) {
+    const int32_t n = (int32_t)std::strlen(s);
+    put(n);
+    b.insert(b.end(), s, s + n);
+  }
+  void zeros(size_t n) { b.insert(b.end(), n, 0); }
+  void param(const vls_grid_desc &g) {
+    put(g.Pmin);
+    put(g.Pmax);
+    put(g.Umin[0]);
+    put(g.Umin[0]);
+    put(g.Umax[0]);
+    put(g.Umax[1]);
+    put(g.Pres);
+    put(g.Ures[0]);
+    put(g.Ures[1]);
+    put(g.Pscale);
+    put(g.Uscale[0]);
+    put(g.Uscale[1]);
+    for (int i = 0; i < 6; ++i) put((int32_t)0);  // margins: P low/high, U low/high
+    put((int32_t)1);                               // nFields
+    put((int32_t)0);                               // haveParentGrid
+    put((int32_t)1);                               // parent_P_DIMS
+    put((int32_t)2);                               // parent_U_DIMS
+    put((int32_t)0);                               // parent_which
+    put((int32_t)1);
+    put((int32_t)2);
+    put((int64_t)0);  // minStorageSize
+    zeros(PARAM_SPARE);
+  }
+};
+
+struct In {
+  const std::vector<char> &b;
+  size_t o = 0;
+  bool swap = false, bad = false;
+  std::string why;
+  explicit In(const std::vector<char> &v) : b(v) {}
+  template <typename V>
+  V get() {
+    V v{};
+    if (o + sizeof(V) > b.size()) {
+      if (!bad) why = "file too short";
+      bad = true;
+      return v;
+    }
+    std::memcpy(&v, b.data() + o, sizeof(V));
+    o += sizeof(V);
+    if (swap) {
+      char *p = reinterpret_cast<char *>(&v);
+      std::reverse(p, p + sizeof(V));
+    }
+    return v;
+  }
+  void tag(const char *s) {
+    const int32_t n = get<int32_t>();
+    const size_t len = std::strlen(s);
+    if (bad) return;
+    if ((size_t)n != len || o + len > b.size() || std::memcmp(b.data() + o, s, len) != 0) {
+      bad = true;
+      why = std::string("tag '") + s + "' not found";
+      return;
+    }
+    o += len;
+  }
+  void skip(size_t n) {
+    if (o + n > b.size()) {
+      if (!bad) why = "file too short";
+      bad = true;
+      return;
+    }
+    o += n;
+  }
+  void param(vls_grid_desc &g) {
+    g.Pmin = get<double>();
+    g.Pmax = get<double>();
+    get<double>();  // Umin[0] (written through Pmax's count)
+    g.Umin[0] = get<double>();
+    g.Umax[0] = get<double>();
+    g.Umax[1] = get<double>();
+    g.Umin[1] = 0.0;  // not in the file
+    g.Pres = get<int32_t>();
+    g.Ures[0] = get<int32_t>();
+    g.Ures[1] = get<int32_t>();
+    g.Pscale = get<int32_t>();
+    g.Uscale[0] = get<int32_t>();
+    g.Uscale[1] = get<int32_t>();
+    for (int i = 0; i < 6; ++i) get<int32_t>();
+    const int32_t nfields = get<int32_t>();
+    if (!bad && nfields != 1) {
+      bad = true;
+      why = "only one field (species) is supported";
+    }
+    skip(sizeof(int32_t) * 6 + sizeof(int64_t) + PARAM_SPARE);
+  }
+};
+
+struct RestartHead {
+  vls_grid_desc grid{};
+  vls_solver_desc solver{};
+  int64_t every[3] = {0, 0, 0};  // snapshotEvery, restartEvery, statsEvery
+  double time = 0;
+  int64_t step = 0;
+  size_t f_offset = 0;  // byte offset of the FP64 grid
+};
+
+bool read_file(const char *path, std::vector<char> &b, std::string &why) {
+  FILE *f = std::fopen(path, "rb");
+  if (!f) {
+    why = std::string("cannot open ") + path;
+    return false;
+  }
+  std::fseek(f, 0, SEEK_END);
+  const long n = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  b.resize(n > 0 ? (size_t)n : 0);
+  const size_t got = b.empty() ? 0 : std::fread(b.data(), 1, b.size(), f);
+  std::fclose(f);
+  if (got != b.size()) {
+    why = std::string("cannot read ") + path;
+    return false;
+  }
+  return true;
+}
+
+// parses up to the grid data; `in` is left at the grid's first value
+bool parse_head(In &in, RestartHead &h) {
+  const int32_t e = in.get<int32_t>();
+  if (e != 1) {
+    in.swap = true;
+    int32_t s = e;
+    char *p = reinterpret_cast<char *>(&s);
+    std::reverse(p, p + 4);
+    if (s != 1) {
+      in.bad = true;
+      in.why = "not a restart file (endianness word)";
+      return false;
+    }
+  }
+  in.tag(TAG_SOLVER);
+  h.solver.G = in.get<double>();
+  h.solver.T0 = in.get<double>();
+  h.solver.Tmax = in.get<double>();
+  h.solver.dt = in.get<double>();
+  const int32_t nsp = in.get<int32_t>();
+  for (int k = 0; k < 3; ++k) h.every[k] = in.get<int64_t>();
+  h.time = in.get<double>();
+  const double dt2 = in.get<double>();
+  (void)dt2;  // deltaTime (equal to solverParam.dt in the reference's runs)
+  h.step = in.get<int64_t>();
+  h.solver.noLinking = in.get<int32_t>();
+  if (!in.bad && nsp != 1) {
+    in.bad = true;
+    in.why = "only one species is supported";
+  }
+  in.tag(TAG_GH);
+  in.get<int32_t>();  // endianness word of the grid handler
+  const int32_t pd = in.get<int32_t>(), ud = in.get<int32_t>(), jd = in.get<int32_t>();
+  const int64_t dsz = in.get<int64_t>(), ngrids = in.get<int64_t>();
+  in.get<int64_t>();  // rank
+  if (!in.bad && (pd != 1 || ud != 2 || jd != 1 || dsz != 8 || ngrids != 1)) {
+    in.bad = true;
+    in.why = "not a single FP64 (r, u, J) grid";
+  }
+  vls_grid_desc full{};
+  in.param(full);
+  in.tag(TAG_GB);
+  in.param(h.grid);
+  h.f_offset = in.o;
+  return !in.bad;
+}
+
+bool same_grid(const vls_grid_desc &a, const vls_grid_desc &b) {
+  return a.Pmin == b.Pmin && a.Pmax == b.Pmax && a.Pres == b.Pres && a.Pscale == b.Pscale &&
+         a.Umin[0] == b.Umin[0] && a.Umax[0] == b.Umax[0] && a.Umax[1] == b.Umax[1] &&
+         a.Ures[0] == b.Ures[0] && a.Ures[1] == b.Ures[1] && a.Uscale[0] == b.Uscale[0] &&
+         a.Uscale[1] == b.Uscale[1];
+}
+}  // namespace
+
+extern "C" int vls_write_restart(vls_handle *h, const char *path, int64_t snapshot_every,
+                                 int64_t restart_every, int64_t stats_every) {
+  if (!h || !path) return VLS_EINVAL;
+  if (!h->have_f) return fail(h, VLS_ESTATE, "vls_write_restart before the grid was set");
+  CK(h, cudaSetDevice(h->solver.device));
+  std::vector<double> f(h->cells);
+  TRY(take_f(h, f.data()));
+  int64_t nch = 0, nel = 0;
+  TRY(vls_get_chains(h, &nch, &nel, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr));
+  std::vector<double> val((size_t)nel);
+  if (nel)
+    TRY(vls_get_chains(h, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                       val.data()));
+  Out o;
+  o.b.reserve(h->cells * 8 + 32768);
+  o.put((int32_t)1);
+  o.tag(TAG_SOLVER);
+  o.put(h->solver.G);
+  o.put(h->solver.T0);
+  o.put(h->solver.Tmax);
+  o.put(h->solver.dt);
+  o.put((int32_t)1);
+  o.put(snapshot_every);
+  o.put(restart_every);
+  o.put(stats_every);
+  o.put(h->time);
+  o.put(h->solver.dt);
+  o.put((int64_t)h->step);
+  o.put((int32_t)(h->solver.noLinking ? 1 : 0));
+  o.tag(TAG_GH);
+  o.put((int32_t)1);
+  o.put((int32_t)1);
+  o.put((int32_t)2);
+  o.put((int32_t)1);
+  o.put((int64_t)sizeof(double));
+  o.put((int64_t)1);  // nGrids
+  o.put((int64_t)0);  // rank
+  o.param(h->grid);
+  o.tag(TAG_GB);
+  o.param(h->grid);
+  {
+    const char *p = reinterpret_cast<const char *>(f.data());
+    o.b.insert(o.b.end(), p, p + h->cells * sizeof(double));
+  }
+  o.tag(TAG_G21);
+  o.zeros(SPARE);
+  o.zeros(SPARE);  // grid handler
+  o.zeros(SPARE);  // vlasovSolver
+  o.tag(TAG_S21);
+  o.put((int32_t)h->solver.kernelType);
+  o.put(0.0);  // kernelMass (always 0, vlasovSolver21.hxx:535)
+  o.put((int32_t)h->solver.kernelBufferSize);
+  o.zeros(SPARE);
+  if (h->solver.kernelType == VLS_KERNEL_DELAYED) {
+    o.tag(TAG_KERNEL);
+    const int64_t nr = h->co.nr, nu = h->co.nu, nj = h->co.nj;
+    o.put(nj);
+    int64_t c = 0;
+    for (int64_t j = 0; j < nj; ++j) {
+      int64_t c1 = c;
+      while (c1 < nch && h->ch_cell_h[c1] / (nr * nu) == j) ++c1;
+      o.put(c1 - c);
+      for (; c < c1; ++c) {
+        o.put(h->ch_cell_h[c]);
+        const int64_t L = h->ch_len_h[c], s0 = h->ch_start_h[c];
+        o.put(L);
+        for (int64_t e = 0; e < L; ++e) {
+          o.put(h->ch_R_h[s0 + e]);
+          o.put(h->ch_U_h[s0 + e]);
+          o.put((int32_t)1);
+          o.put(val[s0 + e]);
+        }
+      }
+    }
+  }
+  o.tag(TAG_SPLINE);
+  o.zeros(SPARE);
+  FILE *fo = std::fopen(path, "wb");
+  if (!fo) return fail(h, VLS_EIO, std::string("cannot open ") + path + " for writing");
+  const size_t w = std::fwrite(o.b.data(), 1, o.b.size(), fo);
+  const int cl = std::fclose(fo);
+  if (w != o.b.size() || cl != 0) return fail(h, VLS_EIO, std::string("cannot write ") + path);
+  return VLS_OK;
+}
+
+extern "C" int vls_restart_info(const char *path, vls_grid_desc *grid, vls_solver_desc *solver,
+                                int64_t *every, double *time, int64_t *step) {
+  std::vector<char> b;
+  std::string why;
+  if (!path || !read_file(path, b, why)) return fail(nullptr, VLS_EIO, why);
+  In in(b);
+  RestartHead hd;
+  if (!parse_head(in, hd)) return fail(nullptr, VLS_EIO, "restart file: " + in.why);
+  // the kernel section follows the grid data and three spares
+  in.skip(sizeof(double) * (size_t)(hd.grid.Pres + 1) * (hd.grid.Ures[0] + 1) * hd.grid.Ures[1]);
+  in.tag(TAG_G21);
+  in.skip(3 * SPARE);
+  in.tag(TAG_S21);
+  hd.solver.kernelType = in.get<int32_t>();
+  in.get<double>();
+  hd.solver.kernelBufferSize = in.get<int32_t>();
+  if (in.bad) return fail(nullptr, VLS_EIO, "restart file: " + in.why);
+  hd.solver.precision = VLS_FP64;
+  hd.solver.device = 0;
+  if (grid) *grid = hd.grid;
+  if (solver) *solver = hd.solver;
+  if (every)
+    for (int k = 0; k < 3; ++k) every[k] = hd.every[k];
+  if (time) *time = hd.time;
+  if (step) *step = hd.step;
+  return VLS_OK;
+}
+
+extern "C" int vls_read_restart(vls_handle *h, const char *path) {
+  if (!h || !path) return VLS_EINVAL;
+  CK(h, cudaSetDevice(h->solver.device));
+  std::vector<char> b;
+  std::string why;
+  if (!read_file(path, b, why)) return fail(h, VLS_EIO, why);
+  In in(b);
+  RestartHead hd;
+  if (!parse_head(in, hd)) return fail(h, VLS_EIO, "restart file: " + in.why);
+  if (!same_grid(hd.grid, h->grid))
+    return fail(h, VLS_EINVAL, "restart file: its grid differs from the handle's");
+  if (hd.solver.dt != h->solver.dt || hd.solver.G != h->solver.G ||
+      (hd.solver.noLinking != 0) != (h->solver.noLinking != 0))
+    return fail(h, VLS_EINVAL, "restart file: dt, G or noLinking differ from the handle's");
+  std::vector<double> f(h->cells);
+  for (size_t i = 0; i < h->cells; ++i) f[i] = in.get<double>();
+  in.tag(TAG_G21);
+  in.skip(3 * SPARE);
+  in.tag(TAG_S21);
+  const int32_t kt = in.get<int32_t>();
+  in.get<double>();
+  const int32_t kbs = in.get<int32_t>();
+  in.skip(SPARE);
+  if (in.bad) return fail(h, VLS_EIO, "restart file: " + in.why);
+  if (kt != h->solver.kernelType || kbs != h->solver.kernelBufferSize)
+    return fail(h, VLS_EINVAL, "restart file: kernel type or buffer size differ");
+  std::vector<double> val((size_t)h->nel);
+  if (kt == VLS_KERNEL_DELAYED) {
+    in.tag(TAG_KERNEL);
+    const int64_t nr = h->co.nr, nu = h->co.nu;
+    const int64_t ns = in.get<int64_t>();
+    int64_t c = 0;
+    for (int64_t j = 0; j < ns && !in.bad; ++j) {
+      const int64_t cnt = in.get<int64_t>();
+      for (int64_t k = 0; k < cnt && !in.bad; ++k, ++c) {
+        const int64_t key = in.get<int64_t>(), L = in.get<int64_t>();
+        if (c >= h->nch || key != h->ch_cell_h[c] || key / (nr * nu) != j ||
+            L != h->ch_len_h[c])
+          return fail(h, VLS_EINVAL, "restart file: its delayed-kernel chains differ");
+        const int64_t s0 = h->ch_start_h[c];
+        for (int64_t e = 0; e < L; ++e) {
+          in.get<double>();  // R, U: the chain geometry, fixed by the grid and dt
+          in.get<double>();
+          const int32_t nv = in.get<int32_t>();
+          if (nv != 1) return fail(h, VLS_EINVAL, "restart file: chains with several values");
+          val[s0 + e] = in.get<double>();
+        }
+      }
+    }
+    if (c != h->nch) return fail(h, VLS_EINVAL, "restart file: its delayed-kernel chains differ");
+  }
+  in.tag(TAG_SPLINE);
+  if (in.bad) return fail(h, VLS_EIO, "restart file: " + in.why);
+  TRY(put_f(h, f.data()));
+  h->ndrift = 0;
+  if (h->nel) TRY(vls_set_chain_values(h, val.data(), h->nel));
+  h->time = hd.time;
+  h->step = hd.step;
+  h->moments_valid = false;
+  return VLS_OK;
+}

@@ -1106,11 +1106,15 @@ __global__ void __launch_bounds__(32 * NW, MINB)
   int ready = 0;  // boxes [0, ready) seen complete by this thread
   bool waits_ok = true;
   double acc = 0.0;
+  // footpoint words and moment weights b_u of the next PF rows in flight
   RawCell<T> q[PF];
+  double bq[PF];
 #pragma unroll
   for (int k = 0; k < PF; ++k) {
     const int u = w + NW * k;
-    q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(u < g.nu && col_ok ? u : 0) * g.nr);
+    const int uc = u < g.nu ? u : 0;
+    q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? uc : 0) * g.nr);
+    bq[k] = __ldg(mt.bu + uc);
   }
   for (int ub = w; ub < g.nu; ub += NW * PF) {
     T part = T(0);
@@ -1118,8 +1122,11 @@ __global__ void __launch_bounds__(32 * NW, MINB)
     for (int k = 0; k < PF; ++k) {
       const int u = ub + NW * k;
       const Cell<T> cl = decode(q[k]);
+      const T bu = (T)bq[k];
       const int un = u + NW * PF;
-      q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(un < g.nu && col_ok ? un : 0) * g.nr);
+      const int unc = un < g.nu ? un : 0;
+      q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? unc : 0) * g.nr);
+      bq[k] = __ldg(mt.bu + unc);
       if (u < g.nu && col_ok) {
         T v = T(0);
         if (cl.kind == 0) {
@@ -1147,7 +1154,7 @@ __global__ void __launch_bounds__(32 * NW, MINB)
           v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
         }
         f[row0 + (size_t)u * g.nr] = v;
-        part += (T)__ldg(mt.bu + u) * v;
+        part += bu * v;
       }
     }
     acc += (double)part;

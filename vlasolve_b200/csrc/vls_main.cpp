@@ -2,9 +2,10 @@
 // (vlasolve.cpp:20-55): options as -group.param v1 v2 ... and/or a parameter
 // file given as the first non-dash argument (paramsParser.hxx:134-218), the
 // initial-condition profiles UDF, PLDF, Plummer and Hernquist with their
-// default grids and solver parameters, then vlasovSolver::run
-// (vlasovSolver.hxx:134-190): statistics.txt rows, snapshot_%4.4f.ND files
-// and the "Computed N timesteps in Ts" line.  The step runs on the GPU
+// default grids and solver parameters, or -reload of a .vls restart file,
+// then vlasovSolver::run (vlasovSolver.hxx:134-190): restart_%.4f.vls files,
+// statistics.txt rows, snapshot_%4.4f.ND files, the "Computed N timesteps in
+// Ts" line and the final_%.4f.vls file.  The step runs on the GPU
 // through the C-ABI; -solver.precision fp64|fp32|fp32all selects the mode
 // (an option the reference does not have; default fp64).
 #include <chrono>
@@ -178,8 +179,9 @@ int main(int argc, char **argv) {
   const std::string prec = p.get<std::string>("solver", "precision", std::string("fp64"));
   s.precision = prec == "fp32" ? VLS_FP32_BULK : prec == "fp32all" ? VLS_FP32_ALL : VLS_FP64;
   s.device = p.get("default", "device", 0);
-  const long statsEvery = p.get("solver", "statsEvery", 25L);
-  const long snapshotEvery = p.get("solver", "snapshotEvery", 500L);
+  long statsEvery = p.get("solver", "statsEvery", 25L);
+  long snapshotEvery = p.get("solver", "snapshotEvery", 500L);
+  long restartEvery = p.get("solver", "restartEvery", 5000L);
   g.Pmin = p.get("grid", "Pmin", g.Pmin, 0);
   g.Pmax = p.get("grid", "Pmax", g.Pmax, 0);
   g.Pres = p.get("grid", "Pres", (int)g.Pres, 0);
@@ -195,13 +197,61 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "ERROR: invalid scale type\n");
     return 1;
   }
+  // -reload name: the state of name.vls (vlasolve.cpp:46-48,
+  // vlasovSolver.hxx:104-131); Tmax, dt and the output intervals may be
+  // overridden on the command line, everything else comes from the file
+  const std::string reload = p.get<std::string>("default", "reload", std::string(""));
+  if (!reload.empty()) {
+    const std::string fname = reload + ".vls";
+    vls_grid_desc rg{};
+    vls_solver_desc rs{};
+    int64_t every[3];
+    double t;
+    int64_t n;
+    if (vls_restart_info(fname.c_str(), &rg, &rs, every, &t, &n) != VLS_OK) {
+      std::fprintf(stderr, "ERROR: %s\n", vls_last_error(nullptr));
+      return 1;
+    }
+    // the J minimum is not in the file; -grid.Umin's second value or 0
+    rg.Umin[1] = p.get("grid", "Umin", 0.0, 1);
+    rs.precision = s.precision;
+    rs.device = s.device;
+    rs.Tmax = p.get("solver", "Tmax", rs.Tmax);
+    snapshotEvery = p.get("solver", "snapshotEvery", (long)every[0]);
+    restartEvery = p.get("solver", "restartEvery", (long)every[1]);
+    statsEvery = p.get("solver", "statsEvery", (long)every[2]);
+    if (p.defined("solver", "dt") && p.get("solver", "dt", rs.dt) != rs.dt) {
+      std::fprintf(stderr, "ERROR: the time step of a reloaded run is the file's (%g)\n", rs.dt);
+      return 1;
+    }
+    try {
+      vls::vlasovSolver21_spline solver(rg, rs, nullptr);
+      solver.readRestart(fname.c_str());
+      std::printf("Reloaded %s at T=%.5f (step %ld)\n", fname.c_str(), t, (long)n);
+      std::printf("Starting at T=%.5f, dt=%g, tmax = %g\n", t, rs.dt, rs.Tmax);
+      const auto t0 = std::chrono::steady_clock::now();
+      solver.run(statsEvery, snapshotEvery, "statistics.txt", restartEvery, true);
+      solver.sync();
+      const double T =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      double t1;
+      int64_t n1;
+      vls_get_time(solver.handle(), &t1, &n1);
+      std::printf("\nComputed %ld timesteps in %gs. (%3.3gs / step)\n", (long)n1, T,
+                  n1 > n ? T / (n1 - n) : 0.0);
+    } catch (const vls::error &e) {
+      std::fprintf(stderr, "ERROR (%d): %s\n", e.code(), e.what());
+      return 2;
+    }
+    return 0;
+  }
   try {
     vls::vlasovSolver21_spline solver(g, s, ini);
     std::printf("Renormalizing mass : M[0]=%g -> %g.\n", solver.massBeforeRenormalisation(),
                 ini.M);
     std::printf("Starting at T=%.5f, dt=%g, tmax = %g\n", s.T0, s.dt, s.Tmax);
     const auto t0 = std::chrono::steady_clock::now();
-    solver.run(statsEvery, snapshotEvery);
+    solver.run(statsEvery, snapshotEvery, "statistics.txt", restartEvery, true);
     solver.sync();
     const double T =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -210,7 +260,6 @@ int main(int argc, char **argv) {
     vls_get_time(solver.handle(), &t, &n);
     std::printf("\nComputed %ld timesteps in %gs. (%3.3gs / step)\n", (long)n, T,
                 n ? T / n : 0.0);
-    if (snapshotEvery >= 0 && n % snapshotEvery == 0) solver.snapshot();
   } catch (const vls::error &e) {
     std::fprintf(stderr, "ERROR (%d): %s\n", e.code(), e.what());
     return 2;

@@ -397,6 +397,18 @@ class VlasovSolver21Spline:
         self._ck(self._L.vls_write_ndfield(self._h, fname.encode()))
         return fname
 
+    def write_restart(self, fname: str, snapshot_every: int = 500, restart_every: int = 5000,
+                      stats_every: int = 25):
+        """vlasovSolver::write: the .vls restart file of the current state."""
+        self._ck(self._L.vls_write_restart(self._h, fname.encode(), int(snapshot_every),
+                                           int(restart_every), int(stats_every)))
+        return fname
+
+    def read_restart(self, fname: str):
+        """Loads the grid, chain values, time and step count of a .vls file
+        (the reference's or write_restart's) into this solver."""
+        self._ck(self._L.vls_read_restart(self._h, fname.encode()))
+
     def load_snapshot(self, fname: str):
         self._ck(self._L.vls_read_ndfield(self._h, fname.encode()))
 
@@ -437,3 +449,24 @@ class VlasovSolver21Spline:
                 break
         if check_timer(sp["snapshotEvery"], self.stepCount):
             self.snapshot(os.path.join(outdir, "snapshot_%4.4f.ND" % self.time))
+
+
+def restart_info(fname: str) -> dict:
+    """Grid and solver parameters, output intervals, time and step count stored
+    in a .vls restart file (vls_restart_info; the J minimum is not stored)."""
+    L = _lib.load()
+    g, sd = _lib.GridDesc(), _lib.SolverDesc()
+    every = (ctypes.c_int64 * 3)()
+    t, st = ctypes.c_double(), ctypes.c_int64()
+    _lib.check(L.vls_restart_info(fname.encode(), ctypes.byref(g), ctypes.byref(sd), every,
+                                  ctypes.byref(t), ctypes.byref(st)))
+    scales = {v: k for k, v in _lib.SCALES.items()}
+    kernels = {v: k for k, v in _lib.KERNELS.items()}
+    return {"Pmin": g.Pmin, "Pmax": g.Pmax, "Pres": g.Pres, "Pscale": scales[g.Pscale],
+            "Umin": (g.Umin[0], g.Umin[1]), "Umax": (g.Umax[0], g.Umax[1]),
+            "Ures": (g.Ures[0], g.Ures[1]), "Uscale": (scales[g.Uscale[0]], scales[g.Uscale[1]]),
+            "G": sd.G, "T0": sd.T0, "Tmax": sd.Tmax, "dt": sd.dt,
+            "noLinking": sd.noLinking, "kernelType": kernels[sd.kernelType],
+            "kernelBufferSize": sd.kernelBufferSize, "snapshotEvery": every[0],
+            "restartEvery": every[1], "statsEvery": every[2], "time": t.value,
+            "step": st.value}
