@@ -116,3 +116,15 @@ def test_reinitialising_a_stepped_handle_restores_the_initial_state():
     s.step(3)
     fresh.step(3)
     np.testing.assert_array_equal(s.f, fresh.f)
+
+
+def test_far_cell_layout_keeps_the_adjoint(monkeypatch):
+    """With the far-cell pass (packed words FP_FAR + list index) the drift's
+    transpose reads the original footpoints from the far list."""
+    p_ref = problem("fp32")
+    target = p_ref.run(THETA + DTHETA)
+    _, g_ref = loss_and_grad(p_ref, target)
+    monkeypatch.setenv("VLS_FAR", "1")
+    p = problem("fp32")
+    _, g = loss_and_grad(p, target)
+    np.testing.assert_allclose(g, g_ref, rtol=1e-6)

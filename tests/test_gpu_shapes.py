@@ -39,12 +39,14 @@ IMPLS = {
     "strip48": {"VLS_DRIFT": "48"},
     "strip64": {"VLS_DRIFT": "64"},
     "strip-48": {"VLS_DRIFT": "-48"},
+    "strip-49": {"VLS_DRIFT": "-49"},
+    "far": {"VLS_FAR": "1"},
 }
 
 
 @pytest.fixture(params=sorted(IMPLS))
 def impl(request, monkeypatch):
-    for k in ("VLS_PREFILTER", "VLS_DRIFT", "VLS_RC"):
+    for k in ("VLS_PREFILTER", "VLS_DRIFT", "VLS_RC", "VLS_FAR"):
         monkeypatch.delenv(k, raising=False)
     for k, v in IMPLS[request.param].items():
         monkeypatch.setenv(k, v)

@@ -111,7 +111,7 @@ __device__ __forceinline__ void scatter16(double *Cbj, int pc, int rI, double x,
   }
 }
 
-constexpr uint32_t AFP_OUT = 0xFFFFFFFFu, AFP_CHAIN = 0xFFFFFFFEu;
+constexpr uint32_t AFP_CHAIN = 0xFFFFFFFEu, AFP_FAR = 0xFFFFFFFDu;
 constexpr int AFP_FBITS = 21;
 
 // drift, transposed: lam (cells) -> Cb (C layout, all slices), chain fronts
@@ -122,7 +122,7 @@ __global__ void drift_adj_kernel(const double *__restrict__ lam, double *__restr
                                  const T *__restrict__ fy, const uint2 *__restrict__ fp2,
                                  const int64_t *__restrict__ ch_start,
                                  const int32_t *__restrict__ ch_len, double *__restrict__ ringb,
-                                 int64_t ndrift, Geometry g) {
+                                 const uint2 *__restrict__ far_w, int64_t ndrift, Geometry g) {
   const size_t n = (size_t)g.nr * g.nu * g.nj;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -143,8 +143,10 @@ __global__ void drift_adj_kernel(const double *__restrict__ lam, double *__restr
         y = (double)fy[i];
       }
     } else {
-      const uint2 w = fp2[i];
-      kind = w.x < AFP_CHAIN ? 0 : (w.x == AFP_OUT ? 1 : 2);
+      uint2 w = fp2[i];
+      // far cells of the strip layout keep their footpoint in the far list
+      if (w.x == AFP_FAR) w = far_w[w.y];
+      kind = w.x < AFP_FAR ? 0 : (w.x == AFP_CHAIN ? 2 : 1);
       ch = w.y;
       if (kind == 0) {
         rI = (int)(w.x >> AFP_FBITS);
@@ -318,11 +320,11 @@ unsigned grid_for(size_t n, int threads) {
 template <typename T>
 cudaError_t launch_drift_adj(const double *lam, double *Cb, const int32_t *idx, const T *fx,
                              const T *fy, const uint2 *fp2, const int64_t *ch_start,
-                             const int32_t *ch_len, double *ringb, int64_t ndrift,
-                             const Geometry &g, cudaStream_t st) {
+                             const int32_t *ch_len, double *ringb, const uint2 *far_w,
+                             int64_t ndrift, const Geometry &g, cudaStream_t st) {
   const size_t n = (size_t)g.nr * g.nu * g.nj;
   drift_adj_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(lam, Cb, idx, fx, fy, fp2, ch_start,
-                                                         ch_len, ringb, ndrift, g);
+                                                         ch_len, ringb, far_w, ndrift, g);
   return cudaGetLastError();
 }
 
@@ -370,11 +372,13 @@ cudaError_t launch_moment_adj(double *lam, const double *beta, const MomentTable
 template cudaError_t launch_drift_adj<float>(const double *, double *, const int32_t *,
                                              const float *, const float *, const uint2 *,
                                              const int64_t *, const int32_t *, double *,
-                                             int64_t, const Geometry &, cudaStream_t);
+                                             const uint2 *, int64_t, const Geometry &,
+                                             cudaStream_t);
 template cudaError_t launch_drift_adj<double>(const double *, double *, const int32_t *,
                                               const double *, const double *, const uint2 *,
                                               const int64_t *, const int32_t *, double *,
-                                              int64_t, const Geometry &, cudaStream_t);
+                                              const uint2 *, int64_t, const Geometry &,
+                                              cudaStream_t);
 template cudaError_t launch_ucol_adj<float>(const float *, double *, double *, double *,
                                             double *, double *, const double *,
                                             const Geometry &, const DirTables &, cudaStream_t);

@@ -82,6 +82,18 @@ struct vls_handle {
   CUtensorMap tmC[8];
   CUtensorMap tmS[8];
   int strip_w = 0;
+  // cells whose taps leave the strip's columns (FP32 strip layout): their
+  // packed word is FP_FAR with the index into far_w / far_cell, sorted by
+  // (slice, column, row); far_col[j * N_r + r] starts column (j, r); farsum
+  // receives each column's moment contribution from the far pass
+  bool far_mode = false;
+  int64_t nfar = 0;
+  uint2 *far_w = nullptr;
+  uint32_t *far_cell = nullptr;
+  int32_t *far_col = nullptr;
+  double *far_prod = nullptr;
+  double *farsum = nullptr;
+  std::vector<int32_t> far_col_h;  // host copy (batch ranges)
   bool have_tma = false;
   // opt-in per-kernel event timing
   bool profiling = false;
@@ -246,7 +258,7 @@ static uint32_t pack_coord(int32_t I, double F, int32_t maxI) {
   if (qi < 0) qi = 0;
   return ((uint32_t)I << 21) | (uint32_t)qi;
 }
-static const uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu;
+static const uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu, FP_FAR = 0xFFFFFFFDu;
 
 static uint2 encode_packed(const Coords &c, int32_t code, double rF, double uF) {
   uint2 w;
@@ -261,6 +273,69 @@ static uint2 encode_packed(const Coords &c, int32_t code, double rF, double uF) 
     w.y = pack_coord(code >> 16, uF, c.nu - 1);
   }
   return w;
+}
+
+// Far cells of one slice (packed words p[0..slice), slice j): words whose
+// taps leave the drift strip's columns are replaced by FP_FAR + list index;
+// their original words and cell indices are appended to the host far list in
+// (column, row) order, and the per-column counts to fcount.
+struct FarHost {
+  std::vector<uint2> w;
+  std::vector<uint32_t> cell;
+  std::vector<int32_t> count;  // per (j, r)
+};
+static void mark_far_slice(const vls_handle *h, int j, uint2 *p, FarHost &fh) {
+  const Coords &c = h->co;
+  const int W = std::abs(h->strip_w) / 16 * 16, XL = (W - 32) / 2;
+  const size_t slice = (size_t)c.nr * c.nu;
+  std::vector<std::pair<uint32_t, uint32_t>> far;  // (r * nu + u, cell within slice)
+  for (size_t i = 0; i < slice; ++i) {
+    const uint2 w = p[i];
+    if (w.x >= FP_FAR) continue;
+    const int r = (int)(i % c.nr), u = (int)(i / c.nr);
+    const int wc = (int)(w.x >> 21) - ((r / 32) * 32 - XL);
+    if (wc < 0 || wc > W - 4) far.push_back({(uint32_t)(r * c.nu + u), (uint32_t)i});
+  }
+  std::sort(far.begin(), far.end());
+  for (auto &e : far) {
+    const size_t i = e.second;
+    const int r = (int)(i % c.nr);
+    fh.count[(size_t)j * c.nr + r]++;
+    const uint32_t idx = (uint32_t)fh.w.size();
+    fh.w.push_back(p[i]);
+    fh.cell.push_back((uint32_t)((size_t)j * slice + i));
+    p[i].x = FP_FAR;
+    p[i].y = idx;
+  }
+}
+
+static int upload_far(vls_handle *h, const FarHost &fh) {
+  auto release = [&](void *q) {
+    if (q) cudaFree(q);
+  };
+  release(h->far_w);
+  release(h->far_cell);
+  release(h->far_col);
+  release(h->far_prod);
+  h->far_w = nullptr;
+  h->far_cell = nullptr;
+  h->far_col = nullptr;
+  h->far_prod = nullptr;
+  h->nfar = (int64_t)fh.w.size();
+  const size_t ncol = (size_t)h->co.nj * h->co.nr;
+  std::vector<int32_t> col(ncol + 1, 0);
+  for (size_t k = 0; k < ncol; ++k) col[k + 1] = col[k] + fh.count[k];
+  CK(h, cudaMalloc(&h->far_w, sizeof(uint2) * std::max<size_t>(fh.w.size(), 1)));
+  CK(h, cudaMalloc(&h->far_cell, sizeof(uint32_t) * std::max<size_t>(fh.cell.size(), 1)));
+  CK(h, cudaMalloc(&h->far_col, sizeof(int32_t) * col.size()));
+  CK(h, cudaMalloc(&h->far_prod, sizeof(double) * std::max<size_t>(fh.w.size(), 1)));
+  h->far_col_h = col;
+  if (!fh.w.empty()) {
+    TRY(upload(h, h->far_w, fh.w.data(), sizeof(uint2) * fh.w.size()));
+    TRY(upload(h, h->far_cell, fh.cell.data(), sizeof(uint32_t) * fh.cell.size()));
+  }
+  TRY(upload(h, h->far_col, col.data(), sizeof(int32_t) * col.size()));
+  return VLS_OK;
 }
 
 // Encoding of one cell: -1 -> outside the box (value 0), <= -2 -> delayed
@@ -279,6 +354,8 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
   if (h->prec != VLS_FP64) packed.resize(slice * batch);
   std::vector<SliceFootpoints> sfp(batch);
   std::vector<SliceChains> sch(batch);
+  FarHost fh;
+  if (h->far_mode) fh.count.assign((size_t)c.nj * c.nr, 0);
   if (build_chains) {
     h->ch_cell_h.clear();
     h->ch_len_h.clear();
@@ -338,9 +415,12 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
       TRY(upload(h, (double *)h->fy + off, fy.data(), n * sizeof(double)));
     } else {
       for (size_t i = 0; i < n; i++) packed[i] = encode_packed(c, idx[i], fx[i], fy[i]);
+      if (h->far_mode)
+        for (int b = 0; b < nb; b++) mark_far_slice(h, j0 + b, packed.data() + (size_t)b * slice, fh);
       TRY(upload(h, h->fp2 + off, packed.data(), n * sizeof(uint2)));
     }
   }
+  if (h->far_mode) TRY(upload_far(h, fh));
   return VLS_OK;
 }
 
@@ -437,7 +517,7 @@ static bool make_tensor_map(vls_handle *h) {
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
     if (h->strip_w != 0) {
-      const cuuint32_t sbox[3] = {(cuuint32_t)std::abs(h->strip_w), 64, 1};
+      const cuuint32_t sbox[3] = {(cuuint32_t)(std::abs(h->strip_w) / 16 * 16), 64, 1};
       if (enc(&h->tmS[s],
               es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
               base, dims, strides, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -484,6 +564,13 @@ static void free_all(vls_handle *h) {
   h->allocs.clear();
   for (void *p : h->adj_allocs) cudaFree(p);
   h->adj_allocs.clear();
+  for (void *p : {(void *)h->far_w, (void *)h->far_cell, (void *)h->far_col,
+                  (void *)h->far_prod})
+    if (p) cudaFree(p);
+  h->far_w = nullptr;
+  h->far_cell = nullptr;
+  h->far_col = nullptr;
+  h->far_prod = nullptr;
   for (int k = 0; k < 8; k++) {
     if (h->bst[k]) cudaStreamDestroy(h->bst[k]);
     if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
@@ -633,12 +720,22 @@ extern "C" int vls_create(const vls_grid_desc *grid,
     // 64 or -48 selects one for measurements)
     const char *dv = std::getenv("VLS_DRIFT");
     const std::string d = dv ? dv : "";
-    const int want = d == "48" ? 48 : d == "64" ? 64 : d == "-48" ? -48 : 0;
+    const int want = d == "48" ? 48 : d == "64" ? 64 : d == "-48" ? -48 : d == "-49" ? -49 : 0;
     h->strip_w = d == "window" ? 0
                  : h->esize == 4 ? drift_strip_width<float>(c.nu, want)
                                  : drift_strip_width<double>(c.nu, want);
   }
   h->have_tma = make_tensor_map(hp);
+  // FP32 strip drift: VLS_FAR=1 moves the far cells to their own pass.  Off
+  // by default: on the 513 x 513 x 256 case it measured 7 % slower than
+  // leaving them to the strip kernel's global-memory path.
+  {
+    const char *fv = std::getenv("VLS_FAR");
+    h->far_mode = h->have_tma && h->strip_w != 0 && h->esize == 4 && fv &&
+                  std::string(fv) == "1";
+    if (h->far_mode && dalloc(hp, &h->farsum, sizeof(double) * (size_t)c.nj * c.nr) != VLS_OK)
+      return fin(VLS_ECUDA);
+  }
   // tables
   std::vector<double> dR(c.nr), dU(c.nu), Ct1(c.nj), bu(c.nu), wj(c.nj), dR4(c.nr),
       Rcoef(c.nr);
@@ -955,6 +1052,13 @@ extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
   } else {
     std::vector<uint2> p(h->cells);
     for (size_t i = 0; i < h->cells; i++) p[i] = encode_packed(c, idx[i], rF[i], uF[i]);
+    if (h->far_mode) {
+      FarHost fh;
+      fh.count.assign((size_t)c.nj * c.nr, 0);
+      const size_t slice = (size_t)c.nr * c.nu;
+      for (int j = 0; j < c.nj; j++) mark_far_slice(h, j, p.data() + (size_t)j * slice, fh);
+      TRY(upload_far(h, fh));
+    }
     TRY(upload(h, h->fp2, p.data(), sizeof(uint2) * h->cells));
   }
   return VLS_OK;
@@ -1019,12 +1123,23 @@ static int drift_once(vls_handle *h, bool kick) {
     CK(h, timed(
               h, VLS_K_DRIFT,
               [&] {
-                if (h->have_tma && h->strip_w != 0)
+                if (h->have_tma && h->strip_w != 0) {
+                  if (h->far_mode) {
+                    const int c_lo = h->far_col_h[(size_t)g.j0 * h->co.nr];
+                    const int c_hi = h->far_col_h[(size_t)(g.j0 + g.nb) * h->co.nr];
+                    const cudaError_t e = launch_far_drift(
+                        (const float *)C, (float *)h->f, h->far_cell, h->far_w, h->far_col,
+                        c_lo, c_hi, moment_tables(h), h->far_prod, h->farsum, g, bs);
+                    h->launches += c_hi > c_lo ? 2 : 1;  // timed with the drift
+                    if (e != cudaSuccess) return e;
+                  }
                   return launch_drift_strip<T>(&h->tmS[sl], h->strip_w, C, (T *)h->f, h->idx,
                                                (const T *)h->fx, (const T *)h->fy, h->fp2,
                                                h->ch_start, h->ch_len, (const T *)h->ch_val,
                                                h->ndrift, moment_tables(h), h->partial,
-                                               h->flag + 1, g, bs);
+                                               h->far_mode ? h->farsum : nullptr, h->flag + 1,
+                                               g, bs);
+                }
                 if (h->have_tma)
                   return launch_drift_tma<T>(&h->tmC[sl], C, (T *)h->f, h->idx,
                                              (const T *)h->fx, (const T *)h->fy, h->fp2,
@@ -1467,7 +1582,7 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift) {
   const size_t cbn = (size_t)g.nj * (g.nu + 3) * g.pc;
   CK(h, cudaMemsetAsync(b.Cb, 0, cbn * sizeof(double), h->st));
   CK(h, launch_drift_adj<T>(b.lam, b.Cb, h->idx, (const T *)h->fx, (const T *)h->fy, h->fp2,
-                            h->ch_start, h->ch_len, b.ringb, ndrift, g, h->st));
+                            h->ch_start, h->ch_len, b.ringb, h->far_w, ndrift, g, h->st));
   CK(h, launch_tails_adj(b.Cb, b.ringb, h->ch_start, h->ch_len, h->t_idx, h->t_x, h->t_y,
                          h->nch, ndrift, g, h->st));
   CK(h, launch_prer_adj(b.Cb, b.Gb, g, tr, h->st));

@@ -13,7 +13,9 @@
 //         fp_x, fp_y [cells] double fractional footpoint offsets
 //   FP32: fp2 [cells] uint2         per direction index<<21 | round(frac*2^21);
 //                                     0xFFFFFFFF = outside, 0xFFFFFFFE = chain
-//                                     (second word = chain id)
+//                                     (second word = chain id), 0xFFFFFFFD =
+//                                     far cell of the strip layout (second
+//                                     word = index into far_w / far_cell)
 //   chains: ch_start/int64, ch_len/int32 per chain, ch_val/T per element
 //           (ring buffer; logical front at (ndrift mod len)), tail footpoint
 //   partial [N_J][N_r] double       per-slice radial moment partial sums
@@ -105,8 +107,15 @@ cudaError_t launch_drift_strip(const CUtensorMap *tmS, int width, const T *C, T 
                                const int32_t *idx, const T *fx, const T *fy, const uint2 *fp2,
                                const int64_t *ch_start, const int32_t *ch_len,
                                const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                               double *partial, unsigned int *err, const Geometry &g,
-                               cudaStream_t st);
+                               double *partial, const double *farsum, unsigned int *err,
+                               const Geometry &g, cudaStream_t st);
+// far cells of the FP32 strip layout (packed word FP_FAR + list index)
+// (far cells [c_lo, c_hi) belong to the launch's slices; far_prod: one FP64
+// slot per far cell)
+cudaError_t launch_far_drift(const float *C, float *f, const uint32_t *far_cell,
+                             const uint2 *far_w, const int32_t *far_col, int c_lo, int c_hi,
+                             const MomentTables &mt, double *far_prod, double *farsum,
+                             const Geometry &g, cudaStream_t st);
 // chains [c_lo, c_hi) (all of the launch's slices) of nchains in total
 template <typename T>
 cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
@@ -133,8 +142,8 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
 template <typename T>
 cudaError_t launch_drift_adj(const double *lam, double *Cb, const int32_t *idx, const T *fx,
                              const T *fy, const uint2 *fp2, const int64_t *ch_start,
-                             const int32_t *ch_len, double *ringb, int64_t ndrift,
-                             const Geometry &g, cudaStream_t st);
+                             const int32_t *ch_len, double *ringb, const uint2 *far_w,
+                             int64_t ndrift, const Geometry &g, cudaStream_t st);
 cudaError_t launch_tails_adj(double *Cb, double *ringb, const int64_t *ch_start,
                              const int32_t *ch_len, const int32_t *t_idx, const double *t_x,
                              const double *t_y, int64_t nch, int64_t ndrift, const Geometry &g,

@@ -555,7 +555,7 @@ __device__ __forceinline__ Foot<double> load_foot(const int32_t *__restrict__ id
 // straight into a float mantissa (value 1.frac, minus 1): no int->float convert.
 constexpr int FP_FBITS = 21;
 constexpr uint32_t FP_FMASK = (1u << FP_FBITS) - 1u;
-constexpr uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu;
+constexpr uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu, FP_FAR = 0xFFFFFFFDu;
 
 __device__ __forceinline__ float frac21(uint32_t w) {
   return __uint_as_float(0x3F800000u | ((w & FP_FMASK) << 2)) - 1.0f;
@@ -803,11 +803,13 @@ __device__ __forceinline__ RawCell<double> load_raw(const int32_t *__restrict__ 
   c.y = __ldg(fy + i);
   return c;
 }
+// kinds: 0 gather, 1 outside (0), 2 delayed-kernel chain front, 3 far cell
+// (computed by the far pass; FP32 strip layout only)
 __device__ __forceinline__ Cell<float> decode(const RawCell<float> &r) {
   Cell<float> c;
   const uint2 w = r.w;
-  const bool ok = w.x < FP_CHAIN;
-  c.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
+  const bool ok = w.x < FP_FAR;
+  c.kind = ok ? 0 : (w.x == FP_OUT ? 1 : (w.x == FP_CHAIN ? 2 : 3));
   c.ch = w.y;
   c.rI = ok ? (int)(w.x >> FP_FBITS) : 0;
   c.uI = ok ? (int)(w.y >> FP_FBITS) : 0;
@@ -1069,7 +1071,7 @@ __device__ __forceinline__ T eval_strip(const T *p, T x, T y) {
     return eval_pitch<T, PITCH>(p, x, y);
 }
 
-template <typename T, int WC, int NW, int MINB>
+template <typename T, int WC, int NW, int MINB, bool WAITALL>
 __global__ void __launch_bounds__(32 * NW, MINB)
     drift_strip_kernel(const __grid_constant__ CUtensorMap tmS, const T *__restrict__ C,
                        T *__restrict__ f, const int32_t *__restrict__ idx,
@@ -1077,7 +1079,7 @@ __global__ void __launch_bounds__(32 * NW, MINB)
                        const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
                        const int32_t *__restrict__ ch_len, const T *__restrict__ ch_val,
                        int64_t ndrift, MomentTables mt, double *__restrict__ partial,
-                       unsigned int *err, Geometry g) {
+                       const double *__restrict__ farsum, unsigned int *err, Geometry g) {
   constexpr int XL = (WC - 32) / 2;
   constexpr int PF = 4;  // rows of footpoints in flight per thread
   constexpr uint32_t BYTES = DS_ROWS * WC * sizeof(T);
@@ -1105,6 +1107,16 @@ __global__ void __launch_bounds__(32 * NW, MINB)
   const bool col_ok = r < g.nr;
   int ready = 0;  // boxes [0, ready) seen complete by this thread
   bool waits_ok = true;
+  if (WAITALL) {
+    // every box before the first cell (the other block on the SM computes
+    // meanwhile); the per-cell test below then never waits
+    for (; ready < nch; ++ready)
+      if (!mbar_wait_bounded(&bar[ready], 0u)) {
+        waits_ok = false;
+        atomicOr(err, 1u);
+        break;
+      }
+  }
   double acc = 0.0;
   // footpoint words and moment weights b_u of the next PF rows in flight
   RawCell<T> q[PF];
@@ -1153,8 +1165,11 @@ __global__ void __launch_bounds__(32 * NW, MINB)
           const int L = __ldg(ch_len + cl.ch);
           v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
         }
-        f[row0 + (size_t)u * g.nr] = v;
-        part += bu * v;
+        // far cells: value and moment come from the far pass
+        if (cl.kind != 3) {
+          f[row0 + (size_t)u * g.nr] = v;
+          part += bu * v;
+        }
       }
     }
     acc += (double)part;
@@ -1170,16 +1185,19 @@ __global__ void __launch_bounds__(32 * NW, MINB)
     double sum = 0.0;
 #pragma unroll
     for (int k = 0; k < NW; ++k) sum += red[k][lane];
+    if (farsum) sum += farsum[(size_t)j * g.nr + r];
     partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * sum;
   }
 }
 
 // strip layouts: 48 (48 columns, 8 warps, two blocks per SM), 64 (64
 // columns, 16 warps, one block per SM), -48 (48 columns, 16 warps, two blocks
-// per SM); 0: none, the windowed kernel is used.  `want` != 0 asks for one
-// layout, returned only if it fits.  The default is -48 for FP32 storage
-// where two blocks fit, else the windowed kernel (FP64 strips fit one block
-// per SM only, which measured slower than the windowed kernel).
+// per SM), -49 (as -48, every box awaited before the first cell); 0: none,
+// the windowed kernel is used.  `want` != 0 asks for one layout, returned
+// only if it fits.  The default is -49 for FP32 storage where two blocks fit
+// (4 % faster than -48 on the 513 x 513 x 256 case: the other block on the SM
+// computes while this one's strip lands), else the windowed kernel (FP64
+// strips fit one block per SM only, which measured slower).
 template <typename T>
 int drift_strip_width(int nu, int want) {
   const int nch = (nu + 3 + DS_ROWS - 1) / DS_ROWS;
@@ -1193,24 +1211,26 @@ int drift_strip_width(int nu, int want) {
   if (want == 48) return fit48x8 ? 48 : 0;
   if (want == 64) return fit64 ? 64 : 0;
   if (want == -48) return fit48x16 ? -48 : 0;
-  return (sizeof(T) == 4 && fit48x16) ? -48 : 0;
+  if (want == -49) return fit48x16 ? -49 : 0;
+  return (sizeof(T) == 4 && fit48x16) ? -49 : 0;
 }
 
-template <typename T, int WC, int NW, int MINB>
+template <typename T, int WC, int NW, int MINB, bool WAITALL = false>
 static cudaError_t drift_strip_go(const CUtensorMap *tmS, const T *C, T *f, const int32_t *idx,
                                   const T *fx, const T *fy, const uint2 *fp2,
                                   const int64_t *ch_start, const int32_t *ch_len,
                                   const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                                  double *partial, unsigned int *err, const Geometry &g,
-                                  cudaStream_t st) {
+                                  double *partial, const double *farsum, unsigned int *err,
+                                  const Geometry &g, cudaStream_t st) {
   const int nch = (g.nu + 3 + DS_ROWS - 1) / DS_ROWS;
   const size_t smem = (size_t)nch * DS_ROWS * WC * sizeof(T) + nch * sizeof(uint64_t);
-  cudaError_t e = cudaFuncSetAttribute(drift_strip_kernel<T, WC, NW, MINB>,
+  cudaError_t e = cudaFuncSetAttribute(drift_strip_kernel<T, WC, NW, MINB, WAITALL>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const dim3 grid((g.nr + 31) / 32, g.nb);
-  drift_strip_kernel<T, WC, NW, MINB><<<grid, 32 * NW, smem, st>>>(
-      *tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val, ndrift, mt, partial, err, g);
+  drift_strip_kernel<T, WC, NW, MINB, WAITALL><<<grid, 32 * NW, smem, st>>>(
+      *tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val, ndrift, mt, partial, farsum, err,
+      g);
   return cudaGetLastError();
 }
 
@@ -1219,21 +1239,75 @@ cudaError_t launch_drift_strip(const CUtensorMap *tmS, int width, const T *C, T 
                                const int32_t *idx, const T *fx, const T *fy, const uint2 *fp2,
                                const int64_t *ch_start, const int32_t *ch_len,
                                const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                               double *partial, unsigned int *err, const Geometry &g,
-                               cudaStream_t st) {
+                               double *partial, const double *farsum, unsigned int *err,
+                               const Geometry &g, cudaStream_t st) {
   switch (width) {
     case 64:
       return drift_strip_go<T, 64, 16, 1>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
-                                          ndrift, mt, partial, err, g, st);
+                                          ndrift, mt, partial, farsum, err, g, st);
     case 48:
       return drift_strip_go<T, 48, 8, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
-                                         ndrift, mt, partial, err, g, st);
+                                         ndrift, mt, partial, farsum, err, g, st);
+    case -49:  // -48 with every box awaited before the first cell
+      return drift_strip_go<T, 48, 16, 2, true>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len,
+                                                ch_val, ndrift, mt, partial, farsum, err, g, st);
     case -48:
       return drift_strip_go<T, 48, 16, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
-                                          ndrift, mt, partial, err, g, st);
+                                          ndrift, mt, partial, farsum, err, g, st);
     default:
       return cudaErrorInvalidValue;
   }
+}
+
+// ---------------------------------------------------------------- far pass
+// Cells of the FP32 strip layout whose taps leave their block's strip
+// columns (0.4 % of the cells of the 513 x 513 x 256 Hernquist case).  One
+// thread per far cell gathers it from C in global memory, writes f and its
+// moment term b_u f; a second pass sums each (slice, r column)'s terms in
+// row order into farsum, which the strip kernel's epilogue adds, so the
+// moment sums keep a fixed order.  Both run before the strip kernel on the
+// same stream; far_prod holds one term per far cell.
+__global__ void far_value_kernel(const float *__restrict__ C, float *__restrict__ f,
+                                 const uint32_t *__restrict__ far_cell,
+                                 const uint2 *__restrict__ far_w, int c_lo, int c_hi,
+                                 MomentTables mt, double *__restrict__ far_prod, Geometry g) {
+  const int c = c_lo + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (c >= c_hi) return;
+  const uint2 w = far_w[c];
+  const uint32_t cell = far_cell[c];
+  const uint32_t slice = (uint32_t)g.nr * (uint32_t)g.nu;
+  const int jl = (int)(cell / slice) - g.j0;
+  const int u = (int)((cell % slice) / (uint32_t)g.nr);
+  const float *Cj = C + (size_t)jl * (g.nu + 3) * g.pc;
+  const float v = eval2d<float>(Cj, g.pc, (int)(w.x >> FP_FBITS), frac21(w.x),
+                                (int)(w.y >> FP_FBITS), frac21(w.y));
+  f[cell] = v;
+  far_prod[c] = (double)((float)__ldg(mt.bu + u) * v);
+}
+
+__global__ void far_sum_kernel(const int32_t *__restrict__ far_col,
+                               const double *__restrict__ far_prod,
+                               double *__restrict__ farsum, Geometry g) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)g.nb * g.nr) return;
+  const size_t col = (size_t)g.j0 * g.nr + (size_t)t;
+  const int c0 = far_col[col], c1 = far_col[col + 1];
+  double acc = 0.0;
+#pragma unroll 4
+  for (int c = c0; c < c1; ++c) acc += far_prod[c];
+  farsum[col] = acc;
+}
+
+cudaError_t launch_far_drift(const float *C, float *f, const uint32_t *far_cell,
+                             const uint2 *far_w, const int32_t *far_col, int c_lo, int c_hi,
+                             const MomentTables &mt, double *far_prod, double *farsum,
+                             const Geometry &g, cudaStream_t st) {
+  if (c_hi > c_lo)
+    far_value_kernel<<<(unsigned)((c_hi - c_lo + 127) / 128), 128, 0, st>>>(
+        C, f, far_cell, far_w, c_lo, c_hi, mt, far_prod, g);
+  const int64_t n = (int64_t)g.nb * g.nr;
+  far_sum_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(far_col, far_prod, farsum, g);
+  return cudaGetLastError();
 }
 
 // tails: chains are independent; the tail slot (ndrift+L-1) mod L differs
@@ -1553,7 +1627,8 @@ cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
   template cudaError_t launch_drift_strip<T>(                                   \
       const CUtensorMap *, int, const T *, T *, const int32_t *, const T *, const T *, \
       const uint2 *, const int64_t *, const int32_t *, const T *, int64_t,       \
-      const MomentTables &, double *, unsigned int *, const Geometry &, cudaStream_t); \
+      const MomentTables &, double *, const double *, unsigned int *, const Geometry &, \
+      cudaStream_t);                                                            \
   template cudaError_t launch_drift_tma<T>(                                     \
       const CUtensorMap *, const T *, T *, const int32_t *, const T *, const T *, \
       const uint2 *, const int64_t *, const int32_t *, const T *, int64_t,        \
