@@ -128,3 +128,15 @@ def test_far_cell_layout_keeps_the_adjoint(monkeypatch):
     p = problem("fp32")
     _, g = loss_and_grad(p, target)
     np.testing.assert_allclose(g, g_ref, rtol=1e-6)
+
+
+def test_chunked_adjoint_lines_match_one_thread_per_line(monkeypatch):
+    """The chunked-register transposed solves against the one-thread-per-line
+    kernels (VLS_PREFILTER=segment selects those for both directions)."""
+    p_ref = problem("fp64")
+    target = p_ref.run(THETA + DTHETA)
+    _, g_ref = loss_and_grad(p_ref, target)
+    monkeypatch.setenv("VLS_PREFILTER", "segment")
+    p = problem("fp64")
+    _, g = loss_and_grad(p, target)
+    np.testing.assert_allclose(g, g_ref, rtol=1e-10)

@@ -113,10 +113,15 @@ struct vls_handle {
     int64_t ndrift = 0, step = 0;
     double time = 0;
   };
-  std::vector<Ckpt> adj_ck;
+  std::vector<Ckpt> adj_ck;  // the first adj_ncp are this run's
   Ckpt adj_final;
   int64_t adj_n = 0;
-  int adj_K = 0;
+  int adj_K = 0, adj_ncp = 0;
+  // backward-pass arrays (FP64) and the segment stash, kept between calls
+  double *ab_lam = nullptr, *ab_Cb = nullptr, *ab_Gb = nullptr, *ab_A = nullptr,
+         *ab_B = nullptr, *ab_ringb = nullptr, *ab_sbar = nullptr, *ab_beta = nullptr;
+  bool ab_rc = false;
+  std::vector<void *> ab_stash;
   bool adj_ready = false;
   std::vector<void *> adj_allocs;
 };
@@ -564,6 +569,11 @@ static void free_all(vls_handle *h) {
   h->allocs.clear();
   for (void *p : h->adj_allocs) cudaFree(p);
   h->adj_allocs.clear();
+  h->adj_ck.clear();
+  h->adj_final = vls_handle::Ckpt();
+  h->ab_lam = h->ab_Cb = h->ab_Gb = h->ab_A = h->ab_B = nullptr;
+  h->ab_ringb = h->ab_sbar = h->ab_beta = nullptr;
+  h->ab_stash.clear();
   for (void *p : {(void *)h->far_w, (void *)h->far_cell, (void *)h->far_col,
                   (void *)h->far_prod})
     if (p) cudaFree(p);
@@ -1489,13 +1499,10 @@ extern "C" int vls_read_ndfield(vls_handle *h, const char *path) {
 // applies the transposed step to the adjoint field from the last step to the
 // first.  Memory: ceil(N/K) + 1 checkpoints and K states of f, plus six FP64
 // arrays of about one grid each.
-static void adj_release(vls_handle *h) {
-  for (void *p : h->adj_allocs) cudaFree(p);
-  h->adj_allocs.clear();
-  h->adj_ck.clear();
-  h->adj_final = vls_handle::Ckpt();
-  h->adj_ready = false;
-}
+// Device buffers of the adjoint stay with the handle between runs (every
+// forward/backward pair of an optimisation loop would otherwise allocate and
+// free ~10 grids); vls_destroy frees them.
+static void adj_release(vls_handle *h) { h->adj_ready = false; }
 
 template <typename P>
 static int adj_alloc(vls_handle *h, P **p, size_t bytes) {
@@ -1549,7 +1556,7 @@ extern "C" int vls_adjoint_forward(vls_handle *h, int32_t nsteps, int32_t checkp
   CK(h, cudaStreamSynchronize(h->st));
   adj_release(h);
   const int ncp = (nsteps + checkpoint_every - 1) / checkpoint_every;
-  h->adj_ck.assign(ncp, vls_handle::Ckpt());
+  if ((int)h->adj_ck.size() < ncp) h->adj_ck.resize(ncp);  // new entries allocate on first save
   for (int s = 0; s < nsteps; ++s) {
     if (s % checkpoint_every == 0) TRY(ckpt_save(h, h->adj_ck[s / checkpoint_every]));
     TRY(vls_step(h, 1));
@@ -1557,6 +1564,7 @@ extern "C" int vls_adjoint_forward(vls_handle *h, int32_t nsteps, int32_t checkp
   TRY(ckpt_save(h, h->adj_final));
   h->adj_n = nsteps;
   h->adj_K = checkpoint_every;
+  h->adj_ncp = ncp;
   h->adj_ready = true;
   return VLS_OK;
 }
@@ -1566,6 +1574,9 @@ struct AdjBufs {
   double *lam, *Cb, *Gb, *A, *B, *ringb, *sbar, *beta;
   std::vector<void *> stash;
   std::vector<int64_t> ndrift;
+  // chunked line kernels (else one thread per line through A and B)
+  bool rc = false;
+  RcDir<double> rcu{}, rcr{};
 };
 }  // namespace
 
@@ -1585,9 +1596,14 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift) {
                             h->ch_start, h->ch_len, b.ringb, h->far_w, ndrift, g, h->st));
   CK(h, launch_tails_adj(b.Cb, b.ringb, h->ch_start, h->ch_len, h->t_idx, h->t_x, h->t_y,
                          h->nch, ndrift, g, h->st));
-  CK(h, launch_prer_adj(b.Cb, b.Gb, g, tr, h->st));
-  CK(h, launch_ucol_adj<T>((const T *)fn, b.Gb, b.A, b.B, b.lam, b.sbar, h->shift, g, tu,
-                           h->st));
+  if (b.rc) {
+    CK(h, launch_prer_adj_rc(b.Cb, b.Gb, g, b.rcr, h->st));
+    CK(h, launch_ucol_adj_rc<T>((const T *)fn, b.Gb, b.lam, b.sbar, h->shift, g, b.rcu, h->st));
+  } else {
+    CK(h, launch_prer_adj(b.Cb, b.Gb, g, tr, h->st));
+    CK(h, launch_ucol_adj<T>((const T *)fn, b.Gb, b.A, b.B, b.lam, b.sbar, h->shift, g, tu,
+                             h->st));
+  }
   CK(h, launch_shift_adj(b.sbar, b.beta, mt, g, h->st));
   CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
   h->launches += 9;
@@ -1602,24 +1618,48 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
   const size_t cells = h->cells;
   const size_t gn = (size_t)g.nj * (g.nu + 2) * g.nr;
   AdjBufs b{};
-  TRY(adj_alloc(h, &b.lam, cells * sizeof(double)));
-  TRY(adj_alloc(h, &b.Cb, (size_t)g.nj * (g.nu + 3) * g.pc * sizeof(double)));
-  TRY(adj_alloc(h, &b.Gb, gn * sizeof(double)));
-  TRY(adj_alloc(h, &b.A, gn * sizeof(double)));
-  TRY(adj_alloc(h, &b.B, gn * sizeof(double)));
-  TRY(adj_alloc(h, &b.ringb, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double)));
-  TRY(adj_alloc(h, &b.sbar, (size_t)g.nj * g.nr * sizeof(double)));
-  TRY(adj_alloc(h, &b.beta, (size_t)g.nr * sizeof(double)));
+  {
+    const char *pf = std::getenv("VLS_PREFILTER");
+    b.rc = rc_adj_supported(h->tu, h->tr) && !(pf && std::string(pf) == "segment");
+    b.rcu = rc_dir<double>(h->tu, 2);
+    b.rcr = rc_dir<double>(h->tr, 2);
+  }
+  if (!h->ab_lam || (h->ab_rc != b.rc && !b.rc)) {
+    if (!h->ab_lam) {
+      TRY(adj_alloc(h, &h->ab_lam, cells * sizeof(double)));
+      TRY(adj_alloc(h, &h->ab_Cb, (size_t)g.nj * (g.nu + 3) * g.pc * sizeof(double)));
+      TRY(adj_alloc(h, &h->ab_Gb, gn * sizeof(double)));
+      TRY(adj_alloc(h, &h->ab_ringb, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double)));
+      TRY(adj_alloc(h, &h->ab_sbar, (size_t)g.nj * g.nr * sizeof(double)));
+      TRY(adj_alloc(h, &h->ab_beta, (size_t)g.nr * sizeof(double)));
+    }
+    // scratch of the one-thread-per-line kernels
+    TRY(adj_alloc(h, &h->ab_A, (b.rc ? 1 : gn) * sizeof(double)));
+    TRY(adj_alloc(h, &h->ab_B, (b.rc ? 1 : gn) * sizeof(double)));
+    h->ab_rc = b.rc;
+  }
+  b.lam = h->ab_lam;
+  b.Cb = h->ab_Cb;
+  b.Gb = h->ab_Gb;
+  b.A = h->ab_A;
+  b.B = h->ab_B;
+  b.ringb = h->ab_ringb;
+  b.sbar = h->ab_sbar;
+  b.beta = h->ab_beta;
   const int K = h->adj_K;
-  b.stash.assign(K, nullptr);
-  for (int k = 0; k < K; ++k) TRY(adj_alloc(h, &b.stash[k], h->esize * cells));
+  while ((int)h->ab_stash.size() < K) {
+    void *q = nullptr;
+    TRY(adj_alloc(h, &q, h->esize * cells));
+    h->ab_stash.push_back(q);
+  }
+  b.stash.assign(h->ab_stash.begin(), h->ab_stash.begin() + K);
   b.ndrift.assign(K, 0);
   // seed: the derivative of the loss with respect to the final radial bins
   TRY(upload(h, b.beta, dbins, (size_t)g.nr * sizeof(double)));
   CK(h, cudaMemsetAsync(b.lam, 0, cells * sizeof(double), h->st));
   CK(h, cudaMemsetAsync(b.ringb, 0, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double), h->st));
   CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
-  const int ncp = (int)h->adj_ck.size();
+  const int ncp = h->adj_ncp;
   for (int seg = ncp - 1; seg >= 0; --seg) {
     const int64_t n0 = (int64_t)seg * K;
     const int64_t n1 = std::min<int64_t>(n0 + K, h->adj_n);
@@ -1650,10 +1690,6 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
   }
   // back to the final state of the forward run
   TRY(ckpt_load(h, h->adj_final));
-  // the stash and adjoint arrays go; the checkpoints stay for another seed
-  const size_t keep = 2 * (h->adj_ck.size() + 1);
-  for (size_t i = keep; i < h->adj_allocs.size(); ++i) cudaFree(h->adj_allocs[i]);
-  h->adj_allocs.resize(keep);
   CK(h, cudaGetLastError());
   return VLS_OK;
 }

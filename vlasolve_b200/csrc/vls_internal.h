@@ -158,6 +158,14 @@ cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTable
                              const Geometry &g, cudaStream_t st);
 cudaError_t launch_moment_adj(double *lam, const double *beta, const MomentTables &mt,
                               const Geometry &g, cudaStream_t st);
+// chunked adjoint line kernels (vls_rc.cu), used when rc_adj_supported
+bool rc_adj_supported(const HostDirTables &tu, const HostDirTables &tr);
+template <typename T>
+cudaError_t launch_ucol_adj_rc(const T *f, const double *Gb, double *lam, double *sbar,
+                               const double *shift, const Geometry &g, const RcDir<double> &tu,
+                               cudaStream_t st);
+cudaError_t launch_prer_adj_rc(const double *Cb, double *Gb, const Geometry &g,
+                               const RcDir<double> &tr, cudaStream_t st);
 template <typename T>
 cudaError_t launch_moment(const T *f, const MomentTables &mt, double *partial,
                           const Geometry &g, cudaStream_t st);

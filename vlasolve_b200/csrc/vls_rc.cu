@@ -465,6 +465,362 @@ cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
   return cudaGetLastError();
 }
 
+// ----------------------------------------------------------- adjoint
+// Transposed natural-BC solve (the adjoint of the forward solve above, read
+// backwards): for c̄ at rows 0..M-1, x̄ at the data rows 1..N is
+//   ascending   e_1 = c̄_1 - a01 c̄_0, e_2 = c̄_2 - a02 c̄_0 - q_1 e_1,
+//               e_k = c̄_k - q_{k-1} e_{k-1};  c̄_{M-1} -= q_N e_N
+//   last row    d̄_{N-1} = e_{N-1} - (hi2/L2) c̄_{M-1},  d̄_N = e_N - (L1/L2) c̄_{M-1}
+//   descending  f_N = d̄_N,  f_k = d̄_k + m_{k+1} f_{k+1}  (m = -rp/6)
+//   x̄_k = rp_k f_k
+// in the same chunked form: local recurrences from zero corrected by carries.
+// The ascending carry enters a chunk through the factor -q at the row before
+// it (q_{16} for the second chunk, a table value; the limit beyond).  v holds
+// c̄ of the chunk's rows on entry and x̄ on exit; c0b (first chunk) and cMb
+// (last chunk) are c̄_0 and c̄_{M-1}.  Lines of at least two chunks only
+// (rc_adj_supported); shorter lines use the one-thread-per-line kernels.
+template <class C>
+__device__ __forceinline__ double adj_first_factor(int s, const RcDir<double> &t) {
+  const int k = s * C::L;  // the row before chunk s
+  return -t.q0[k < 31 ? k : 31];
+}
+
+template <class C>
+__device__ __forceinline__ void rc_solve_adj(double (&v)[C::L], const Role &ro, double *E,
+                                             double *F, const RcDir<double> &t, double c0b,
+                                             double cMb_in) {
+  constexpr int L = C::L, LN = C::LN;
+  const int S = t.S, N = t.N;
+  const int s = ro.s;
+  const int kfirst = 1 + s * L;
+  const int slot = s * LN + ro.ln;
+  // ---------------------------------------------------------- phase A
+  if (s == 0) {
+    v[0] -= t.a01 * c0b;
+    if (N >= 2) v[1] -= t.a02 * c0b;
+    double e = 0.0;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      e = rfma(-t.q0[i], e, v[i]);  // factor -q_{k-1}, k = 1 + i
+      v[i] = e;
+    }
+    if (ro.active && S >= 2) E[slot] = e;
+  } else {
+    double e = 0.0;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      e = rfma(-t.q_inf, e, v[i]);
+      v[i] = e;
+    }
+    if (ro.active && s <= S - 2) E[slot] = e;
+  }
+  __syncthreads();
+  // ---------------------------------------------------------- phase B
+  if (ro.active) {
+    if (s > 0) {
+      double ein = E[slot - LN];
+      if (s >= 2) ein = rfma(adj_first_factor<C>(s - 1, t) * t.qpow[L - 1], E[slot - 2 * LN], ein);
+      const double af = adj_first_factor<C>(s, t) * ein;
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = rfma(t.qpow[i], af, v[i]);
+      double fk = 0.0;
+      if (s == S - 1) {
+        const int iN = N - kfirst;  // 0 .. L-1
+        double eN = v[0];
+#pragma unroll
+        for (int i = 1; i < L; ++i)
+          if (i == iN) eN = v[i];
+        const double cMb = cMb_in - t.q0[N < 31 ? N : 31] * eN;
+        const double Bn = -(t.L1 / t.L2) * cMb, Bp = -(t.hi2 / t.L2) * cMb;
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+          if (i == iN) v[i] += Bn;
+          if (i + 1 == iN) v[i] += Bp;
+        }
+#pragma unroll
+        for (int i = L - 1; i >= 0; --i)
+          if (i <= iN) {
+            fk = (i == iN) ? v[i] : rfma(t.m_inf, fk, v[i]);
+            v[i] = fk;
+          }
+        // with one row here, d̄_{N-1} belongs to the previous chunk: pass its
+        // term through the carry (m T' = m T + Bp)
+        F[slot] = v[0] + (iN == 0 ? Bp / t.m_inf : 0.0);
+      } else {
+#pragma unroll
+        for (int i = L - 1; i >= 0; --i) {
+          fk = rfma(t.m_inf, fk, v[i]);
+          v[i] = fk;
+        }
+        F[slot] = fk;
+      }
+    }
+  }
+  __syncthreads();
+  // ---------------------------------------------------------- phase C
+  if (ro.active && S >= 2 && s <= S - 2) {
+    double T = F[slot + LN];
+    if (s + 2 <= S - 1) T = rfma(t.mpow[L], F[slot + 2 * LN], T);
+    if (s == 0) {
+      double fk = T;
+#pragma unroll
+      for (int i = L - 1; i >= 0; --i) {
+        fk = rfma(t.m0[i + 2], fk, v[i]);
+        v[i] = fk;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = rfma(t.mpow[L - i], T, v[i]);
+    }
+  }
+  // x̄ = rp f
+  if (s == 0) {
+#pragma unroll
+    for (int i = 0; i < L; ++i) v[i] *= t.rp0[i + 1];
+  } else {
+#pragma unroll
+    for (int i = 0; i < L; ++i) v[i] *= t.rp_inf;
+  }
+}
+
+// adjoint of the kick weights: w_m(fr) and dw_m/dfr
+__device__ __forceinline__ void adj_kick_weights(double fr, double w[4], double dw[4]) {
+  const double a = 1.0 - fr;
+  w[0] = w_bv2<double>(a) / 6.0;
+  w[1] = w_bv1<double>(a) / 6.0;
+  w[2] = w_bv1<double>(fr) / 6.0;
+  w[3] = w_bv2<double>(fr) / 6.0;
+  dw[0] = -3.0 * a * a / 6.0;
+  dw[1] = -(3.0 + 6.0 * a - 9.0 * a * a) / 6.0;
+  dw[2] = (3.0 + 6.0 * fr - 9.0 * fr * fr) / 6.0;
+  dw[3] = 3.0 * fr * fr / 6.0;
+}
+
+// u lines of the adjoint step, per (16 r columns, J slice):
+//   g = P_u f_n          (recomputed; kept in shared memory GS)
+//   f̄' = P_u^T Ḡ        (rows of the kicked values)
+//   ḡ = Kick^T f̄', s̄   (gather in shift-fraction form, or shared-memory
+//                          scatter when a column takes the exact per-row path)
+//   λ = P_u^T ḡ
+template <typename T, class CF>
+__global__ void __launch_bounds__(CF::NT, CF::MINB)
+    ucol_adj_rc_kernel(const T *__restrict__ f, const double *__restrict__ Gb,
+                       double *__restrict__ lam, double *__restrict__ sbar,
+                       const double *__restrict__ shift, Geometry g,
+                       const __grid_constant__ RcDir<double> t) {
+  constexpr int L = CF::L, LN = CF::LN;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int S = t.S, N = t.N;  // N == g.nu
+  const int M = N + 2;
+  double *E = reinterpret_cast<double *>(smem_raw);
+  double *F = E + S * LN;
+  double *GS = F + S * LN;              // (M + 1) rows x LN
+  double *FB = GS + (size_t)(M + 1) * LN;  // N rows x LN
+  const Role ro = rc_role<CF>(S);
+  const int r = blockIdx.x * LN + ro.ln;
+  const bool colok = r < g.nr;
+  const int j = blockIdx.y;
+  const int kfirst = 1 + ro.s * L;
+  const int rc = colok ? r : g.nr - 1;
+  double v[L];
+  // 1. g = P_u f_n
+  {
+    const T *fc = f + (size_t)j * N * g.nr + rc;
+#pragma unroll
+    for (int i = 0; i < L; ++i) v[i] = (double)__ldg(fc + (size_t)(min(kfirst + i, N) - 1) * g.nr);
+  }
+  double c0 = 0.0, cM = 0.0;
+  rc_solve<double, CF>(v, ro, E, F, t, c0, cM);
+  if (ro.active) {
+#pragma unroll
+    for (int i = 0; i < L; ++i)
+      if (kfirst + i <= N) GS[(kfirst + i) * LN + ro.ln] = v[i];
+    if (ro.s == 0) GS[ro.ln] = c0;
+    if (ro.s == S - 1) {
+      GS[(M - 1) * LN + ro.ln] = cM;
+      GS[M * LN + ro.ln] = 0.0;
+    }
+  }
+  // 2. f̄' = P_u^T Ḡ
+  const double *Gc = Gb + (size_t)j * M * g.nr + rc;
+#pragma unroll
+  for (int i = 0; i < L; ++i) v[i] = Gc[(size_t)min(kfirst + i, N) * g.nr];
+  const double c0b = ro.s == 0 ? Gc[0] : 0.0;
+  const double cMb = ro.s == S - 1 ? Gc[(size_t)(M - 1) * g.nr] : 0.0;
+  __syncthreads();  // E, F reused
+  rc_solve_adj<CF>(v, ro, E, F, t, c0b, cMb);
+  if (ro.active) {
+#pragma unroll
+    for (int i = 0; i < L; ++i)
+      if (kfirst + i <= N) FB[(kfirst + i - 1) * LN + ro.ln] = v[i];
+  }
+  __syncthreads();
+  // 3. kick, transposed
+  const double sft = colok ? __ldg(shift + r) : 0.0;
+  const double qf = sft * g.hu;
+  const double fl = floor(qf);
+  const double frd = qf - fl;
+  const bool fast = frd > 1e-9 && frd < 1.0 - 1e-9 && fabs(qf) < 1e6;
+  double w[4], dw[4];
+  adj_kick_weights(frd, w, dw);
+  const int o = (int)fl;
+  // inside rows of the fraction form, clipped to the grid's rows
+  const int ulo = fast ? max((int)floor(-qf) + 1, 0) : 0;
+  const int uhi = fast ? min((int)ceil((double)(N - 1) - qf) - 1, N - 1) : -1;
+  double sb = 0.0;
+  // shift derivative: sum over this thread's kicked rows
+  if (ro.active) {
+#pragma unroll 1
+    for (int i = 0; i < L; ++i) {
+      const int u = kfirst + i - 1;
+      if (u >= N) break;
+      const double fb = FB[u * LN + ro.ln];
+      if (fast) {
+        if (u < ulo || u > uhi) continue;
+        const double *gp = GS + (ptrdiff_t)(u + o) * LN + ro.ln;
+        sb += fb * (dw[0] * gp[0] + dw[1] * gp[LN] + dw[2] * gp[2 * LN] + dw[3] * gp[3 * LN]);
+      } else {
+        const double newU = __ldg(g.U + u) + sft;
+        if (!(newU > g.u0 && newU < g.umax)) continue;
+        const double y = (newU - g.su) * g.hu;
+        const double yf = floor(y);
+        double ww[4], dd[4];
+        adj_kick_weights(y - yf, ww, dd);
+        const int Ny = 1 + (int)yf;
+        for (int m = 0; m < 4; ++m)
+          if (Ny - 1 + m < M) sb += fb * dd[m] * GS[(Ny - 1 + m) * LN + ro.ln];
+      }
+    }
+  }
+  sb *= g.hu;
+  // ḡ: gather when every column of the block is in fraction form
+  const bool scatter = __syncthreads_or(ro.active && colok && !fast);
+  double gk[L];
+  double g0 = 0.0, gM = 0.0;
+  if (!scatter) {
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const int k = kfirst + i;
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int u = k - o - m;
+        if (u >= ulo && u <= uhi) acc += w[m] * FB[u * LN + ro.ln];
+      }
+      gk[i] = acc;
+    }
+    if (ro.s == 0)
+      for (int m = 0; m < 4; ++m) {
+        const int u = 0 - o - m;
+        if (u >= ulo && u <= uhi) g0 += w[m] * FB[u * LN + ro.ln];
+      }
+    if (ro.s == S - 1)
+      for (int m = 0; m < 4; ++m) {
+        const int u = M - 1 - o - m;
+        if (u >= ulo && u <= uhi) gM += w[m] * FB[u * LN + ro.ln];
+      }
+  } else {
+    // shared-memory scatter into GS (g is no longer needed)
+    for (int e = threadIdx.x; e < (M + 1) * LN; e += blockDim.x) GS[e] = 0.0;
+    __syncthreads();
+    if (ro.active) {
+#pragma unroll 1
+      for (int i = 0; i < L; ++i) {
+        const int u = kfirst + i - 1;
+        if (u >= N) break;
+        const double fb = FB[u * LN + ro.ln];
+        if (fast) {
+          if (u < ulo || u > uhi) continue;
+          for (int m = 0; m < 4; ++m) atomicAdd(&GS[(u + o + m) * LN + ro.ln], w[m] * fb);
+        } else {
+          const double newU = __ldg(g.U + u) + sft;
+          if (!(newU > g.u0 && newU < g.umax)) continue;
+          const double y = (newU - g.su) * g.hu;
+          const double yf = floor(y);
+          double ww[4], dd[4];
+          adj_kick_weights(y - yf, ww, dd);
+          const int Ny = 1 + (int)yf;
+          for (int m = 0; m < 4; ++m)
+            if (Ny - 1 + m < M) atomicAdd(&GS[(Ny - 1 + m) * LN + ro.ln], ww[m] * fb);
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < L; ++i) gk[i] = GS[min(kfirst + i, M) * LN + ro.ln];
+    g0 = GS[ro.ln];
+    gM = GS[(M - 1) * LN + ro.ln];
+  }
+  // s̄ of the column, summed over its chunks in chunk order
+  __syncthreads();
+  if (ro.active) F[ro.s * LN + ro.ln] = sb;
+  __syncthreads();
+  if (ro.active && ro.s == 0 && colok) {
+    double tot = 0.0;
+    for (int c = 0; c < S; ++c) tot += F[c * LN + ro.ln];
+    sbar[(size_t)j * g.nr + r] = tot;
+  }
+  __syncthreads();
+  // 4. λ = P_u^T ḡ
+#pragma unroll
+  for (int i = 0; i < L; ++i) v[i] = gk[i];
+  rc_solve_adj<CF>(v, ro, E, F, t, ro.s == 0 ? g0 : 0.0, ro.s == S - 1 ? gM : 0.0);
+  if (ro.active && colok) {
+    double *lc = lam + (size_t)j * N * g.nr + r;
+#pragma unroll
+    for (int i = 0; i < L; ++i)
+      if (kfirst + i <= N) lc[(size_t)(kfirst + i - 1) * g.nr] = v[i];
+  }
+}
+
+// r lines of the adjoint step: rows of C̄ (all slices) -> P_r^T -> rows of Ḡ
+template <class CF>
+__global__ void __launch_bounds__(CF::NT, CF::MINB)
+    prer_adj_rc_kernel(const double *__restrict__ Cb, double *__restrict__ Gb, Geometry g,
+                       const __grid_constant__ RcDir<double> t) {
+  constexpr int L = CF::L, LN = CF::LN;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int S = t.S, N = t.N;  // N == g.nr
+  const int M = N + 2;
+  const int P = rc_tile_pitch(M, sizeof(double), LN);
+  double *E = reinterpret_cast<double *>(smem_raw);
+  double *F = E + S * LN;
+  double *tile = reinterpret_cast<double *>(smem_raw + al16(2 * (size_t)S * LN * sizeof(double)));
+  const Role ro = rc_role<CF>(S);
+  const int j = blockIdx.y;
+  const int rows = g.nu + 2;
+  const int kr0 = blockIdx.x * LN;
+  const int nrow = min(LN, rows - kr0);
+  const double *Cs = Cb + ((size_t)j * (g.nu + 3) + kr0) * g.pc;
+  for (int p = 0; p < nrow; ++p)
+    for (int k = threadIdx.x; k < M; k += blockDim.x)
+      cp_async_el(tile + p * P + k, Cs + (size_t)p * g.pc + k);
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  const int kfirst = 1 + ro.s * L;
+  double v[L];
+  const double *row = tile + ro.ln * P;
+#pragma unroll
+  for (int i = 0; i < L; ++i) v[i] = row[min(kfirst + i, N)];
+  const double c0b = ro.s == 0 ? row[0] : 0.0;
+  const double cMb = ro.s == S - 1 ? row[M - 1] : 0.0;
+  __syncthreads();  // every thread has its chunk before rows are overwritten
+  rc_solve_adj<CF>(v, ro, E, F, t, c0b, cMb);
+  if (ro.active && ro.ln < nrow) {
+    double *wr = tile + ro.ln * P;
+#pragma unroll
+    for (int i = 0; i < L; ++i)
+      if (kfirst + i <= N) wr[kfirst + i] = v[i];
+  }
+  __syncthreads();
+  double *Gs = Gb + ((size_t)j * rows + kr0) * g.nr;
+  for (int p = 0; p < nrow; ++p)
+    for (int k = threadIdx.x; k < N; k += blockDim.x) Gs[(size_t)p * g.nr + k] = tile[p * P + 1 + k];
+}
+
+using CfgAdjU = RcCfg<15, 16, 576, 1>;
+using CfgAdjR = RcCfg<15, 8, 320, 2>;
+
 }  // namespace
 
 // ------------------------------------------------------------- host side
@@ -561,6 +917,53 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
       return cudaErrorInvalidValue;
   }
 }
+
+// adjoint line kernels (FP64): u lines with 15-row chunks of 16 lines, r
+// lines with 15-row chunks of 8 lines; tables from rc_dir<double>(t, 2)
+bool rc_adj_supported(const HostDirTables &tu, const HostDirTables &tr) {
+  return tu.M - 2 > CfgAdjU::L && tr.M - 2 > CfgAdjR::L &&
+         cfg_fits<CfgAdjU>(tu.M - 2, tu.kc64) && cfg_fits<CfgAdjR>(tr.M - 2, tr.kc64);
+}
+
+template <typename T>
+cudaError_t launch_ucol_adj_rc(const T *f, const double *Gb, double *lam, double *sbar,
+                               const double *shift, const Geometry &g, const RcDir<double> &tu,
+                               cudaStream_t st) {
+  const int nt = rc_threads<CfgAdjU>(tu.S);
+  if (tu.N != g.nu || nt > CfgAdjU::NT || tu.L != CfgAdjU::L) return cudaErrorInvalidValue;
+  const int M = tu.N + 2;
+  const size_t smem = 2 * (size_t)tu.S * CfgAdjU::LN * sizeof(double) +
+                      (size_t)(M + 1 + tu.N) * CfgAdjU::LN * sizeof(double);
+  auto k = ucol_adj_rc_kernel<T, CfgAdjU>;
+  cudaError_t e = rc_attr(k, smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((g.nr + CfgAdjU::LN - 1) / CfgAdjU::LN, g.nj);
+  k<<<grid, nt, smem, st>>>(f, Gb, lam, sbar, shift, g, tu);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prer_adj_rc(const double *Cb, double *Gb, const Geometry &g,
+                               const RcDir<double> &tr, cudaStream_t st) {
+  const int nt = rc_threads<CfgAdjR>(tr.S);
+  if (tr.N != g.nr || nt > CfgAdjR::NT || tr.L != CfgAdjR::L) return cudaErrorInvalidValue;
+  const int M = tr.N + 2;
+  const size_t smem = al16(2 * (size_t)tr.S * CfgAdjR::LN * sizeof(double)) +
+                      (size_t)CfgAdjR::LN * rc_tile_pitch(M, sizeof(double), CfgAdjR::LN) *
+                          sizeof(double);
+  auto k = prer_adj_rc_kernel<CfgAdjR>;
+  cudaError_t e = rc_attr(k, smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((g.nu + 2 + CfgAdjR::LN - 1) / CfgAdjR::LN, g.nj);
+  k<<<grid, nt, smem, st>>>(Cb, Gb, g, tr);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_ucol_adj_rc<float>(const float *, const double *, double *, double *,
+                                               const double *, const Geometry &,
+                                               const RcDir<double> &, cudaStream_t);
+template cudaError_t launch_ucol_adj_rc<double>(const double *, const double *, double *,
+                                                double *, const double *, const Geometry &,
+                                                const RcDir<double> &, cudaStream_t);
 
 #define VLS_RC_INST(T, R)                                                                 \
   template cudaError_t launch_ucol_rc<T, R>(int, bool, const T *, T *, const double *,   \
