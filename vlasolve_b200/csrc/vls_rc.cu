@@ -254,11 +254,19 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   R c0 = R(0), cM = R(0);
   rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
   if (KICK) {
+    // chunks wholly inside the line (every chunk but the last) store without
+    // per-row tests
+    const bool full = kfirst + L - 1 <= N;
     if (ro.active) {
+      if (full) {
 #pragma unroll
-      for (int i = 0; i < L; ++i) {
-        const int k = kfirst + i;
-        if (k <= N) kb[k * LN + ro.ln] = (T)v[i];
+        for (int i = 0; i < L; ++i) kb[(kfirst + i) * LN + ro.ln] = (T)v[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < L; ++i) {
+          const int k = kfirst + i;
+          if (k <= N) kb[k * LN + ro.ln] = (T)v[i];
+        }
       }
       if (ro.s == 0) kb[ro.ln] = (T)c0;
       if (ro.s == S - 1) {
@@ -290,14 +298,23 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
         // row k = kfirst + i (u = k - 1) reads coefficient rows k+o-1 .. k+o+2
         const int ilo = ulo - kfirst + 1, ihi = min(uhi, N - 1) - kfirst + 1;
         const T *base = kb + (ptrdiff_t)(kfirst + o - 1) * LN + ro.ln;
+        if (ilo <= 0 && ihi >= L - 1) {
+          // every row of the chunk inside
 #pragma unroll
-        for (int i = 0; i < L; ++i) {
-          T x = T(0);
-          if (i >= ilo && i <= ihi) {
+          for (int i = 0; i < L; ++i) {
             const T *p = base + i * LN;
-            x = w0 * p[0] + w1 * p[LN] + w2 * p[2 * LN] + w3 * p[3 * LN];
+            v[i] = (R)(w0 * p[0] + w1 * p[LN] + w2 * p[2 * LN] + w3 * p[3 * LN]);
           }
-          v[i] = (R)x;
+        } else {
+#pragma unroll
+          for (int i = 0; i < L; ++i) {
+            T x = T(0);
+            if (i >= ilo && i <= ihi) {
+              const T *p = base + i * LN;
+              x = w0 * p[0] + w1 * p[LN] + w2 * p[2 * LN] + w3 * p[3 * LN];
+            }
+            v[i] = (R)x;
+          }
         }
       } else {
         // exact per-cell path (localSpline.hxx:426-429)
@@ -326,10 +343,16 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   }
   if (ro.active && colok) {
     T *Gc = G + (size_t)jl * M * g.nr + r;
+    if (kfirst + L - 1 <= N) {
+      T *p = Gc + (size_t)kfirst * g.nr;
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-      const int k = kfirst + i;
-      if (k <= N) Gc[(size_t)k * g.nr] = (T)v[i];
+      for (int i = 0; i < L; ++i) p[(size_t)i * g.nr] = (T)v[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) {
+        const int k = kfirst + i;
+        if (k <= N) Gc[(size_t)k * g.nr] = (T)v[i];
+      }
     }
     if (ro.s == 0) Gc[0] = (T)c0;
     if (ro.s == S - 1) Gc[(size_t)(M - 1) * g.nr] = (T)cM;
