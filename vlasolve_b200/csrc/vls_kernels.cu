@@ -1120,15 +1120,14 @@ __global__ void __launch_bounds__(32 * NW, MINB)
       }
   }
   double acc = 0.0;
-  // footpoint words and moment weights b_u of the next PF rows in flight
+  // footpoint words of the next PF rows in flight (the moment weights b_u are
+  // read where used: prefetching them too cost 10 % from register pressure)
   RawCell<T> q[PF];
-  double bq[PF];
 #pragma unroll
   for (int k = 0; k < PF; ++k) {
     const int u = w + NW * k;
     const int uc = u < g.nu ? u : 0;
     q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? uc : 0) * g.nr);
-    bq[k] = __ldg(mt.bu + uc);
   }
   for (int ub = w; ub < g.nu; ub += NW * PF) {
     T part = T(0);
@@ -1136,11 +1135,9 @@ __global__ void __launch_bounds__(32 * NW, MINB)
     for (int k = 0; k < PF; ++k) {
       const int u = ub + NW * k;
       const Cell<T> cl = decode(q[k]);
-      const T bu = (T)bq[k];
       const int un = u + NW * PF;
       const int unc = un < g.nu ? un : 0;
       q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? unc : 0) * g.nr);
-      bq[k] = __ldg(mt.bu + unc);
       if (u < g.nu && col_ok) {
         T v = T(0);
         if (cl.kind == 0) {
@@ -1170,7 +1167,7 @@ __global__ void __launch_bounds__(32 * NW, MINB)
         // far cells: value and moment come from the far pass
         if (cl.kind != 3) {
           f[row0 + (size_t)u * g.nr] = v;
-          part += bu * v;
+          part += (T)__ldg(mt.bu + u) * v;
         }
       }
     }
