@@ -675,12 +675,21 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   A(dalloc(hp, &h->f, es * cells));
   A(dalloc(hp, &h->G, es * (size_t)h->NS * h->B * (c.nu + 2) * c.nr));
   A(dalloc(hp, &h->C, es * (size_t)h->NS * h->B * (c.nu + 3) * h->pc));
-  if (h->prec == VLS_FP64) {
-    A(dalloc(hp, &h->idx, sizeof(int32_t) * cells));
-    A(dalloc(hp, &h->fx, es * cells));
-    A(dalloc(hp, &h->fy, es * cells));
-  } else {
-    A(dalloc(hp, &h->fp2, sizeof(uint2) * cells));
+  {
+    const size_t fcells = cells + (size_t)FOOT_PAD_ROWS * c.nr + 32;
+    if (h->prec == VLS_FP64) {
+      A(dalloc(hp, &h->idx, sizeof(int32_t) * fcells));
+      A(dalloc(hp, &h->fx, es * fcells));
+      A(dalloc(hp, &h->fy, es * fcells));
+      if (s == VLS_OK && (cudaMemset(h->idx, 0, sizeof(int32_t) * fcells) != cudaSuccess ||
+          cudaMemset(h->fx, 0, es * fcells) != cudaSuccess ||
+          cudaMemset(h->fy, 0, es * fcells) != cudaSuccess))
+        return fail(nullptr, VLS_ECUDA, "cudaMemset of the footpoint tables failed");
+    } else {
+      A(dalloc(hp, &h->fp2, sizeof(uint2) * fcells));
+      if (s == VLS_OK && cudaMemset(h->fp2, 0, sizeof(uint2) * fcells) != cudaSuccess)
+        return fail(nullptr, VLS_ECUDA, "cudaMemset of the footpoint tables failed");
+    }
   }
   A(dalloc(hp, &h->rp_r, sizeof(double) * h->tr.M));
   A(dalloc(hp, &h->q_r, sizeof(double) * h->tr.M));

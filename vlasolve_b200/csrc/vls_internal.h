@@ -16,6 +16,9 @@
 //                                     (second word = chain id), 0xFFFFFFFD =
 //                                     far cell of the strip layout (second
 //                                     word = index into far_w / far_cell)
+//   the footpoint tables end with FOOT_PAD_ROWS zeroed rows of N_r cells and
+//   32 more zeroed cells past the last slice, so that the strip drift
+//   prefetches the next rows of a slice without clamping the row index
 //   chains: ch_start/int64, ch_len/int32 per chain, ch_val/T per element
 //           (ring buffer; logical front at (ndrift mod len)), tail footpoint
 //   partial [N_J][N_r] double       per-slice radial moment partial sums
@@ -27,6 +30,10 @@
 #include <cuda_runtime.h>
 
 namespace vls {
+
+// readable rows past the end of the footpoint tables (the strip drift reads
+// at most 16 warps x 4 rows ahead; 32 cells more cover the lanes past N_r)
+constexpr int FOOT_PAD_ROWS = 66;
 
 // Thomas tables of one direction of the natural-BC cubic B-spline solve
 // (localSpline.hxx:953-1182).  Row k of the padded line, M = dim + 2.

@@ -1072,6 +1072,138 @@ __device__ __forceinline__ T eval_strip(const T *p, T x, T y) {
     return eval_pitch<T, PITCH>(p, x, y);
 }
 
+// Footpoint fields needed by the strip's fast path: the gather test and the
+// tap position.  For non-gather words the values are unused.
+template <typename T>
+struct FastFoot {
+  bool gather;
+  int rI, uI;
+  T x, y;
+};
+__device__ __forceinline__ FastFoot<float> fast_foot(const RawCell<float> &c) {
+  FastFoot<float> p;
+  p.gather = c.w.x < FP_FAR;
+  p.rI = (int)(c.w.x >> FP_FBITS);
+  p.uI = (int)(c.w.y >> FP_FBITS);
+  p.x = frac21(c.w.x);
+  p.y = frac21(c.w.y);
+  return p;
+}
+__device__ __forceinline__ FastFoot<double> fast_foot(const RawCell<double> &c) {
+  FastFoot<double> p;
+  p.gather = c.code >= 0;
+  p.rI = c.code & 0xffff;
+  p.uI = c.code >> 16;
+  p.x = c.x;
+  p.y = c.y;
+  return p;
+}
+
+// One cell of the strip drift once every box has landed (wcap = WC - 3, or 0
+// after a failed wait, which sends every cell to the global-memory gather).
+// The in-strip gather runs for every lane, with the tap offset zeroed where
+// it does not apply; a warp vote sends the rare other cells (outside,
+// chain fronts, far cells, taps outside the strip's columns) through the
+// general decode.  `put`: the cell's value is stored and enters the moment.
+template <typename T, int WC>
+__device__ __forceinline__ T strip_cell(const RawCell<T> &c, const T *win, int x0,
+                                        uint32_t wcap, bool col_ok, const T *__restrict__ Cj,
+                                        const int64_t *__restrict__ ch_start,
+                                        const int32_t *__restrict__ ch_len,
+                                        const T *__restrict__ ch_val, int64_t ndrift,
+                                        const Geometry &g, bool &put) {
+  const FastFoot<T> p = fast_foot(c);
+  const int wc = p.rI - x0;
+  const bool in = col_ok && p.gather && (uint32_t)wc < wcap;
+  const int so = in ? p.uI * WC + wc : 0;
+  T v = eval_strip<T, WC>(win + so, p.x, p.y);
+  put = col_ok;
+  const bool slow = col_ok && !in;
+  if (__any_sync(0xffffffffu, slow)) {
+    if (slow) {
+      const Cell<T> cl = decode(c);
+      v = T(0);
+      if (cl.kind == 0)
+        v = eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
+      else if (cl.kind == 2)
+        v = ch_val[__ldg(ch_start + cl.ch) + ndrift % __ldg(ch_len + cl.ch)];
+      // far cells: value and moment come from the far pass
+      put = cl.kind != 3;
+    }
+  }
+  return v;
+}
+
+// The rows of one strip column (lane) for warp w: rows w, w + NW, ...,
+// footpoints PF rows ahead in flight.  Offsets are relative to slice j and
+// 32-bit; the prefetch runs past the slice's last row into the next slice
+// or the tables' padding (FOOT_PAD_ROWS rows and 32 cells), and lanes past
+// N_r read the next row's words, which they do not use.
+template <typename T, int WC, int NW, int PF>
+__device__ __forceinline__ void strip_rows(
+    const T *win, int x0, bool waits_ok, bool col_ok, int j, int r, int w,
+    const T *__restrict__ Cj, T *__restrict__ f,
+    const int32_t *__restrict__ idx, const T *__restrict__ fx, const T *__restrict__ fy,
+    const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
+    const int32_t *__restrict__ ch_len, const T *__restrict__ ch_val, int64_t ndrift,
+    const MomentTables &mt, const Geometry &g, double &acc) {
+  static_assert(NW * PF + 1 <= FOOT_PAD_ROWS, "prefetch reaches past the padding rows");
+  const size_t sb = (size_t)j * g.nu * g.nr;
+  const int32_t *ids = idx;
+  const T *fxs = fx, *fys = fy;
+  const uint2 *fps = fp2;
+  if constexpr (sizeof(T) == 4)
+    fps += sb;
+  else {
+    ids += sb;
+    fxs += sb;
+    fys += sb;
+  }
+  T *fs = f + sb;
+  const uint32_t step = (uint32_t)NW * (uint32_t)g.nr;
+  const uint32_t ahead = (uint32_t)PF * step;
+  const uint32_t wcap = waits_ok ? (uint32_t)(WC - 3) : 0u;
+  uint32_t off = (uint32_t)w * (uint32_t)g.nr + (uint32_t)r;
+  RawCell<T> q[PF];
+#pragma unroll
+  for (int k = 0; k < PF; ++k) q[k] = load_raw(ids, fxs, fys, fps, off + k * step);
+  int u = w;
+  // groups whose PF rows all lie in the slice
+  for (; u + NW * (PF - 1) < g.nu; u += NW * PF) {
+    T part = T(0);
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      const RawCell<T> c = q[k];
+      q[k] = load_raw(ids, fxs, fys, fps, off + ahead);
+      bool put;
+      const T v = strip_cell<T, WC>(c, win, x0, wcap, col_ok, Cj, ch_start, ch_len, ch_val,
+                                    ndrift, g, put);
+      if (put) {
+        fs[off] = v;
+        part += (T)__ldg(mt.bu + u + NW * k) * v;
+      }
+      off += step;
+    }
+    acc += (double)part;
+  }
+  // the last, partial group
+  T part = T(0);
+#pragma unroll
+  for (int k = 0; k < PF; ++k) {
+    if (u + NW * k < g.nu) {
+      bool put;
+      const T v = strip_cell<T, WC>(q[k], win, x0, wcap, col_ok, Cj, ch_start, ch_len, ch_val,
+                                    ndrift, g, put);
+      if (put) {
+        fs[off] = v;
+        part += (T)__ldg(mt.bu + u + NW * k) * v;
+      }
+      off += step;
+    }
+  }
+  acc += (double)part;
+}
+
 template <typename T, int WC, int NW, int MINB, bool WAITALL>
 __global__ void __launch_bounds__(32 * NW, MINB)
     drift_strip_kernel(const __grid_constant__ CUtensorMap tmS, const T *__restrict__ C,
@@ -1120,58 +1252,63 @@ __global__ void __launch_bounds__(32 * NW, MINB)
       }
   }
   double acc = 0.0;
-  // footpoint words of the next PF rows in flight (the moment weights b_u are
-  // read where used: prefetching them too cost 10 % from register pressure)
-  RawCell<T> q[PF];
-#pragma unroll
-  for (int k = 0; k < PF; ++k) {
-    const int u = w + NW * k;
-    const int uc = u < g.nu ? u : 0;
-    q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? uc : 0) * g.nr);
-  }
-  for (int ub = w; ub < g.nu; ub += NW * PF) {
-    T part = T(0);
+  if constexpr (WAITALL) {
+    strip_rows<T, WC, NW, PF>(win, x0, waits_ok, col_ok, j, r, w, Cj, f, idx, fx, fy, fp2,
+                              ch_start, ch_len, ch_val, ndrift, mt, g, acc);
+  } else {
+    // footpoint words of the next PF rows in flight (the moment weights b_u are
+    // read where used: prefetching them too cost 10 % from register pressure)
+    RawCell<T> q[PF];
 #pragma unroll
     for (int k = 0; k < PF; ++k) {
-      const int u = ub + NW * k;
-      const Cell<T> cl = decode(q[k]);
-      const int un = u + NW * PF;
-      const int unc = un < g.nu ? un : 0;
-      q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? unc : 0) * g.nr);
-      if (u < g.nu && col_ok) {
-        T v = T(0);
-        if (cl.kind == 0) {
-          const int wc = cl.rI - x0;
-          bool inwin = waits_ok && wc >= 0 && wc <= WC - 4;
-          if (inwin) {
-            // boxes complete in issue order; wait up to the one holding the last tap row
-            const int cb = (cl.uI + 3) / DS_ROWS;
-            while (ready <= cb) {
-              if (!mbar_wait_bounded(&bar[ready], 0u)) {
-                waits_ok = false;
-                inwin = false;
-                atomicOr(err, 1u);
-                break;
+      const int u = w + NW * k;
+      const int uc = u < g.nu ? u : 0;
+      q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? uc : 0) * g.nr);
+    }
+    for (int ub = w; ub < g.nu; ub += NW * PF) {
+      T part = T(0);
+#pragma unroll
+      for (int k = 0; k < PF; ++k) {
+        const int u = ub + NW * k;
+        const Cell<T> cl = decode(q[k]);
+        const int un = u + NW * PF;
+        const int unc = un < g.nu ? un : 0;
+        q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? unc : 0) * g.nr);
+        if (u < g.nu && col_ok) {
+          T v = T(0);
+          if (cl.kind == 0) {
+            const int wc = cl.rI - x0;
+            bool inwin = waits_ok && wc >= 0 && wc <= WC - 4;
+            if (inwin) {
+              // boxes complete in issue order; wait up to the one holding the last tap row
+              const int cb = (cl.uI + 3) / DS_ROWS;
+              while (ready <= cb) {
+                if (!mbar_wait_bounded(&bar[ready], 0u)) {
+                  waits_ok = false;
+                  inwin = false;
+                  atomicOr(err, 1u);
+                  break;
+                }
+                ++ready;
               }
-              ++ready;
             }
+            if (inwin)
+              v = eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y);
+            else
+              v = eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
+          } else if (cl.kind == 2) {
+            const int L = __ldg(ch_len + cl.ch);
+            v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
           }
-          if (inwin)
-            v = eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y);
-          else
-            v = eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
-        } else if (cl.kind == 2) {
-          const int L = __ldg(ch_len + cl.ch);
-          v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
-        }
-        // far cells: value and moment come from the far pass
-        if (cl.kind != 3) {
-          f[row0 + (size_t)u * g.nr] = v;
-          part += (T)__ldg(mt.bu + u) * v;
+          // far cells: value and moment come from the far pass
+          if (cl.kind != 3) {
+            f[row0 + (size_t)u * g.nr] = v;
+            part += (T)__ldg(mt.bu + u) * v;
+          }
         }
       }
+      acc += (double)part;
     }
-    acc += (double)part;
   }
   // extra: the grid has N_r / 32 blocks and N_r = 32 k + 1; the last block
   // also computes the last column from its strip (columns r0 - 8 .. r0 + 39
