@@ -34,6 +34,7 @@ struct vls_handle {
   cudaStream_t st = nullptr;
   // device buffers
   void *f = nullptr, *G = nullptr, *C = nullptr;
+  float *bu32 = nullptr;         // the moment weights b_u in FP32
   int32_t *idx = nullptr;        // FP64 footpoints
   void *fx = nullptr, *fy = nullptr;
   uint2 *fp2 = nullptr;          // FP32 packed footpoints
@@ -209,6 +210,7 @@ static DirTables dir_tables(const HostDirTables &t, const double *rp,
 static MomentTables moment_tables(const vls_handle *h) {
   MomentTables m{};
   m.bu = h->bu;
+  m.bu32 = h->bu32;
   m.wj = h->wj;
   m.dR4 = h->dR4;
   m.Rcoef = h->Rcoef;
@@ -702,6 +704,7 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   A(dalloc(hp, &h->d_dU, sizeof(double) * c.nu));
   A(dalloc(hp, &h->d_Ct1, sizeof(double) * c.nj));
   A(dalloc(hp, &h->bu, sizeof(double) * c.nu));
+  A(dalloc(hp, &h->bu32, sizeof(float) * c.nu));
   A(dalloc(hp, &h->wj, sizeof(double) * c.nj));
   A(dalloc(hp, &h->dR4, sizeof(double) * c.nr));
   A(dalloc(hp, &h->Rcoef, sizeof(double) * c.nr));
@@ -787,6 +790,10 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   U2(h->d_dU, dU.data(), sizeof(double) * c.nu);
   U2(h->d_Ct1, Ct1.data(), sizeof(double) * c.nj);
   U2(h->bu, bu.data(), sizeof(double) * c.nu);
+  {
+    const std::vector<float> b32(bu.begin(), bu.end());
+    U2(h->bu32, b32.data(), sizeof(float) * c.nu);
+  }
   U2(h->wj, wj.data(), sizeof(double) * c.nj);
   U2(h->dR4, dR4.data(), sizeof(double) * c.nr);
   U2(h->Rcoef, Rcoef.data(), sizeof(double) * c.nr);

@@ -32,7 +32,7 @@
 namespace vls {
 
 // readable rows past the end of the footpoint tables (the strip drift reads
-// at most 16 warps x 4 rows ahead; 32 cells more cover the lanes past N_r)
+// at most 16 warps x 2 rows ahead; 32 cells more cover the lanes past N_r)
 constexpr int FOOT_PAD_ROWS = 66;
 
 // Thomas tables of one direction of the natural-BC cubic B-spline solve
@@ -65,6 +65,7 @@ struct MomentTables {
   const double *wj;  // 8 pi^2 J_j dJ_j
   const double *dR4; // dR_r / 4 (0 for the last vertex)
   const double *Rcoef;  // G/(R_r^2) * dt
+  const float *bu32;    // bu rounded to FP32 (the FP32 strip drift's products)
 };
 
 // Register-resident prefilter (vls_rc.cu): L rows of a line per thread,
