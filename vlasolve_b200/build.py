@@ -33,7 +33,7 @@ def _stale(target, deps):
 
 def build(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(CSRC, s) for s in SOURCES]
-    deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(REPO, "include", "vlasolve_b200.h"))
     deps.append(os.path.join(REPO, "include", "vlasolve_b200.hpp"))
     deps.append(os.path.join(CSRC, "vls_main.cpp"))

@@ -31,6 +31,7 @@ struct vls_handle {
   size_t esize = 8;
   size_t cells = 0;
   int pc = 0;
+  int gp = 0;  // row pitch of G: N_r rounded up to 16 bytes
   cudaStream_t st = nullptr;
   // device buffers
   void *f = nullptr, *G = nullptr, *C = nullptr;
@@ -179,6 +180,7 @@ static Geometry geometry(const vls_handle *h) {
   g.nu = h->co.nu;
   g.nj = h->co.nj;
   g.pc = h->pc;
+  g.gp = h->gp;
   g.j0 = 0;
   g.nb = h->co.nj;
   g.U = h->dU_val;
@@ -627,6 +629,10 @@ extern "C" int vls_create(const vls_grid_desc *grid,
     return fail(nullptr, VLS_EINVAL, "at most 2048 vertices along r and along v_r");
   h->cells = (size_t)c.nr * c.nu * c.nj;
   h->pc = ((c.nr + 3) + 3) / 4 * 4;
+  {
+    const int per16 = (int)(16 / h->esize);
+    h->gp = (c.nr + per16 - 1) / per16 * per16;
+  }
   h->tr = thomas_tables(c.nr, c.sstep_inv[0]);
   h->tu = thomas_tables(c.nu, c.sstep_inv[1]);
   {
@@ -675,7 +681,7 @@ extern "C" int vls_create(const vls_grid_desc *grid,
         return fail(nullptr, VLS_ECUDA, "cudaEventCreate failed");
   }
   A(dalloc(hp, &h->f, es * cells));
-  A(dalloc(hp, &h->G, es * (size_t)h->NS * h->B * (c.nu + 2) * c.nr));
+  A(dalloc(hp, &h->G, es * (size_t)h->NS * h->B * (c.nu + 2) * h->gp));
   A(dalloc(hp, &h->C, es * (size_t)h->NS * h->B * (c.nu + 3) * h->pc));
   {
     const size_t fcells = cells + (size_t)FOOT_PAD_ROWS * c.nr + 32;
@@ -1106,7 +1112,7 @@ template <typename T, typename R>
 static int drift_once(vls_handle *h, bool kick) {
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
   const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
-  const size_t gslot = (size_t)h->B * (h->co.nu + 2) * h->co.nr;
+  const size_t gslot = (size_t)h->B * (h->co.nu + 2) * h->gp;
   const size_t cslot = (size_t)h->B * (h->co.nu + 3) * h->pc;
   CK(h, cudaEventRecord(h->ev_fork, h->st));
   for (int k = 0; k < h->NS; k++) CK(h, cudaStreamWaitEvent(h->bst[k], h->ev_fork, 0));
@@ -1131,7 +1137,8 @@ static int drift_once(vls_handle *h, bool kick) {
               h, VLS_K_PRER,
               [&] {
                 if (h->rcr_cfg >= 0)
-                  return launch_prer_rc<T, R>(h->rcr_cfg, G, C, g, rcdir<R>(h, false), bs);
+                  return launch_prer_rc<T, R>(h->rcr_cfg, G, C, g, rcdir<R>(h, false),
+                                              h->flag + 1, bs);
                 return launch_prer<T, R>(G, C, g, tr, bs);
               },
               bs));
@@ -1238,14 +1245,17 @@ extern "C" int vls_step(vls_handle *h, int32_t nsteps) {
 
 // device-side status words: flag[1] bit 0/1 = a bounded mbarrier wait of the
 // drift timed out (the step then read global memory instead; results stay
-// valid but the hardware path misbehaved)
+// valid but the hardware path misbehaved); bit 2/3 = the r-solve's bulk row
+// staging timed out (that step's results are not valid)
 static int check_device_flags(vls_handle *h) {
   unsigned int fl[4] = {0, 0, 0, 0};
   CK(h, cudaMemcpyAsync(fl, h->flag, sizeof(fl), cudaMemcpyDeviceToHost, h->st));
   CK(h, cudaStreamSynchronize(h->st));
   if (fl[1]) {
     CK(h, cudaMemsetAsync(h->flag, 0, sizeof(fl), h->st));
-    return fail(h, VLS_ECUDA, "a bounded device wait timed out in the drift kernel");
+    return fail(h, VLS_ECUDA,
+                (fl[1] & 12u) ? "a bounded device wait timed out in the r-solve kernel"
+                              : "a bounded device wait timed out in the drift kernel");
   }
   return VLS_OK;
 }

@@ -2,9 +2,10 @@
 //
 // Device layout (HBM), one GPU holds everything:
 //   f      [N_J][N_u][N_r]          T (float or double), r fastest
-//   G      [slot][B][N_u+2][N_r]    T: u-direction spline coefficients of the
+//   G      [slot][B][N_u+2][Pg]     T: u-direction spline coefficients of the
 //                                     kicked f (rows 0 and N_u+1 are ghosts),
-//                                     for a batch of B slices per ring slot
+//                                     for a batch of B slices per ring slot;
+//                                     Pg = N_r rounded up to 16 bytes
 //   C      [slot][B][N_u+3][Pc]     T: 2D coefficients, Pc >= N_r+3; row N_u+2
 //                                     and columns >= N_r+2 stay zero (reads
 //                                     at index N exist for footpoints that
@@ -52,6 +53,7 @@ struct DirTables {
 struct Geometry {
   int nr, nu, nj;
   int pc;  // row pitch of C
+  int gp;  // row pitch of G (16-byte rows)
   // slices [j0, j0 + nb) are processed by this launch (grid.y = nb); the
   // scratch arrays G and C hold only those slices (local index j - j0)
   int j0, nb;
@@ -142,9 +144,11 @@ RcDir<R> rc_dir(const HostDirTables &t, int cfg);
 template <typename T, typename R>
 cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *shift,
                            const Geometry &g, const RcDir<R> &tu, cudaStream_t st);
+// err: bit 2 (4) when the bulk staging of a block's rows timed out, bit 3
+// (8) when the rows still had not landed at the block's end
 template <typename T, typename R>
 cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
-                           cudaStream_t st);
+                           unsigned int *err, cudaStream_t st);
 // adjoint of the step (vls_adjoint.cu); all adjoint arrays FP64: Cb in C
 // layout and Gb, A, B in G layout, each over all J slices
 template <typename T>

@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include "vls_async.cuh"
 #include "vls_internal.h"
 
 namespace vls {
@@ -352,11 +353,11 @@ __global__ void __launch_bounds__(UC_THREADS)
     solve_lines<Prec<T>::K, R>(bufB + col, TW, k0, k1, tu, rp, qq);
     out = bufB;
   }
-  T *Gs = G + (size_t)jl * M * g.nr;
+  T *Gs = G + (size_t)jl * M * g.gp;
   for (int e = tid; e < M * TW; e += UC_THREADS) {
     const int k = e / TW, c = e % TW;
     const int rr = r0 + c;
-    if (rr < g.nr) Gs[(size_t)k * g.nr + rr] = (T)out[k * TW + c];
+    if (rr < g.nr) Gs[(size_t)k * g.gp + rr] = (T)out[k * TW + c];
   }
 }
 
@@ -421,14 +422,14 @@ __global__ void __launch_bounds__(PrerCfg<R>::THREADS)
   const int j = blockIdx.y;  // slice within the batch (G and C are batch scratch)
   const int kr0 = blockIdx.x * ROWS;
   const int nrows = g.nu + 2;
-  const T *Gs = G + (size_t)j * nrows * g.nr;
+  const T *Gs = G + (size_t)j * nrows * g.gp;
   load_tables<R>(rp, qq, tr);
   // rows of the tile, each copied by the whole block (no index division)
   for (int p = 0; p < ROWS; ++p) {
     const int kr = kr0 + p;
     R *dst = buf + p * LS + 1;
     if (kr < nrows) {
-      const T *src = Gs + (size_t)kr * g.nr;
+      const T *src = Gs + (size_t)kr * g.gp;
       if constexpr (sizeof(T) == sizeof(R)) {
         for (int k = tid; k < g.nr; k += NT) cp_async(reinterpret_cast<T *>(dst + k), src + k);
       } else {
@@ -689,55 +690,6 @@ __global__ void __launch_bounds__(32 * DR_W, 4)
 // timeout the block records an error flag and falls back to global reads.
 constexpr int DW_COLS = 64, DW_ROWS = 40, DW_CH = 16, DW_XOFF = 16, DW_YOFF = 12;
 constexpr int DT_THREADS = 256;  // 8 warps x 32 columns; 2 rows per warp per chunk
-// a wait gives up after ~2^20 polls (tens of milliseconds at most)
-constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 20;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// non-blocking polls with a short sleep between them, at most MBAR_SPIN_LIMIT
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (uint32_t i = 0; i < MBAR_SPIN_LIMIT; ++i) {
-    if (mbar_test_wait(bar, parity)) return true;
-    if (i >= 32) __nanosleep(20);
-  }
-  return false;
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-// 3D tiled TMA load (no multicast) of one box into shared memory
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, int x, int y,
-                                            int z, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
-
 template <typename T>
 struct Cell {
   int rI, uI, kind;

@@ -33,6 +33,7 @@
 #include <cmath>
 #include <string>
 
+#include "vls_async.cuh"
 #include "vls_internal.h"
 #include "vls_setup.h"
 
@@ -242,13 +243,24 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   const int kfirst = 1 + ro.s * L;
   R v[L];
   {
-    // unpredicated loads kept inside the slice (rows clamped to N, columns
-    // to N_r - 1): values of rows beyond N and of idle threads are never used
+    // unpredicated loads kept inside the slice (columns clamped to N_r - 1,
+    // rows to N in the last chunk): values of rows beyond N and of idle
+    // threads are never used.  Offsets within the slice are 32-bit.
     const T *fc = f + (size_t)j * g.nu * g.nr + (colok ? r : g.nr - 1);
+    const uint32_t nr = (uint32_t)g.nr;
+    if (kfirst + L - 1 <= N) {
+      uint32_t o = (uint32_t)(kfirst - 1) * nr;
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-      const int k = min(kfirst + i, N);
-      v[i] = (R)__ldg(fc + (size_t)(k - 1) * g.nr);
+      for (int i = 0; i < L; ++i) {
+        v[i] = (R)__ldg(fc + o);
+        o += nr;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) {
+        const int k = min(kfirst + i, N);
+        v[i] = (R)__ldg(fc + (uint32_t)(k - 1) * nr);
+      }
     }
   }
   R c0 = R(0), cM = R(0);
@@ -342,38 +354,60 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
     rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
   }
   if (ro.active && colok) {
-    T *Gc = G + (size_t)jl * M * g.nr + r;
+    T *Gc = G + (size_t)jl * M * g.gp + r;
+    const uint32_t gp = (uint32_t)g.gp;
     if (kfirst + L - 1 <= N) {
-      T *p = Gc + (size_t)kfirst * g.nr;
+      uint32_t o = (uint32_t)kfirst * gp;
 #pragma unroll
-      for (int i = 0; i < L; ++i) p[(size_t)i * g.nr] = (T)v[i];
+      for (int i = 0; i < L; ++i) {
+        Gc[o] = (T)v[i];
+        o += gp;
+      }
     } else {
 #pragma unroll
       for (int i = 0; i < L; ++i) {
         const int k = kfirst + i;
-        if (k <= N) Gc[(size_t)k * g.nr] = (T)v[i];
+        if (k <= N) Gc[(uint32_t)k * gp] = (T)v[i];
       }
     }
     if (ro.s == 0) Gc[0] = (T)c0;
-    if (ro.s == S - 1) Gc[(size_t)(M - 1) * g.nr] = (T)cM;
+    if (ro.s == S - 1) Gc[(uint32_t)(M - 1) * gp] = (T)cM;
   }
 }
 
 // ------------------------------------------------------------------ prer
 // Block: LN rows of G (u lines of the padded grid) of one J slice; a row is
-// an r line.  The rows are staged in shared memory (coalesced cp.async), each
-// thread moves its chunk into registers, solves, and writes it back; the
-// block then stores the tile to C with coalesced rows.
+// an r line.  The rows are staged in shared memory, each thread moves its
+// chunk into registers, solves, and writes it back; the block then stores the
+// tile to C.
 //
 // Tile row pitch P: the lanes of a warp read (line ln, chunk slot m) at
-// ln*P + m*L + const.  FP32 words: P = LN/... chosen so that 32/LN lines
-// times the chunk slots cover the 32 banks (L odd): P = 2 mod 32 for 16
-// lines, 4 mod 32 for 8 lines.  FP64 words (16 lanes per wavefront): odd P
-// for 16 lines, 2 mod 16 for 8 lines.
+// ln*P + m*L + const.  FP32 words: P = 2 mod 32 for 16 lines, 4 mod 32 for 8
+// lines, so that the 32/LN lines times the chunk slots (L odd) cover the 32
+// banks.  FP64 words (16 lanes per wavefront): odd P for 16 lines, 2 mod 16
+// for 8 lines.
+//
+// With 8 lines the pitch is a multiple of 16 bytes, and whole rows move as
+// bulk copies: G row -> tile row from word OFF = 16 bytes on (x_k at
+// OFF - 1 + k), and tile row -> C row from word 0 (c_k at k, words M .. Pc-1
+// zeroed).  A thread reads its whole chunk before the solve's first barrier
+// and writes after its last one, so the two offsets do not race.  Otherwise
+// (16 lines) the rows are copied element-wise with x_k at word k.
+template <class CF>
+__host__ __device__ constexpr bool rc_bulk_rows() {
+  return CF::LN == 8;
+}
 __host__ __device__ inline int rc_tile_pitch(int M, int elem, int LN) {
   if (elem == 4) return (M + 31) / 32 * 32 + (LN == 16 ? 2 : 4);
   if (LN == 16) return M | 1;
   return (M + 15) / 16 * 16 + 2;
+}
+// the forward r-solve's tile: with bulk rows, room for OFF + Pg words in and
+// Pc words out, at the same pitch residues
+__host__ __device__ inline int rc_tile_pitch_rows(int M, int gp, int pc, int elem, int LN) {
+  if (LN != 8) return rc_tile_pitch(M, elem, LN);
+  const int need = max(max(16 / elem + gp, pc), M);
+  return elem == 4 ? (need - 4 + 31) / 32 * 32 + 4 : (need - 2 + 15) / 16 * 16 + 2;
 }
 
 template <typename T>
@@ -387,12 +421,15 @@ __device__ __forceinline__ void cp_async_el(T *smem, const T *gmem) {
 template <typename T, typename R, class CF>
 __global__ void __launch_bounds__(CF::NT, CF::MINB)
     prer_rc_kernel(const T *__restrict__ G, T *__restrict__ C, Geometry g,
-                   const __grid_constant__ RcDir<R> t) {
+                   const __grid_constant__ RcDir<R> t, unsigned int *err) {
   constexpr int L = CF::L, LN = CF::LN;
+  constexpr bool BULK = rc_bulk_rows<CF>();
+  constexpr int OFF = BULK ? (int)(16 / sizeof(T)) : 1;  // word of x_1 in a tile row
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t bar;
   const int S = t.S, N = t.N;  // N == g.nr
   const int M = N + 2;
-  const int P = rc_tile_pitch(M, sizeof(T), LN);
+  const int P = rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), LN);
   R *dend = reinterpret_cast<R *>(smem_raw);
   R *cst = dend + S * LN;
   T *tile = reinterpret_cast<T *>(smem_raw + al16(2 * (size_t)S * LN * sizeof(R)));
@@ -401,42 +438,89 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   const int rows = g.nu + 2;
   const int kr0 = blockIdx.x * LN;
   const int nrow = min(LN, rows - kr0);
-  const T *Gs = G + ((size_t)jl * rows + kr0) * g.nr;
-  for (int p = 0; p < nrow; ++p) {
-    const T *src = Gs + (size_t)p * g.nr;
-    T *dst = tile + p * P + 1;
-    for (int k = threadIdx.x; k < N; k += blockDim.x) cp_async_el(dst + k, src + k);
+  const T *Gs = G + ((size_t)jl * rows + kr0) * g.gp;
+  bool landed = true;
+  if constexpr (BULK) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      mbar_fence_init();
+      const uint32_t bytes = (uint32_t)g.gp * sizeof(T);
+      mbar_expect_tx(&bar, bytes * (uint32_t)nrow);
+      for (int p = 0; p < nrow; ++p) bulk_load(tile + p * P + OFF, Gs + (size_t)p * g.gp, bytes, &bar);
+    }
+    __syncthreads();
+    if (!mbar_wait_bounded(&bar, 0u)) {
+      landed = false;
+      atomicOr(err, 4u);
+    }
+  } else {
+    for (int p = 0; p < nrow; ++p) {
+      const T *src = Gs + (size_t)p * g.gp;
+      T *dst = tile + p * P + OFF;
+      for (int k = threadIdx.x; k < N; k += blockDim.x) cp_async_el(dst + k, src + k);
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
   }
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-  __syncthreads();
   const bool lineok = ro.ln < nrow;
   const int kfirst = 1 + ro.s * L;
   R v[L];
   {
-    // rows clamped to N; rows beyond N and lines beyond the tile's last
-    // row are computed but never stored
-    const T *row = tile + ro.ln * P;
+    // rows clamped to N in the last chunk; rows beyond N and lines beyond the
+    // tile's last row are computed but never stored
+    const T *row = tile + ro.ln * P + (OFF - 1);
+    if (kfirst + L - 1 <= N) {
 #pragma unroll
-    for (int i = 0; i < L; ++i) v[i] = (R)row[min(kfirst + i, N)];
+      for (int i = 0; i < L; ++i) v[i] = (R)row[kfirst + i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = (R)row[min(kfirst + i, N)];
+    }
   }
   R c0 = R(0), cM = R(0);
   rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
   if (ro.active && lineok) {
     T *row = tile + ro.ln * P;
+    if (kfirst + L - 1 <= N) {
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-      const int k = kfirst + i;
-      if (k <= N) row[k] = (T)v[i];
+      for (int i = 0; i < L; ++i) row[kfirst + i] = (T)v[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) {
+        const int k = kfirst + i;
+        if (k <= N) row[k] = (T)v[i];
+      }
     }
     if (ro.s == 0) row[0] = (T)c0;
-    if (ro.s == S - 1) row[M - 1] = (T)cM;
+    if (ro.s == S - 1) {
+      row[M - 1] = (T)cM;
+      if (BULK)
+        for (int k = M; k < g.pc; ++k) row[k] = T(0);
+    }
   }
-  __syncthreads();
   T *Cs = C + ((size_t)jl * (g.nu + 3) + kr0) * g.pc;
-  for (int p = 0; p < nrow; ++p) {
-    const T *src = tile + p * P;
-    T *dst = Cs + (size_t)p * g.pc;
-    for (int k = threadIdx.x; k < M; k += blockDim.x) dst[k] = src[k];
+  if constexpr (BULK) {
+    fence_proxy_async();  // this thread's tile writes, visible to the bulk copies
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (landed) {
+        const uint32_t bytes = (uint32_t)g.pc * sizeof(T);
+        for (int p = 0; p < nrow; ++p) bulk_store(Cs + (size_t)p * g.pc, tile + p * P, bytes);
+        bulk_commit();
+        bulk_wait_read();
+      } else if (!mbar_wait_bounded(&bar, 0u)) {
+        // the rows never landed: nothing stored, and the block leaves only
+        // after a second bounded wait for the copies in flight
+        atomicOr(err, 8u);
+      }
+    }
+  } else {
+    __syncthreads();
+    for (int p = 0; p < nrow; ++p) {
+      const T *src = tile + p * P;
+      T *dst = Cs + (size_t)p * g.pc;
+      for (int k = threadIdx.x; k < M; k += blockDim.x) dst[k] = src[k];
+    }
   }
 }
 
@@ -474,17 +558,23 @@ cudaError_t ucol_rc_go(const T *f, T *G, const double *shift, const Geometry &g,
 
 template <typename T, typename R, class CF>
 cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
-                       cudaStream_t st) {
+                       unsigned int *err, cudaStream_t st) {
   const int nt = rc_threads<CF>(tr.S);
   if (tr.N != g.nr || nt > CF::NT || tr.L != CF::L) return cudaErrorInvalidValue;
+  // bulk rows: 16-byte rows of G and C, 16-byte aligned slices
+  if (rc_bulk_rows<CF>() &&
+      ((g.gp * sizeof(T)) % 16 != 0 || (g.pc * sizeof(T)) % 16 != 0 ||
+       reinterpret_cast<uintptr_t>(G) % 16 != 0 || reinterpret_cast<uintptr_t>(C) % 16 != 0))
+    return cudaErrorInvalidValue;
   const int M = tr.N + 2;
-  const size_t smem = al16(2 * (size_t)tr.S * CF::LN * sizeof(R)) +
-                      (size_t)CF::LN * rc_tile_pitch(M, sizeof(T), CF::LN) * sizeof(T);
+  const size_t smem =
+      al16(2 * (size_t)tr.S * CF::LN * sizeof(R)) +
+      (size_t)CF::LN * rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), CF::LN) * sizeof(T);
   const dim3 grid((g.nu + 2 + CF::LN - 1) / CF::LN, g.nb);
   auto k = prer_rc_kernel<T, R, CF>;
   cudaError_t e = rc_attr(k, smem);
   if (e != cudaSuccess) return e;
-  k<<<grid, nt, smem, st>>>(G, C, g, tr);
+  k<<<grid, nt, smem, st>>>(G, C, g, tr, err);
   return cudaGetLastError();
 }
 
@@ -924,18 +1014,18 @@ cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *s
 
 template <typename T, typename R>
 cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
-                           cudaStream_t st) {
+                           unsigned int *err, cudaStream_t st) {
   switch (cfg) {
     case 0:
-      return prer_rc_go<T, R, CfgA>(G, C, g, tr, st);
+      return prer_rc_go<T, R, CfgA>(G, C, g, tr, err, st);
     case 1:
-      return prer_rc_go<T, R, CfgA1>(G, C, g, tr, st);
+      return prer_rc_go<T, R, CfgA1>(G, C, g, tr, err, st);
     case 2:
-      return prer_rc_go<T, R, CfgB>(G, C, g, tr, st);
+      return prer_rc_go<T, R, CfgB>(G, C, g, tr, err, st);
     case 3:
-      return prer_rc_go<T, R, CfgB1>(G, C, g, tr, st);
+      return prer_rc_go<T, R, CfgB1>(G, C, g, tr, err, st);
     case 4:
-      return prer_rc_go<T, R, CfgC>(G, C, g, tr, st);
+      return prer_rc_go<T, R, CfgC>(G, C, g, tr, err, st);
     default:
       return cudaErrorInvalidValue;
   }
@@ -993,7 +1083,7 @@ template cudaError_t launch_ucol_adj_rc<double>(const double *, const double *, 
                                             const Geometry &, const RcDir<R> &,          \
                                             cudaStream_t);                               \
   template cudaError_t launch_prer_rc<T, R>(int, const T *, T *, const Geometry &,       \
-                                            const RcDir<R> &, cudaStream_t);
+                                            const RcDir<R> &, unsigned int *, cudaStream_t);
 VLS_RC_INST(double, double)
 VLS_RC_INST(float, double)
 VLS_RC_INST(float, float)
