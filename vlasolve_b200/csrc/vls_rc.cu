@@ -85,6 +85,18 @@ __device__ __forceinline__ T w_bv1(T x) {
   return T(1) + T(3) * x + T(3) * x * x - T(3) * x * x * x;
 }
 
+// w / 6 without a division: FP32 multiplies by 1/6 split into a rounded
+// head and its remainder (one multiply, one FMA), so the quotient carries no
+// rounding bias of the constant; FP64 multiplies by the rounded 1/6
+template <typename T>
+__device__ __forceinline__ T over6(T w) {
+  return w * (T(1) / T(6));
+}
+template <>
+__device__ __forceinline__ float over6<float>(float w) {
+  return __fmaf_rn(w, 0.1666666716337204f, w * -4.967053879312289e-09f);
+}
+
 __host__ __device__ constexpr size_t al16(size_t b) { return (b + 15) / 16 * 16; }
 
 // chunk index, role and activity of this thread
@@ -301,10 +313,10 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
       if (fast) {
         const int o = (int)fl;
         const T fr = (T)frd;
-        // weights divided by 6 (a rounded 1/6 factor would bias every kick
-        // the same way, a steady mass drift in FP32)
-        const T w0 = w_bv2<T>(T(1) - fr) / T(6), w1 = w_bv1<T>(T(1) - fr) / T(6);
-        const T w2 = w_bv1<T>(fr) / T(6), w3 = w_bv2<T>(fr) / T(6);
+        // weights divided by 6 (a single rounded 1/6 factor would bias every
+        // kick the same way, a steady mass drift in FP32)
+        const T w0 = over6(w_bv2<T>(T(1) - fr)), w1 = over6(w_bv1<T>(T(1) - fr));
+        const T w2 = over6(w_bv1<T>(fr)), w3 = over6(w_bv2<T>(fr));
         const int ulo = (int)floor(-qf) + 1;
         const int uhi = (int)ceil((double)(N - 1) - qf) - 1;
         // row k = kfirst + i (u = k - 1) reads coefficient rows k+o-1 .. k+o+2
@@ -342,9 +354,8 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
               const T fr = (T)(y - yf);
               const int Ny = 1 + (int)yf;
               const T *p = kb + (ptrdiff_t)(Ny - 1) * LN + ro.ln;
-              x = (R)((w_bv2<T>(T(1) - fr) * p[0] + w_bv1<T>(T(1) - fr) * p[LN] +
-                       w_bv1<T>(fr) * p[2 * LN] + w_bv2<T>(fr) * p[3 * LN]) /
-                      T(6));
+              x = (R)over6(w_bv2<T>(T(1) - fr) * p[0] + w_bv1<T>(T(1) - fr) * p[LN] +
+                           w_bv1<T>(fr) * p[2 * LN] + w_bv2<T>(fr) * p[3 * LN]);
             }
           }
           v[i] = x;
