@@ -241,6 +241,30 @@ int vls_adjoint_forward(vls_handle *h, int32_t nsteps, int32_t checkpoint_every)
 int vls_adjoint_backward(vls_handle *h, const double *dbins, int64_t nbins, double *df0,
                          size_t ncells, double *dchain0, int64_t nelems);
 
+/* Second level of checkpoints for the adjoint (no counterpart in the
+   reference).  The backward pass recomputes a segment of checkpoint_every
+   steps and keeps each of its states on the device; when those states do not
+   fit (a 1025 x 1025 x 512 FP32 grid is 2.15 GB per state, 215 GB for a
+   segment of 100 steps), it first runs through the segment keeping a
+   checkpoint every inner_every steps and then recomputes and transposes one
+   sub-segment of inner_every steps at a time: device memory of inner_every
+   states plus ceil(checkpoint_every / inner_every) checkpoints, at the cost
+   of one more forward run.  inner_every = 0 (the default) chooses it at each
+   backward pass from the free device memory: one level when the segment's
+   states fit, else the spacing that stores the fewest states (about
+   sqrt(checkpoint_every): the extra forward run costs the same for every
+   spacing).  vls_adjoint_inner_used
+   returns the spacing the last backward pass used (0: one level).  The
+   gradient does not depend on the choice: the recomputed states are the
+   same. */
+int vls_adjoint_set_inner(vls_handle *h, int32_t inner_every);
+/* Device memory the handle holds, in bytes: grid, coefficients, footpoint
+   tables, chains, moments and, once used, the adjoint's checkpoints, stash
+   and FP64 arrays (no counterpart in the reference).  A handle frees its
+   memory only in vls_destroy, so this is also its peak. */
+int vls_device_bytes(vls_handle *h, size_t *bytes);
+int vls_adjoint_inner_used(vls_handle *h, int32_t *inner_every);
+
 /* Radial moment of a grid that already lives in device memory, without any
    allocation (no counterpart in the reference, whose grid is host memory).
    For callers that own all device memory and must not let a library call

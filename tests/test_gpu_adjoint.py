@@ -75,6 +75,36 @@ def test_checkpoint_interval_does_not_change_gradient(K):
     np.testing.assert_allclose(g, g_ref, rtol=1e-10, atol=1e-14 * np.max(np.abs(g_ref)))
 
 
+@pytest.mark.parametrize("inner", [1, 2, 3])
+def test_second_level_checkpoints_do_not_change_gradient(inner):
+    """Segments of 5 steps split into sub-segments of `inner` steps (the last
+    one shorter for 2 and 3) give the gradient of the one-level pass."""
+    p_ref = problem(K=5)
+    target = p_ref.run(THETA + DTHETA)
+    _, g_ref = loss_and_grad(p_ref, target)
+    assert p_ref.solver.adjoint_inner_used() == 0
+    p = problem(K=5)
+    p.solver.adjoint_set_inner(inner)
+    _, g = loss_and_grad(p, target)
+    assert p.solver.adjoint_inner_used() == inner
+    np.testing.assert_allclose(g, g_ref, rtol=1e-10, atol=1e-14 * np.max(np.abs(g_ref)))
+    # after a backward pass the handle holds the final state of the forward
+    # run (vjp re-initialised this FP64 handle for the initial-state map, so
+    # run the forward again first)
+    s = p.solver
+    p.run(THETA)
+    f_final = s.f
+    s.adjoint_backward(np.linspace(0.0, 1.0, s.nr))
+    np.testing.assert_array_equal(s.f, f_final)
+
+
+def test_second_level_rejects_negative_spacing():
+    from vlasolve_b200._lib import VlsError
+    p = problem()
+    with pytest.raises(VlsError):
+        p.solver.adjoint_set_inner(-1)
+
+
 def test_backward_restores_final_state_and_repeats():
     p = problem()
     p.run(THETA)

@@ -29,7 +29,8 @@ EXPORTED = [
     "vls_moments", "vls_last_mass", "vls_stats", "vls_get_time", "vls_set_time",
     "vls_write_ndfield", "vls_read_ndfield", "vls_stream", "vls_set_profiling",
     "vls_profile_read", "vls_radial_mass_noalloc", "vls_noalloc_last_error",
-    "vls_adjoint_forward", "vls_adjoint_backward", "vls_write_restart",
+    "vls_adjoint_forward", "vls_adjoint_backward", "vls_adjoint_set_inner",
+    "vls_adjoint_inner_used", "vls_device_bytes", "vls_write_restart",
     "vls_restart_info", "vls_read_restart",
 ]
 KERNEL_KINDS = ["ucol_kick", "ucol", "prer", "tails", "drift", "scan", "moment",
@@ -122,6 +123,9 @@ def load(path: str = LIB_PATH):
         "vls_read_restart": [H, ctypes.c_char_p],
         "vls_adjoint_forward": [H, i32, i32],
         "vls_adjoint_backward": [H, P(d), i64, P(d), ctypes.c_size_t, P(d), i64],
+        "vls_adjoint_set_inner": [H, i32],
+        "vls_adjoint_inner_used": [H, P(i32)],
+        "vls_device_bytes": [H, P(ctypes.c_size_t)],
         "vls_radial_mass_noalloc": [ctypes.c_void_p, i32, i64, i64, i64, P(d), P(d), P(d),
                                     P(d), ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, i32],

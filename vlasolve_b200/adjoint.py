@@ -29,8 +29,11 @@ class DensityProblem:
 
     def __init__(self, cfg, precision: str = "fp64", nsteps: int = 1,
                  checkpoint_every: int = 1, params=("R0", "alpha", "smoothingRadius"),
-                 ic_step: float = 1e-6, device: int = 0):
+                 ic_step: float = 1e-6, device: int = 0, inner_every: int = 0):
         self.solver = VlasovSolver21Spline(cfg, precision=precision, device=device, init=False)
+        # second-level checkpoint spacing of the backward pass (0: chosen from
+        # free device memory)
+        self.solver.adjoint_set_inner(inner_every)
         # the initial-state map is differenced in FP64 whatever the storage
         # precision (differences of FP32-rounded grids would lose the digits)
         self.ic = (self.solver if precision == "fp64" else

@@ -119,6 +119,12 @@ struct vls_handle {
   Ckpt adj_final;
   int64_t adj_n = 0;
   int adj_K = 0, adj_ncp = 0;
+  // second level: checkpoints every adj_inner steps inside a segment (0:
+  // chosen from free device memory at the backward pass), kept between calls
+  int adj_inner = 0, adj_last_inner = 0;
+  // device bytes this handle holds (its allocations are freed by vls_destroy only)
+  size_t dev_bytes = 0, far_bytes = 0;
+  std::vector<Ckpt> adj_sub;
   // backward-pass arrays (FP64) and the segment stash, kept between calls
   double *ab_lam = nullptr, *ab_Cb = nullptr, *ab_Gb = nullptr, *ab_A = nullptr,
          *ab_B = nullptr, *ab_ringb = nullptr, *ab_sbar = nullptr, *ab_beta = nullptr;
@@ -158,6 +164,7 @@ static int dalloc(vls_handle *h, P **p, size_t bytes) {
                     cudaGetErrorString(e));
   }
   h->allocs.push_back(q);
+  h->dev_bytes += bytes;
   *p = reinterpret_cast<P *>(q);
   return VLS_OK;
 }
@@ -326,6 +333,8 @@ static int upload_far(vls_handle *h, const FarHost &fh) {
   release(h->far_cell);
   release(h->far_col);
   release(h->far_prod);
+  h->dev_bytes -= h->far_bytes;
+  h->far_bytes = 0;
   h->far_w = nullptr;
   h->far_cell = nullptr;
   h->far_col = nullptr;
@@ -338,6 +347,10 @@ static int upload_far(vls_handle *h, const FarHost &fh) {
   CK(h, cudaMalloc(&h->far_cell, sizeof(uint32_t) * std::max<size_t>(fh.cell.size(), 1)));
   CK(h, cudaMalloc(&h->far_col, sizeof(int32_t) * col.size()));
   CK(h, cudaMalloc(&h->far_prod, sizeof(double) * std::max<size_t>(fh.w.size(), 1)));
+  h->far_bytes = (sizeof(uint2) + sizeof(uint32_t) + sizeof(double)) *
+                     std::max<size_t>(fh.w.size(), 1) +
+                 sizeof(int32_t) * col.size();
+  h->dev_bytes += h->far_bytes;
   h->far_col_h = col;
   if (!fh.w.empty()) {
     TRY(upload(h, h->far_w, fh.w.data(), sizeof(uint2) * fh.w.size()));
@@ -574,6 +587,7 @@ static void free_all(vls_handle *h) {
   for (void *p : h->adj_allocs) cudaFree(p);
   h->adj_allocs.clear();
   h->adj_ck.clear();
+  h->adj_sub.clear();
   h->adj_final = vls_handle::Ckpt();
   h->ab_lam = h->ab_Cb = h->ab_Gb = h->ab_A = h->ab_B = nullptr;
   h->ab_ringb = h->ab_sbar = h->ab_beta = nullptr;
@@ -581,6 +595,8 @@ static void free_all(vls_handle *h) {
   for (void *p : {(void *)h->far_w, (void *)h->far_cell, (void *)h->far_col,
                   (void *)h->far_prod})
     if (p) cudaFree(p);
+  h->dev_bytes = 0;
+  h->far_bytes = 0;
   h->far_w = nullptr;
   h->far_cell = nullptr;
   h->far_col = nullptr;
@@ -1542,6 +1558,7 @@ static int adj_alloc(vls_handle *h, P **p, size_t bytes) {
                     cudaGetErrorString(e));
   }
   h->adj_allocs.push_back(q);
+  h->dev_bytes += bytes;
   *p = reinterpret_cast<P *>(q);
   return VLS_OK;
 }
@@ -1673,31 +1690,78 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
   b.sbar = h->ab_sbar;
   b.beta = h->ab_beta;
   const int K = h->adj_K;
-  while ((int)h->ab_stash.size() < K) {
+  // states stashed per pass: the whole segment (K), or with a second level of
+  // checkpoints every K2 steps, K2 states plus ceil(K / K2) checkpoints
+  int K2 = h->adj_inner > 0 ? std::min(h->adj_inner, K) : K;
+  if (h->adj_inner <= 0) {
+    size_t fr = 0, tot = 0;
+    CK(h, cudaMemGetInfo(&fr, &tot));
+    const size_t state = h->esize * cells, ckb = state + h->esize * (size_t)h->nel;
+    const size_t have = h->ab_stash.size() * state + h->adj_sub.size() * ckb;
+    const size_t margin = std::max<size_t>(tot / 50, (size_t)1 << 30);
+    const size_t room = (fr > margin ? fr - margin : 0) + have;
+    if ((size_t)K * state > room) {
+      // two levels cost one more forward run whatever the spacing, so take
+      // the spacing with the fewest stored states, K2 + ceil(K / K2) (about
+      // 2 sqrt(K)); the larger spacing on a tie
+      K2 = 1;
+      for (int k = 1; k < K; ++k)
+        if (k + (K + k - 1) / k <= K2 + (K + K2 - 1) / K2) K2 = k;
+      if ((size_t)K2 * state + (size_t)((K + K2 - 1) / K2) * ckb > room)
+        return fail(h, VLS_ENOMEM,
+                    "adjoint: the states of one segment do not fit in device memory");
+    }
+  }
+  const bool two_level = K2 < K;
+  while ((int)h->ab_stash.size() < K2) {
     void *q = nullptr;
     TRY(adj_alloc(h, &q, h->esize * cells));
     h->ab_stash.push_back(q);
   }
-  b.stash.assign(h->ab_stash.begin(), h->ab_stash.begin() + K);
-  b.ndrift.assign(K, 0);
+  if (two_level && (int)h->adj_sub.size() < (K + K2 - 1) / K2)
+    h->adj_sub.resize((K + K2 - 1) / K2);  // entries allocate on first save
+  b.stash.assign(h->ab_stash.begin(), h->ab_stash.begin() + K2);
+  b.ndrift.assign(K2, 0);
   // seed: the derivative of the loss with respect to the final radial bins
   TRY(upload(h, b.beta, dbins, (size_t)g.nr * sizeof(double)));
   CK(h, cudaMemsetAsync(b.lam, 0, cells * sizeof(double), h->st));
   CK(h, cudaMemsetAsync(b.ringb, 0, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double), h->st));
   CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
+  // from the state at step a: stash the states of steps a .. b-1, then apply
+  // the transposed steps b-1 .. a
+  auto pass = [&](int64_t a, int64_t e) -> int {
+    for (int64_t n = a; n < e; ++n) {
+      CK(h, cudaMemcpyAsync(b.stash[n - a], h->f, h->esize * cells, cudaMemcpyDeviceToDevice,
+                            h->st));
+      b.ndrift[n - a] = h->ndrift;
+      if (n + 1 < e) TRY(vls_step(h, 1));
+    }
+    for (int64_t n = e - 1; n >= a; --n) TRY(adj_step<T>(h, b, b.stash[n - a], b.ndrift[n - a]));
+    return VLS_OK;
+  };
   const int ncp = h->adj_ncp;
   for (int seg = ncp - 1; seg >= 0; --seg) {
     const int64_t n0 = (int64_t)seg * K;
     const int64_t n1 = std::min<int64_t>(n0 + K, h->adj_n);
     TRY(ckpt_load(h, h->adj_ck[seg]));
-    for (int64_t n = n0; n < n1; ++n) {
-      CK(h, cudaMemcpyAsync(b.stash[n - n0], h->f, h->esize * cells, cudaMemcpyDeviceToDevice,
-                            h->st));
-      b.ndrift[n - n0] = h->ndrift;
-      if (n + 1 < n1) TRY(vls_step(h, 1));
+    if (!two_level || n1 - n0 <= K2) {
+      TRY(pass(n0, n1));
+      continue;
     }
-    for (int64_t n = n1 - 1; n >= n0; --n) TRY(adj_step<T>(h, b, b.stash[n - n0], b.ndrift[n - n0]));
+    // second level: run through the segment keeping a state every K2 steps,
+    // then take its sub-segments from the last
+    const int nsub = (int)((n1 - n0 + K2 - 1) / K2);
+    for (int s = 0; s < nsub; ++s) {
+      TRY(ckpt_save(h, h->adj_sub[s]));
+      if (s + 1 < nsub) TRY(vls_step(h, K2));
+    }
+    for (int s = nsub - 1; s >= 0; --s) {
+      TRY(ckpt_load(h, h->adj_sub[s]));
+      const int64_t a = n0 + (int64_t)s * K2;
+      TRY(pass(a, std::min<int64_t>(a + K2, n1)));
+    }
   }
+  h->adj_last_inner = two_level ? K2 : 0;
   // results: the derivative with respect to the initial grid and the initial
   // chain values (logical ring order at the first step)
   CK(h, cudaMemcpyAsync(df0, b.lam, cells * sizeof(double), cudaMemcpyDeviceToHost, h->st));
@@ -1717,6 +1781,25 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
   // back to the final state of the forward run
   TRY(ckpt_load(h, h->adj_final));
   CK(h, cudaGetLastError());
+  return VLS_OK;
+}
+
+extern "C" int vls_device_bytes(vls_handle *h, size_t *bytes) {
+  if (!h || !bytes) return VLS_EINVAL;
+  *bytes = h->dev_bytes;
+  return VLS_OK;
+}
+
+extern "C" int vls_adjoint_set_inner(vls_handle *h, int32_t inner_every) {
+  if (!h) return VLS_EINVAL;
+  if (inner_every < 0) return fail(h, VLS_EINVAL, "adjoint: inner_every must be >= 0");
+  h->adj_inner = inner_every;
+  return VLS_OK;
+}
+
+extern "C" int vls_adjoint_inner_used(vls_handle *h, int32_t *inner_every) {
+  if (!h || !inner_every) return VLS_EINVAL;
+  *inner_every = h->adj_last_inner;
   return VLS_OK;
 }
 

@@ -378,6 +378,23 @@ class VlasovSolver21Spline:
             _dptr(dch) if ne.value else None, ne.value))
         return df0, dch
 
+    def adjoint_set_inner(self, inner_every: int = 0):
+        """Second-level checkpoint spacing of the backward pass (0: chosen
+        from free device memory; vls_adjoint_set_inner)."""
+        self._ck(self._L.vls_adjoint_set_inner(self._h, int(inner_every)))
+
+    def adjoint_inner_used(self) -> int:
+        """Second-level spacing the last backward pass used (0: one level)."""
+        v = ctypes.c_int32()
+        self._ck(self._L.vls_adjoint_inner_used(self._h, ctypes.byref(v)))
+        return v.value
+
+    def device_bytes(self) -> int:
+        """Device memory the handle holds (vls_device_bytes); also its peak."""
+        v = ctypes.c_size_t()
+        self._ck(self._L.vls_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
     def set_init_params(self, **kw):
         """Changes init.* parameters (R0, alpha, smoothingRadius, M, eta, n, Ra)
         and regenerates the initial state."""
