@@ -443,6 +443,113 @@ def adjoint_block(nsteps, K):
     return out
 
 
+# large case: PLDF (M=1, n=1, alpha=1, eta=0.1, smoothingRadius=0.5) on
+# 1025 x 1025 x 512 (FP32 f of 2.15 GB), the PLDF default ranges (r log on
+# [0.01, 200], v_r within 16 sigma, J quadratic on [0, 1.6]), dt = 0.005;
+# the gradient check runs the same problem on 257 x 257 x 128
+LARGE = dict(type="PLDF", M=1.0, n=1.0, alpha=1.0, eta=0.1, smoothingRadius=0.5,
+             Pres=1024, Ures=(1024, 512), dt=0.005)
+LARGE_SUB = dict(LARGE, Pres=256, Ures=(256, 128))
+LARGE_PARAMS = ("n", "alpha", "smoothingRadius")
+
+
+def large_block(nsteps, K):
+    """Forward cell updates/s, device memory and the adjoint (checkpoint every
+    K steps, second level chosen from free memory) of the 1025 x 1025 x 512
+    PLDF case; FP32-storage gradient against the FP64 adjoint on the
+    257 x 257 x 128 grid.  Loss ||rho(theta) - rho(theta + dtheta)||_2 of the
+    final radial density, theta = (n, alpha, smoothingRadius)."""
+    import numpy as np
+    import torch
+    from vlasolve_b200.adjoint import DensityProblem, final_density
+    theta = np.array([1.0, 1.0, 0.5])
+    dtheta = np.array([0.05, -0.02, 0.03])
+    out = {"workload": "pldf_1024x1024x512", "steps": nsteps, "checkpoint_every": K,
+           "params": list(LARGE_PARAMS), "theta": theta.tolist(),
+           "loss": "||rho - rho_target||_2, rho_target at theta + " + str(dtheta.tolist())}
+    t_all = time.perf_counter()
+    free0, total = torch.cuda.mem_get_info()
+    t0 = time.perf_counter()
+    p = DensityProblem(LARGE, precision="fp32", nsteps=nsteps, checkpoint_every=K,
+                       params=LARGE_PARAMS)
+    s = p.solver
+    s.set_init_params(**dict(zip(LARGE_PARAMS, map(float, theta))))
+    s.sync()
+    out["setup_s"] = time.perf_counter() - t0
+    out["cells"] = s.nr * s.nu * s.nj
+    out["grid"] = [s.nr, s.nu, s.nj]
+    fwd_bytes = s.device_bytes()
+    # plain forward, device time on the solver's stream
+    stream = torch.cuda.ExternalStream(s.stream_ptr())
+    s.step(3)
+    s.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(nsteps)
+    e1.record(stream)
+    s.sync()
+    ms = e0.elapsed_time(e1)
+    out["forward_ms_per_step"] = ms / nsteps
+    out["value"] = out["cells"] * nsteps / (ms * 1e-3)
+    out["unit"] = "cell updates/s"
+    # adjoint
+    target = p.run(theta + dtheta)
+    th = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
+    t1 = time.perf_counter()
+    rho = final_density(th, p)
+    s.sync()
+    t2 = time.perf_counter()
+    L = torch.linalg.norm(rho - torch.as_tensor(target))
+    L.backward()
+    s.sync()
+    t3 = time.perf_counter()
+    free1, _ = torch.cuda.mem_get_info()
+    # the step adjoint alone (recomputation included, initial-state map
+    # excluded): one more backward pass with the same seed
+    dbins = np.zeros(s.nr)
+    dbins[:-1] = (rho.detach().numpy() - target) / np.linalg.norm(rho.detach().numpy() - target)
+    dbins[:-1] /= s.shell_volumes()
+    s.sync()
+    ta = time.perf_counter()
+    s.adjoint_backward(dbins)
+    s.sync()
+    out["step_adjoint_s"] = time.perf_counter() - ta
+    out["step_adjoint_ms_per_step"] = 1e3 * out["step_adjoint_s"] / nsteps
+    out["grad"] = th.grad.numpy().tolist()
+    out["loss_value"] = float(L.detach())
+    out["forward_checkpointed_s"] = t2 - t1
+    out["backward_s"] = t3 - t2
+    out["inner_every_used"] = s.adjoint_inner_used()
+    out["hbm_gb"] = {"step_handle_forward": fwd_bytes / 1e9,
+                     "step_handle_with_adjoint": s.device_bytes() / 1e9,
+                     "initial_state_handle_fp64": p.ic.device_bytes() / 1e9,
+                     "device_used_after_backward": (total - free1) / 1e9,
+                     "device_used_before": (total - free0) / 1e9}
+    p.ic.close()
+    s.close()
+    del p
+    # gradient of the FP32-storage adjoint against the FP64 adjoint, 257 x 257 x 128
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        q = DensityProblem(LARGE_SUB, precision=prec, nsteps=nsteps, checkpoint_every=K,
+                           params=LARGE_PARAMS)
+        if prec == "fp64":
+            tgt = q.run(theta + dtheta)
+        th = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
+        Lq = torch.linalg.norm(final_density(th, q) - torch.as_tensor(tgt))
+        Lq.backward()
+        grads[prec] = th.grad.numpy().copy()
+        if q.ic is not q.solver:
+            q.ic.close()
+        q.solver.close()
+    out["subsample"] = {"workload": "pldf_256x256x128", "grad_fp64": grads["fp64"].tolist(),
+                        "grad_fp32": grads["fp32"].tolist(),
+                        "fp32_vs_fp64_rel": float(np.max(np.abs(grads["fp32"] - grads["fp64"]))
+                                                  / np.max(np.abs(grads["fp64"])))}
+    out["seconds"] = time.perf_counter() - t_all
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -493,11 +600,17 @@ def main():
     ap.add_argument("--quick", action="store_true",
                     help="timing of the chosen precision only (for profiler runs)")
     ap.add_argument("--workload", default=WORKLOAD_NAME, choices=sorted(WORKLOADS))
+    ap.add_argument("--large", action="store_true",
+                    help="only the 1025 x 1025 x 512 PLDF forward + adjoint block")
+    ap.add_argument("--large-steps", type=int, default=1000)
+    ap.add_argument("--large-every", type=int, default=100)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         reference_arm(args)
+    elif args.large:
+        print(json.dumps({"large": large_block(args.large_steps, args.large_every)}), flush=True)
     else:
         gpu_arm(args)
 
