@@ -77,6 +77,7 @@ template <typename R>
 struct RcDir {
   R rp0[32], m0[32], q0[32];  // rp_k, -rp_k/6, q_k for rows k = 0..31
   R mpow[33], qpow[33];       // (-rp_inf/6)^i and (-q_inf)^i, i = 0..32
+  R qfirst[32];               // prod_{k=i}^{L-1} (-q_{1+k}), i = 0..L-1 (first chunk)
   R rp_inf, m_inf, q_inf;
   R a01, a02, hi2, L1, L2;
   int N, L, S;                // data rows, rows per chunk, chunks

@@ -230,6 +230,154 @@ __device__ __forceinline__ void rc_solve(R (&v)[C::L], const Role &ro, R *dend, 
   }
 }
 
+// ------------------------------------------------- forward solve layout
+// The forward kernels use a second layout in which no warp runs two chunk
+// kinds one after the other: warp 0 holds only the first chunk (lanes
+// 0..LN-1; its other lanes compute the same chunk and store nothing), and
+// the last chunk follows the middle chunks in the other warps.  Per phase:
+//   A  every chunk: local forward recurrence (the first with its per-row
+//      coefficients, exact since it starts at row 1)
+//   B  first chunk: local backward from zero with its per-row q;
+//      others: forward correction by the carry, then the backward from zero
+//      (the last chunk from its boundary row, exact)
+//   C  first chunk: backward correction qfirst[i] * carry (independent
+//      products instead of the dependent exact backward), then c_0;
+//      middle chunks: qpow[L - i] * carry
+// so every warp's dependent chains are one forward and one backward pass.
+template <class C>
+__host__ __device__ constexpr int rc2_maxs() {
+  return 1 + (C::NT / 32 - 1) * C::CPW;
+}
+template <class C>
+int rc2_threads(int S) {
+  return S == 1 ? 32 : 32 * (1 + (S - 1 + C::CPW - 1) / C::CPW);
+}
+template <class C>
+__device__ __forceinline__ Role rc2_role(int S) {
+  Role o;
+  const int lane = threadIdx.x & 31;
+  o.warp = threadIdx.x >> 5;
+  o.grp = lane / C::LN;
+  o.ln = lane % C::LN;
+  if (o.warp == 0) {
+    o.s = 0;
+    o.active = o.grp == 0;
+  } else {
+    o.s = 1 + (o.warp - 1) * C::CPW + o.grp;
+    o.active = o.s <= S - 1;
+  }
+  return o;
+}
+
+template <typename R, class C>
+__device__ __forceinline__ void rc2_solve(R (&v)[C::L], const Role &ro, R *dend, R *cst,
+                                          const RcDir<R> &t, R &c0, R &cM) {
+  constexpr int L = C::L, LN = C::LN;
+  const int S = t.S, N = t.N;
+  const int s = ro.s;
+  const int kfirst = 1 + s * L;
+  const int slot = s * LN + ro.ln;
+  // the warp holding the last chunk (its other lanes hold middle chunks)
+  const bool lastwarp = ro.warp == (S - 2) / C::CPW + 1;
+  // ---------------------------------------------------------- phase A
+  if (s == 0) {
+    R d = R(0);
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      d = rfma(d, t.m0[1 + i], v[i] * t.rp0[1 + i]);
+      v[i] = d;
+    }
+    if (ro.active && S >= 2) dend[slot] = d;
+  } else {
+    R d = R(0);
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      d = rfma(d, t.m_inf, v[i] * t.rp_inf);
+      v[i] = d;
+    }
+    if (ro.active) dend[slot] = d;
+  }
+  __syncthreads();
+  // ---------------------------------------------------------- phase B
+  if (S == 1) {
+    // the only chunk is first and last: exact recurrences throughout
+    const int iN = N - 1;
+    R dl = v[0], dp = R(0);
+#pragma unroll
+    for (int i = 1; i < L; ++i)
+      if (i == iN) {
+        dl = v[i];
+        dp = v[i - 1];
+      }
+    cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+    R c = cM;
+#pragma unroll
+    for (int i = L - 1; i >= 0; --i)
+      if (i <= iN) {
+        c = rfma(-t.q0[1 + i], c, v[i]);
+        v[i] = c;
+      }
+    c0 = (R(0) - t.a01 * v[0]) - t.a02 * (N >= 2 ? v[1] : cM);
+  } else if (s == 0) {
+    R c = R(0);
+#pragma unroll
+    for (int i = L - 1; i >= 0; --i) {
+      c = rfma(-t.q0[1 + i], c, v[i]);
+      v[i] = c;
+    }
+  } else {
+    // lanes past the last chunk read nothing (their slots lie past dend)
+    R carry = ro.active ? dend[slot - LN] : R(0);
+    if (s >= 2 && ro.active) carry = rfma(t.mpow[L], dend[slot - 2 * LN], carry);
+#pragma unroll
+    for (int i = 0; i < L; ++i) v[i] = rfma(t.mpow[i + 1], carry, v[i]);
+    R c = R(0);
+    if (lastwarp) {
+      // the last chunk starts from its boundary row; rows past N skipped
+      const bool last = s == S - 1;
+      const int iN = last ? N - kfirst : L - 1;  // 0 .. L-1
+      if (last) {
+        R dl = v[0], dp = carry;
+#pragma unroll
+        for (int i = 1; i < L; ++i)
+          if (i == iN) {
+            dl = v[i];
+            dp = v[i - 1];
+          }
+        cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+        c = cM;
+      }
+#pragma unroll
+      for (int i = L - 1; i >= 0; --i)
+        if (i <= iN) {
+          c = rfma(-t.q_inf, c, v[i]);
+          v[i] = c;
+        }
+    } else {
+#pragma unroll
+      for (int i = L - 1; i >= 0; --i) {
+        c = rfma(-t.q_inf, c, v[i]);
+        v[i] = c;
+      }
+    }
+    if (ro.active) cst[slot] = c;
+  }
+  __syncthreads();
+  // ---------------------------------------------------------- phase C
+  if (S >= 2 && s <= S - 2) {
+    R carry = cst[slot + LN];
+    if (s + 2 <= S - 1) carry = rfma(t.qpow[L], cst[slot + 2 * LN], carry);
+    if (s == 0) {
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = rfma(t.qfirst[i], carry, v[i]);
+      c0 = (R(0) - t.a01 * v[0]) - t.a02 * v[1];
+    } else {
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = rfma(t.qpow[L - i], carry, v[i]);
+    }
+  }
+}
+
 // ------------------------------------------------------------------ ucol
 // Block: LN r columns of one J slice; a column is a u line.  With KICK: the
 // u-solve of f, the kick gather (vlasovSolver21_spline.hxx:752-770 with the
@@ -248,7 +396,7 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   R *dend = reinterpret_cast<R *>(smem_raw);
   R *cst = dend + S * LN;
   T *kb = reinterpret_cast<T *>(smem_raw + al16(2 * (size_t)S * LN * sizeof(R)));
-  const Role ro = rc_role<CF>(S);
+  const Role ro = rc2_role<CF>(S);
   const int r = blockIdx.x * LN + ro.ln;
   const bool colok = r < g.nr;
   const int jl = blockIdx.y, j = g.j0 + jl;
@@ -276,7 +424,7 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
     }
   }
   R c0 = R(0), cM = R(0);
-  rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
+  rc2_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
   if (KICK) {
     // chunks wholly inside the line (every chunk but the last) store without
     // per-row tests
@@ -362,7 +510,7 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
         }
       }
     }
-    rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
+    rc2_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
   }
   if (ro.active && colok) {
     T *Gc = G + (size_t)jl * M * g.gp + r;
@@ -444,7 +592,7 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   R *dend = reinterpret_cast<R *>(smem_raw);
   R *cst = dend + S * LN;
   T *tile = reinterpret_cast<T *>(smem_raw + al16(2 * (size_t)S * LN * sizeof(R)));
-  const Role ro = rc_role<CF>(S);
+  const Role ro = rc2_role<CF>(S);
   const int jl = blockIdx.y;
   const int rows = g.nu + 2;
   const int kr0 = blockIdx.x * LN;
@@ -489,7 +637,7 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
     }
   }
   R c0 = R(0), cM = R(0);
-  rc_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
+  rc2_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
   if (ro.active && lineok) {
     T *row = tile + ro.ln * P;
     if (kfirst + L - 1 <= N) {
@@ -546,6 +694,12 @@ bool cfg_fits(int N, int kc) {
   const int S = (N + CF::L - 1) / CF::L;
   return N >= 2 && kc <= 1 + CF::L && S <= CF::MAXS;
 }
+// the same for the forward kernels' layout (rc2_role)
+template <class CF>
+bool cfg2_fits(int N, int kc) {
+  const int S = (N + CF::L - 1) / CF::L;
+  return N >= 2 && kc <= 1 + CF::L && S <= rc2_maxs<CF>();
+}
 
 template <typename K>
 cudaError_t rc_attr(K kern, size_t smem) {
@@ -555,7 +709,7 @@ cudaError_t rc_attr(K kern, size_t smem) {
 template <typename T, typename R, bool KICK, class CF>
 cudaError_t ucol_rc_go(const T *f, T *G, const double *shift, const Geometry &g,
                        const RcDir<R> &tu, cudaStream_t st) {
-  const int nt = rc_threads<CF>(tu.S);
+  const int nt = rc2_threads<CF>(tu.S);
   if (tu.N != g.nu || nt > CF::NT || tu.L != CF::L) return cudaErrorInvalidValue;
   const size_t smem = al16(2 * (size_t)tu.S * CF::LN * sizeof(R)) +
                       (size_t)(tu.N + 3) * CF::LN * sizeof(T);
@@ -570,7 +724,7 @@ cudaError_t ucol_rc_go(const T *f, T *G, const double *shift, const Geometry &g,
 template <typename T, typename R, class CF>
 cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
                        unsigned int *err, cudaStream_t st) {
-  const int nt = rc_threads<CF>(tr.S);
+  const int nt = rc2_threads<CF>(tr.S);
   if (tr.N != g.nr || nt > CF::NT || tr.L != CF::L) return cudaErrorInvalidValue;
   // bulk rows: 16-byte rows of G and C, 16-byte aligned slices
   if (rc_bulk_rows<CF>() &&
@@ -957,13 +1111,13 @@ int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
   const int N = t.M - 2;
   const int kc = sizeof(R) == 8 ? t.kc64 : t.kc32;
   const std::string p = pref ? pref : "";
-  const int b = cfg_fits<CfgB>(N, kc) ? 2 : cfg_fits<CfgB1>(N, kc) ? 3 : -1;
-  if (p == "A") return cfg_fits<CfgA>(N, kc) ? 0 : cfg_fits<CfgA1>(N, kc) ? 1 : -1;
+  const int b = cfg2_fits<CfgB>(N, kc) ? 2 : cfg2_fits<CfgB1>(N, kc) ? 3 : -1;
+  if (p == "A") return cfg2_fits<CfgA>(N, kc) ? 0 : cfg2_fits<CfgA1>(N, kc) ? 1 : -1;
   if (p == "B") return b;
-  if (p == "C") return cfg_fits<CfgC>(N, kc) ? 4 : -1;
+  if (p == "C") return cfg2_fits<CfgC>(N, kc) ? 4 : -1;
   // default (fastest measured on 513 x 513 x 256): 16-line blocks for the u
   // lines, 8-line blocks for the r lines
-  if (u_lines && cfg_fits<CfgC>(N, kc)) return 4;
+  if (u_lines && cfg2_fits<CfgC>(N, kc)) return 4;
   return b;
 }
 
@@ -992,6 +1146,20 @@ RcDir<R> rc_dir(const HostDirTables &t, int cfg) {
     o.qpow[i] = (R)pq;
     pm *= m;
     pq *= -t.q_inf;
+  }
+  // first chunk's backward correction factors prod_{k=i}^{L-1} (-q_{1+k})
+  {
+    double pf = 1.0;
+    for (int i = 31; i >= 0; --i) {
+      if (i < L) {
+        const int k = 1 + i;
+        const double q = (k >= 1 && k <= M - 2) ? t.q[k] : t.q_inf;
+        pf *= -q;
+        o.qfirst[i] = (R)pf;
+      } else {
+        o.qfirst[i] = (R)0;
+      }
+    }
   }
   o.a01 = (R)t.a01;
   o.a02 = (R)t.a02;
