@@ -30,7 +30,9 @@
 // multiples of L, fall on distinct shared-memory banks.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 #include "vls_async.cuh"
@@ -44,14 +46,18 @@ namespace {
 template <int L_, int LN_, int NT_, int MINB_>
 struct RcCfg {
   static constexpr int L = L_, LN = LN_, CPW = 32 / LN_, NT = NT_, MINB = MINB_;
-  // most chunks one block holds: warp 0 + (NT/32 - 1) warps of CPW chunks
-  static constexpr int MAXS = 2 + (NT_ / 32 - 1) * (32 / LN_);
 };
+// most chunks one block holds in the adjoint kernels' layout: warp 0 (first
+// and last chunk) + (NT/32 - 1) warps of CPW chunks
+template <class C>
+__host__ __device__ constexpr int rc_maxs() {
+  return 2 + (C::NT / 32 - 1) * C::CPW;
+}
 // configuration ids (host and device agree on the order)
 using CfgA = RcCfg<31, 16, 320, 2>;   // 31-row chunks, 16 lines, two blocks per SM
 using CfgA1 = RcCfg<31, 16, 576, 1>;  // the same for up to 35 chunks
 using CfgB = RcCfg<15, 8, 320, 3>;    // 15-row chunks, 8 lines, three blocks per SM
-using CfgB1 = RcCfg<15, 8, 640, 1>;   // the same for up to 78 chunks
+using CfgB1 = RcCfg<15, 8, 640, 1>;   // the same for up to 77 chunks
 using CfgC = RcCfg<15, 16, 576, 2>;   // 15-row chunks, 16 lines, two blocks per SM
 
 template <typename R>
@@ -683,6 +689,136 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   }
 }
 
+// Persistent form of the bulk-row r-solve: each block walks groups of LN
+// rows (gid = blockIdx.x, + gridDim.x, ...) through RC_PIPE_TILES row tiles,
+// with the bulk loads of the next RC_PIPE_AHEAD groups in flight while it
+// solves one: a group's solve is shorter than an HBM load, and three
+// blocks of one group each keep too few bytes in flight per SM.  Thread 0
+// issues the loads, and the bulk stores of each group after its solve; a
+// tile is reloaded only once the stores issued from it have finished
+// reading it.  Waits are bounded: after a timeout the block stores nothing
+// more, waits (bounded) for its loads in flight and leaves, and the error
+// word tells the host.
+constexpr int RC_PIPE_TILES = 4, RC_PIPE_AHEAD = 2;
+
+template <typename T, typename R, class CF>
+__global__ void __launch_bounds__(CF::NT, CF::MINB)
+    prer_pipe_kernel(const T *__restrict__ G, T *__restrict__ C, Geometry g,
+                     const __grid_constant__ RcDir<R> t, unsigned int *err, int gps,
+                     int ngroups) {
+  constexpr int L = CF::L, LN = CF::LN;
+  static_assert(rc_bulk_rows<CF>(), "the pipelined r-solve needs bulk rows");
+  // the tile reloaded for group i + AHEAD was stored from at group
+  // i + AHEAD - TILES, at least two groups before: wait_group.read 1
+  static_assert(RC_PIPE_TILES - RC_PIPE_AHEAD >= 2, "tile reuse distance");
+  constexpr int OFF = (int)(16 / sizeof(T));  // word of x_1 in a tile row
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t bar[RC_PIPE_TILES];
+  __shared__ int bad;
+  const int S = t.S, N = t.N;  // N == g.nr
+  const int M = N + 2;
+  const int P = rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), LN);
+  R *dend = reinterpret_cast<R *>(smem_raw);
+  R *cst = dend + S * LN;
+  T *tiles = reinterpret_cast<T *>(smem_raw + al16(2 * (size_t)S * LN * sizeof(R)));
+  const Role ro = rc2_role<CF>(S);
+  const int rows = g.nu + 2;
+  const int cnt =
+      (int)blockIdx.x < ngroups ? (ngroups - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const uint32_t gbytes = (uint32_t)g.gp * sizeof(T), cbytes = (uint32_t)g.pc * sizeof(T);
+  auto group = [&](int i, int &jl, int &kr0, int &nrow) {
+    const int gid = (int)blockIdx.x + i * (int)gridDim.x;
+    jl = gid / gps;
+    kr0 = (gid - jl * gps) * LN;
+    nrow = min(LN, rows - kr0);
+  };
+  auto issue = [&](int i) {
+    int jl, kr0, nrow;
+    group(i, jl, kr0, nrow);
+    const int b = i % RC_PIPE_TILES;
+    T *tile = tiles + (size_t)b * LN * P;
+    const T *Gs = G + ((size_t)jl * rows + kr0) * g.gp;
+    mbar_expect_tx(&bar[b], gbytes * (uint32_t)nrow);
+    for (int p = 0; p < nrow; ++p)
+      bulk_load(tile + p * P + OFF, Gs + (size_t)p * g.gp, gbytes, &bar[b]);
+  };
+  int issued = 0;  // groups whose loads thread 0 issued
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < RC_PIPE_TILES; ++b) mbar_init(&bar[b], 1);
+    mbar_fence_init();
+    bad = 0;
+    for (; issued < RC_PIPE_AHEAD && issued < cnt; ++issued) issue(issued);
+  }
+  __syncthreads();
+  int i = 0;
+  for (; i < cnt; ++i) {
+    const int b = i % RC_PIPE_TILES;
+    const uint32_t par = (uint32_t)(i / RC_PIPE_TILES) & 1u;
+    T *tile = tiles + (size_t)b * LN * P;
+    if (threadIdx.x == 0 && i + RC_PIPE_AHEAD < cnt) {
+      asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+      issue(i + RC_PIPE_AHEAD);
+      issued = i + RC_PIPE_AHEAD + 1;
+    }
+    if (!mbar_wait_bounded(&bar[b], par)) {
+      atomicOr(err, 4u);
+      bad = 1;
+    }
+    int jl, kr0, nrow;
+    group(i, jl, kr0, nrow);
+    const bool lineok = ro.ln < nrow;
+    const int kfirst = 1 + ro.s * L;
+    R v[L];
+    {
+      const T *row = tile + ro.ln * P + (OFF - 1);
+      if (kfirst + L - 1 <= N) {
+#pragma unroll
+        for (int k = 0; k < L; ++k) v[k] = (R)row[kfirst + k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < L; ++k) v[k] = (R)row[min(kfirst + k, N)];
+      }
+    }
+    R c0 = R(0), cM = R(0);
+    rc2_solve<R, CF>(v, ro, dend, cst, t, c0, cM);
+    if (ro.active && lineok) {
+      T *row = tile + ro.ln * P;
+      if (kfirst + L - 1 <= N) {
+#pragma unroll
+        for (int k = 0; k < L; ++k) row[kfirst + k] = (T)v[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+          const int kk = kfirst + k;
+          if (kk <= N) row[kk] = (T)v[k];
+        }
+      }
+      if (ro.s == 0) row[0] = (T)c0;
+      if (ro.s == S - 1) {
+        row[M - 1] = (T)cM;
+        for (int k = M; k < g.pc; ++k) row[k] = T(0);
+      }
+    }
+    fence_proxy_async();  // this thread's tile writes, visible to the bulk copies
+    __syncthreads();
+    const bool stop = bad != 0;
+    if (threadIdx.x == 0 && !stop) {
+      T *Cs = C + ((size_t)jl * (g.nu + 3) + kr0) * g.pc;
+      for (int p = 0; p < nrow; ++p) bulk_store(Cs + (size_t)p * g.pc, tile + p * P, cbytes);
+      bulk_commit();
+    }
+    if (stop) break;
+  }
+  if (threadIdx.x == 0) {
+    bulk_wait_read();
+    // after a timeout: the loads issued beyond the failed group must land
+    // before the block's shared memory is released
+    for (int k = i + 1; k < issued; ++k)
+      if (!mbar_wait_bounded(&bar[k % RC_PIPE_TILES], (uint32_t)(k / RC_PIPE_TILES) & 1u))
+        atomicOr(err, 8u);
+  }
+}
+
 template <class CF>
 int rc_threads(int S) {
   const int warps = S == 1 ? 1 : 1 + (S - 2 + CF::CPW - 1) / CF::CPW;
@@ -692,7 +828,7 @@ int rc_threads(int S) {
 template <class CF>
 bool cfg_fits(int N, int kc) {
   const int S = (N + CF::L - 1) / CF::L;
-  return N >= 2 && kc <= 1 + CF::L && S <= CF::MAXS;
+  return N >= 2 && kc <= 1 + CF::L && S <= rc_maxs<CF>();
 }
 // the same for the forward kernels' layout (rc2_role)
 template <class CF>
@@ -735,6 +871,32 @@ cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
   const size_t smem =
       al16(2 * (size_t)tr.S * CF::LN * sizeof(R)) +
       (size_t)CF::LN * rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), CF::LN) * sizeof(T);
+  if constexpr (rc_bulk_rows<CF>()) {
+    static const bool pipe = [] {
+      const char *e = std::getenv("VLS_PRER_PIPE");
+      return !(e && std::string(e) == "0");
+    }();
+    if (pipe) {
+      // persistent blocks, as many as fit on the device at once
+      const size_t psmem = al16(2 * (size_t)tr.S * CF::LN * sizeof(R)) +
+                           (size_t)RC_PIPE_TILES * CF::LN *
+                               rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), CF::LN) * sizeof(T);
+      auto kp = prer_pipe_kernel<T, R, CF>;
+      cudaError_t e = rc_attr(kp, psmem);
+      if (e != cudaSuccess) return e;
+      int dev = 0, nsm = 0, per = 0;
+      if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+      if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kp, nt, psmem)) != cudaSuccess)
+        return e;
+      const int gps = (g.nu + 2 + CF::LN - 1) / CF::LN;
+      const int ngroups = gps * g.nb;
+      const int blocks = std::max(1, std::min(ngroups, nsm * std::max(per, 1)));
+      kp<<<blocks, nt, psmem, st>>>(G, C, g, tr, err, gps, ngroups);
+      return cudaGetLastError();
+    }
+  }
   const dim3 grid((g.nu + 2 + CF::LN - 1) / CF::LN, g.nb);
   auto k = prer_rc_kernel<T, R, CF>;
   cudaError_t e = rc_attr(k, smem);
