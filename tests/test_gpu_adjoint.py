@@ -98,6 +98,21 @@ def test_second_level_checkpoints_do_not_change_gradient(inner):
     np.testing.assert_array_equal(s.f, f_final)
 
 
+def test_device_bytes_counts_the_adjoint_buffers():
+    """vls_device_bytes: at least the grid, coefficients and footpoints after
+    set-up; it grows by the checkpoints, stash and FP64 arrays of the adjoint."""
+    p = problem(K=5)
+    s = p.solver
+    cells = s.nr * s.nu * s.nj
+    before = s.device_bytes()
+    assert before >= 3 * 8 * cells  # f, G, C in FP64 at least
+    p.run(THETA)
+    s.adjoint_backward(np.linspace(0.0, 1.0, s.nr))
+    after = s.device_bytes()
+    # 3 checkpoints + final state + 5 stashed states + lam, Cb, Gb (FP64)
+    assert after >= before + (3 + 1 + 5) * 8 * cells + 3 * 8 * cells
+
+
 def test_second_level_rejects_negative_spacing():
     from vlasolve_b200._lib import VlsError
     p = problem()
