@@ -890,11 +890,15 @@ cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
         return e;
       if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kp, nt, psmem)) != cudaSuccess)
         return e;
-      const int gps = (g.nu + 2 + CF::LN - 1) / CF::LN;
-      const int ngroups = gps * g.nb;
-      const int blocks = std::max(1, std::min(ngroups, nsm * std::max(per, 1)));
-      kp<<<blocks, nt, psmem, st>>>(G, C, g, tr, err, gps, ngroups);
-      return cudaGetLastError();
+      // only where it keeps the plain kernel's blocks per SM (four FP64
+      // tiles of a 513-column row group hold one block per SM)
+      if (per >= CF::MINB) {
+        const int gps = (g.nu + 2 + CF::LN - 1) / CF::LN;
+        const int ngroups = gps * g.nb;
+        const int blocks = std::max(1, std::min(ngroups, nsm * per));
+        kp<<<blocks, nt, psmem, st>>>(G, C, g, tr, err, gps, ngroups);
+        return cudaGetLastError();
+      }
     }
   }
   const dim3 grid((g.nu + 2 + CF::LN - 1) / CF::LN, g.nb);
