@@ -80,6 +80,7 @@ struct RcDir {
   R qfirst[32];               // prod_{k=i}^{L-1} (-q_{1+k}), i = 0..L-1 (first chunk)
   R rp_inf, m_inf, q_inf;
   R a01, a02, hi2, L1, L2;
+  R inv_L2;                   // 1 / L2 (the last row without a division)
   int N, L, S;                // data rows, rows per chunk, chunks
 };
 

@@ -7,7 +7,7 @@
 // recurrences there:
 //
 //   forward   d_k = (x_k - d_{k-1}/6) rp_k          (written d = d m_k + x rp_k)
-//   last row  c_{M-1} = ((0 - hi2 d_{N-1}) - L1 d_N) / L2
+//   last row  c_{M-1} = ((0 - hi2 d_{N-1}) - L1 d_N) / L2   (times 1/L2 from the host)
 //   backward  c_k = d_k - q_k c_{k+1},  c_0 = (0 - a01 c_1) - a02 c_2
 //
 // Chunks other than the first start their recurrence from zero and are
@@ -173,7 +173,7 @@ __device__ __forceinline__ void rc_solve(R (&v)[C::L], const Role &ro, R *dend, 
           dl = v[i];
           dp = v[i - 1];
         }
-      cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+      cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) * t.inv_L2;
       R c = cM;
 #pragma unroll
       for (int i = L - 1; i >= 0; --i)
@@ -197,7 +197,7 @@ __device__ __forceinline__ void rc_solve(R (&v)[C::L], const Role &ro, R *dend, 
             dl = v[i];
             dp = v[i - 1];
           }
-        cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+        cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) * t.inv_L2;
         c = cM;
 #pragma unroll
         for (int i = L - 1; i >= 0; --i)
@@ -315,7 +315,7 @@ __device__ __forceinline__ void rc2_solve(R (&v)[C::L], const Role &ro, R *dend,
         dl = v[i];
         dp = v[i - 1];
       }
-    cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+    cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) * t.inv_L2;
     R c = cM;
 #pragma unroll
     for (int i = L - 1; i >= 0; --i)
@@ -350,7 +350,7 @@ __device__ __forceinline__ void rc2_solve(R (&v)[C::L], const Role &ro, R *dend,
             dl = v[i];
             dp = v[i - 1];
           }
-        cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) / t.L2;
+        cM = ((R(0) - t.hi2 * dp) - t.L1 * dl) * t.inv_L2;
         c = cM;
       }
 #pragma unroll
@@ -1332,6 +1332,7 @@ RcDir<R> rc_dir(const HostDirTables &t, int cfg) {
   o.hi2 = (R)t.hi2;
   o.L1 = (R)t.L1;
   o.L2 = (R)t.L2;
+  o.inv_L2 = (R)(1.0 / t.L2);
   o.N = N;
   o.L = L;
   o.S = (N + L - 1) / L;
