@@ -213,6 +213,34 @@ class vlasovSolver21_spline {
   std::vector<double> getValCoord21_U() const { return coord(1); }
   std::vector<double> getValCoord21_J() const { return coord(2); }
 
+  // Adjoint of `nsteps` linked steps (no counterpart in the reference):
+  // adjointForward runs them keeping a checkpoint every `checkpointEvery`
+  // steps; adjointBackward takes dL/d(final radial bins) (N_r values) and
+  // returns dL/d(initial grid) ([j][u][r]) and, if asked, dL/d(initial chain
+  // values); the handle holds the final state again afterwards
+  void adjointForward(int nsteps, int checkpointEvery) {
+    check(vls_adjoint_forward(h_, nsteps, checkpointEvery), h_);
+  }
+  void adjointBackward(const std::vector<double> &dbins, std::vector<double> &df0,
+                       std::vector<double> *dchain0 = nullptr) {
+    df0.resize(nr_ * nu_ * nj_);
+    int64_t nc = 0, ne = 0;
+    check(vls_get_chains(h_, &nc, &ne, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr),
+          h_);
+    if (dchain0) dchain0->resize((size_t)ne);
+    check(vls_adjoint_backward(h_, dbins.data(), (int64_t)dbins.size(), df0.data(), df0.size(),
+                               dchain0 ? dchain0->data() : nullptr, dchain0 ? ne : 0),
+          h_);
+  }
+  // second checkpoint level inside a segment (0: chosen from free memory)
+  void adjointSetInner(int innerEvery) { check(vls_adjoint_set_inner(h_, innerEvery), h_); }
+  // device memory the handle holds (also its peak)
+  size_t deviceBytes() {
+    size_t b = 0;
+    check(vls_device_bytes(h_, &b), h_);
+    return b;
+  }
+
   double massBeforeRenormalisation() const { return mass_before_; }
   size_t nr() const { return nr_; }
   size_t nu() const { return nu_; }
