@@ -325,6 +325,7 @@ def gpu_arm(args):
     if "fp64" in line:
         line["fp32_over_fp64"] = value / line["fp64"]["value"]
     if world == 1 and not args.no_accuracy:
+        line["configs"] = configs_block(100)
         line["accuracy"] = accuracy_block(args.accuracy_steps)
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_block(args.adjoint_steps, args.adjoint_every)
@@ -342,6 +343,35 @@ ACCURACY = dict(type="Plummer", Pmin=0.01, Pmax=25.0, Pres=256, Pscale="logarith
 ADJOINT = dict(type="UDF", Pmin=0.01, Pmax=25.0, Pres=256, Pscale="logarithmic",
                Umin=(-2.0, 0.0), Umax=(2.0, 1.6), Ures=(256, 128),
                Uscale=("linear", "quadratic"), dt=0.005)
+
+
+# the listed configurations' grids, timed in both storage precisions
+CONFIGS = {
+    "udf_200x200x200": dict(type="UDF", Pmin=0.01, Pmax=25.0, Pres=200, Pscale="logarithmic",
+                            Umin=(-2.0, 0.0), Umax=(2.0, 1.6), Ures=(200, 200),
+                            Uscale=("linear", "quadratic"), dt=0.005),
+}
+
+
+def configs_block(steps):
+    """Cell updates/s of the FP64 and FP32-bulk step on the UDF 201x201x200
+    and Plummer 257x257x128 grids (device time, CUDA events, after 5 warm-up
+    steps)."""
+    import torch
+    from vlasolve_b200 import VlasovSolver21Spline
+    out = {}
+    for name, w in (("udf_200x200x200", CONFIGS["udf_200x200x200"]),
+                    ("plummer_256x256x128", ACCURACY)):
+        out[name] = {}
+        for prec in ("fp64", "fp32"):
+            s = VlasovSolver21Spline(w, precision=prec)
+            ms, _ = time_steps(s, steps, 5, torch, None)
+            cells = s.nr * s.nu * s.nj
+            out[name][prec] = {"ms_per_step": ms / steps, "value": cells * steps / (ms * 1e-3),
+                               "cells": cells}
+            s.close()
+        out[name]["fp32_over_fp64"] = out[name]["fp32"]["value"] / out[name]["fp64"]["value"]
+    return out
 
 
 def accuracy_block(steps):
