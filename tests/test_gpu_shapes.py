@@ -13,8 +13,14 @@ pytestmark = pytest.mark.gpu
 
 # (grid.Pres, grid.Ures[0]) -> N_r = Pres + 1 r vertices, N_u = Ures0 + 1 u
 # vertices; chunks of 31 rows: 4 -> 1 chunk, 32 -> 2 chunks with a last
-# chunk of one row, 62 -> 2 full chunks, 63 -> 3 chunks, 94 -> 4 chunks
-SHAPES = [(3, 31), (31, 32), (32, 61), (61, 62), (62, 93), (93, 3), (150, 40)]
+# chunk of one row, 62 -> 2 full chunks, 63 -> 3 chunks, 94 -> 4 chunks;
+# chunks of 23 rows: 47 -> 2 full chunks and one row, 69 -> 3 full chunks;
+# 701 u vertices: lines too long for 16-line blocks of 15-row chunks, which
+# take 23-row chunks by default; 1001 r vertices: FP64 rows whose four
+# persistent r-solve tiles exceed a block's shared memory (the plain kernel
+# takes them)
+SHAPES = [(3, 31), (31, 32), (32, 61), (61, 62), (62, 93), (93, 3), (150, 40),
+          (46, 68), (20, 700), (1000, 8)]
 
 FP64_TOL = 1e-12
 FP32_L2 = 2e-6
@@ -36,6 +42,7 @@ IMPLS = {
     "rcA": {"VLS_RC": "A"},
     "rcB": {"VLS_RC": "B"},
     "rcC": {"VLS_RC": "C"},
+    "rcD": {"VLS_RC": "D"},
     "strip48": {"VLS_DRIFT": "48"},
     "strip64": {"VLS_DRIFT": "64"},
     "strip-48": {"VLS_DRIFT": "-48"},

@@ -59,6 +59,7 @@ using CfgA1 = RcCfg<31, 16, 576, 1>;  // the same for up to 35 chunks
 using CfgB = RcCfg<15, 8, 320, 3>;    // 15-row chunks, 8 lines, three blocks per SM
 using CfgB1 = RcCfg<15, 8, 640, 1>;   // the same for up to 77 chunks
 using CfgC = RcCfg<15, 16, 576, 2>;   // 15-row chunks, 16 lines, two blocks per SM
+using CfgD = RcCfg<23, 8, 384, 2>;    // 23-row chunks, 8 lines, two blocks per SM (up to 45 chunks)
 
 template <typename R>
 struct Dev;
@@ -882,14 +883,23 @@ cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
                            (size_t)RC_PIPE_TILES * CF::LN *
                                rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), CF::LN) * sizeof(T);
       auto kp = prer_pipe_kernel<T, R, CF>;
-      cudaError_t e = rc_attr(kp, psmem);
-      if (e != cudaSuccess) return e;
-      int dev = 0, nsm = 0, per = 0;
+      int dev = 0, nsm = 0, per = 0, smax = 0;
+      cudaError_t e;
       if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-      if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+      if ((e = cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
+          cudaSuccess)
         return e;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kp, nt, psmem)) != cudaSuccess)
-        return e;
+      // four tiles of long FP64 rows (1025 columns: 272 KB) do not fit a
+      // block: the plain kernel below then takes the rows
+      if (psmem <= (size_t)smax) {
+        if ((e = rc_attr(kp, psmem)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) !=
+            cudaSuccess)
+          return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kp, nt, psmem)) !=
+            cudaSuccess)
+          return e;
+      }
       // only where it keeps the plain kernel's blocks per SM (four FP64
       // tiles of a 513-column row group hold one block per SM)
       if (per >= CF::MINB) {
@@ -1269,9 +1279,10 @@ using CfgAdjR = RcCfg<15, 8, 320, 2>;
 
 // ------------------------------------------------------------- host side
 // configuration for one direction (u_lines: the ucol kernel's columns, else
-// the prer kernel's rows): `pref` "A", "B" or "C" (31-row chunks of 16
-// lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines) or empty for
-// the default; -1 when no configuration takes the shape
+// the prer kernel's rows): `pref` "A", "B", "C" or "D" (31-row chunks of 16
+// lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines; 23-row chunks
+// of 8 lines) or empty for the default; -1 when no configuration takes the
+// shape
 template <typename R>
 int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
   const int N = t.M - 2;
@@ -1281,13 +1292,18 @@ int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
   if (p == "A") return cfg2_fits<CfgA>(N, kc) ? 0 : cfg2_fits<CfgA1>(N, kc) ? 1 : -1;
   if (p == "B") return b;
   if (p == "C") return cfg2_fits<CfgC>(N, kc) ? 4 : -1;
+  if (p == "D") return cfg2_fits<CfgD>(N, kc) ? 5 : -1;
   // default (fastest measured on 513 x 513 x 256): 16-line blocks for the u
-  // lines, 8-line blocks for the r lines
+  // lines, 8-line blocks for the r lines; lines too long for those take
+  // 23-row chunks with two blocks per SM (1025-row lines: ucol 2.85 -> 1.85
+  // ms, prer 1.17 -> 0.97 ms against 15-row chunks at one block per SM)
   if (u_lines && cfg2_fits<CfgC>(N, kc)) return 4;
+  if (cfg2_fits<CfgB>(N, kc)) return 2;
+  if (cfg2_fits<CfgD>(N, kc)) return 5;
   return b;
 }
 
-static int cfg_L(int cfg) { return cfg <= 1 ? CfgA::L : CfgB::L; }
+static int cfg_L(int cfg) { return cfg <= 1 ? CfgA::L : cfg == 5 ? CfgD::L : CfgB::L; }
 
 template <typename R>
 RcDir<R> rc_dir(const HostDirTables &t, int cfg) {
@@ -1352,6 +1368,7 @@ cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *s
     VLS_UCOL_CFG(2, CfgB)
     VLS_UCOL_CFG(3, CfgB1)
     VLS_UCOL_CFG(4, CfgC)
+    VLS_UCOL_CFG(5, CfgD)
     default:
       return cudaErrorInvalidValue;
   }
@@ -1372,6 +1389,8 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
       return prer_rc_go<T, R, CfgB1>(G, C, g, tr, err, st);
     case 4:
       return prer_rc_go<T, R, CfgC>(G, C, g, tr, err, st);
+    case 5:
+      return prer_rc_go<T, R, CfgD>(G, C, g, tr, err, st);
     default:
       return cudaErrorInvalidValue;
   }
