@@ -175,6 +175,22 @@ def test_far_cell_layout_keeps_the_adjoint(monkeypatch):
     np.testing.assert_allclose(g, g_ref, rtol=1e-6)
 
 
+def test_long_line_adjoint_layout_keeps_the_gradient(monkeypatch):
+    """The 8-line chunk layouts the transposed solves take for lines too long
+    for the default ones (1025 rows), forced here on short lines."""
+    p_ref = problem("fp64")
+    target = p_ref.run(THETA + DTHETA)
+    _, g_ref = loss_and_grad(p_ref, target)
+    monkeypatch.setenv("VLS_ADJ_RC", "long")
+    for prec in ("fp64", "fp32"):
+        p = problem(prec)
+        _, g = loss_and_grad(p, target)
+        if prec == "fp64":
+            np.testing.assert_allclose(g, g_ref, rtol=1e-10)
+        else:
+            assert np.all(np.abs(g - g_ref) <= FP32_RTOL * np.max(np.abs(g_ref)))
+
+
 def test_chunked_adjoint_lines_match_one_thread_per_line(monkeypatch):
     """The chunked-register transposed solves against the one-thread-per-line
     kernels (VLS_PREFILTER=segment selects those for both directions)."""

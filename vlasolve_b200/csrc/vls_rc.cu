@@ -1274,6 +1274,9 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
 
 using CfgAdjU = RcCfg<15, 16, 576, 1>;
 using CfgAdjR = RcCfg<15, 8, 320, 2>;
+// lines too long for those (up to 70 and 78 chunks: 1025-row lines)
+using CfgAdjU2 = RcCfg<15, 8, 576, 1>;
+using CfgAdjR2 = RcCfg<15, 8, 640, 1>;
 
 }  // namespace
 
@@ -1397,43 +1400,69 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
 }
 
 // adjoint line kernels (FP64): u lines with 15-row chunks of 16 lines, r
-// lines with 15-row chunks of 8 lines; tables from rc_dir<double>(t, 2)
+// lines with 15-row chunks of 8 lines; lines too long for those in 8-line
+// blocks of up to 70 / 78 chunks (VLS_ADJ_RC=long takes those for every
+// length, for tests); tables from rc_dir<double>(t, 2)
+static bool adj_long_forced() {
+  static const bool f = [] {
+    const char *e = std::getenv("VLS_ADJ_RC");
+    return e && std::string(e) == "long";
+  }();
+  return f;
+}
 bool rc_adj_supported(const HostDirTables &tu, const HostDirTables &tr) {
   return tu.M - 2 > CfgAdjU::L && tr.M - 2 > CfgAdjR::L &&
-         cfg_fits<CfgAdjU>(tu.M - 2, tu.kc64) && cfg_fits<CfgAdjR>(tr.M - 2, tr.kc64);
+         (cfg_fits<CfgAdjU>(tu.M - 2, tu.kc64) || cfg_fits<CfgAdjU2>(tu.M - 2, tu.kc64)) &&
+         (cfg_fits<CfgAdjR>(tr.M - 2, tr.kc64) || cfg_fits<CfgAdjR2>(tr.M - 2, tr.kc64));
+}
+
+template <typename T, class CF>
+static cudaError_t ucol_adj_go(const T *f, const double *Gb, double *lam, double *sbar,
+                               const double *shift, const Geometry &g, const RcDir<double> &tu,
+                               cudaStream_t st) {
+  const int nt = rc_threads<CF>(tu.S);
+  if (tu.N != g.nu || nt > CF::NT || tu.L != CF::L) return cudaErrorInvalidValue;
+  const int M = tu.N + 2;
+  const size_t smem = 2 * (size_t)tu.S * CF::LN * sizeof(double) +
+                      (size_t)(M + 1 + tu.N) * CF::LN * sizeof(double);
+  auto k = ucol_adj_rc_kernel<T, CF>;
+  cudaError_t e = rc_attr(k, smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((g.nr + CF::LN - 1) / CF::LN, g.nj);
+  k<<<grid, nt, smem, st>>>(f, Gb, lam, sbar, shift, g, tu);
+  return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_ucol_adj_rc(const T *f, const double *Gb, double *lam, double *sbar,
                                const double *shift, const Geometry &g, const RcDir<double> &tu,
                                cudaStream_t st) {
-  const int nt = rc_threads<CfgAdjU>(tu.S);
-  if (tu.N != g.nu || nt > CfgAdjU::NT || tu.L != CfgAdjU::L) return cudaErrorInvalidValue;
-  const int M = tu.N + 2;
-  const size_t smem = 2 * (size_t)tu.S * CfgAdjU::LN * sizeof(double) +
-                      (size_t)(M + 1 + tu.N) * CfgAdjU::LN * sizeof(double);
-  auto k = ucol_adj_rc_kernel<T, CfgAdjU>;
+  if (tu.S <= rc_maxs<CfgAdjU>() && !adj_long_forced())
+    return ucol_adj_go<T, CfgAdjU>(f, Gb, lam, sbar, shift, g, tu, st);
+  return ucol_adj_go<T, CfgAdjU2>(f, Gb, lam, sbar, shift, g, tu, st);
+}
+
+template <class CF>
+static cudaError_t prer_adj_go(const double *Cb, double *Gb, const Geometry &g,
+                               const RcDir<double> &tr, cudaStream_t st) {
+  const int nt = rc_threads<CF>(tr.S);
+  if (tr.N != g.nr || nt > CF::NT || tr.L != CF::L) return cudaErrorInvalidValue;
+  const int M = tr.N + 2;
+  const size_t smem = al16(2 * (size_t)tr.S * CF::LN * sizeof(double)) +
+                      (size_t)CF::LN * rc_tile_pitch(M, sizeof(double), CF::LN) * sizeof(double);
+  auto k = prer_adj_rc_kernel<CF>;
   cudaError_t e = rc_attr(k, smem);
   if (e != cudaSuccess) return e;
-  const dim3 grid((g.nr + CfgAdjU::LN - 1) / CfgAdjU::LN, g.nj);
-  k<<<grid, nt, smem, st>>>(f, Gb, lam, sbar, shift, g, tu);
+  const dim3 grid((g.nu + 2 + CF::LN - 1) / CF::LN, g.nj);
+  k<<<grid, nt, smem, st>>>(Cb, Gb, g, tr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_prer_adj_rc(const double *Cb, double *Gb, const Geometry &g,
                                const RcDir<double> &tr, cudaStream_t st) {
-  const int nt = rc_threads<CfgAdjR>(tr.S);
-  if (tr.N != g.nr || nt > CfgAdjR::NT || tr.L != CfgAdjR::L) return cudaErrorInvalidValue;
-  const int M = tr.N + 2;
-  const size_t smem = al16(2 * (size_t)tr.S * CfgAdjR::LN * sizeof(double)) +
-                      (size_t)CfgAdjR::LN * rc_tile_pitch(M, sizeof(double), CfgAdjR::LN) *
-                          sizeof(double);
-  auto k = prer_adj_rc_kernel<CfgAdjR>;
-  cudaError_t e = rc_attr(k, smem);
-  if (e != cudaSuccess) return e;
-  const dim3 grid((g.nu + 2 + CfgAdjR::LN - 1) / CfgAdjR::LN, g.nj);
-  k<<<grid, nt, smem, st>>>(Cb, Gb, g, tr);
-  return cudaGetLastError();
+  if (tr.S <= rc_maxs<CfgAdjR>() && !adj_long_forced())
+    return prer_adj_go<CfgAdjR>(Cb, Gb, g, tr, st);
+  return prer_adj_go<CfgAdjR2>(Cb, Gb, g, tr, st);
 }
 
 template cudaError_t launch_ucol_adj_rc<float>(const float *, const double *, double *, double *,
