@@ -522,6 +522,11 @@ def large_block(nsteps, K):
     out["forward_ms_per_step"] = ms / nsteps
     out["value"] = out["cells"] * nsteps / (ms * 1e-3)
     out["unit"] = "cell updates/s"
+    s.set_profiling(True)
+    s.step(5)
+    prof = s.profile_read()
+    s.set_profiling(False)
+    out["kernels_ms_per_step"] = {k: v[0] / 5 for k, v in prof.items()}
     # adjoint
     target = p.run(theta + dtheta)
     th = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
