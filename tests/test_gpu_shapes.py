@@ -47,6 +47,8 @@ IMPLS = {
     "strip64": {"VLS_DRIFT": "64"},
     "strip-48": {"VLS_DRIFT": "-48"},
     "strip-49": {"VLS_DRIFT": "-49"},
+    "strip50": {"VLS_DRIFT": "50"},
+    "strip51": {"VLS_DRIFT": "51"},
     "far": {"VLS_FAR": "1"},
 }
 

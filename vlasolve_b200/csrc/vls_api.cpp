@@ -761,10 +761,16 @@ extern "C" int vls_create(const vls_grid_desc *grid,
     return fin(fail(hp, VLS_ECUDA, "cudaMemsetAsync failed"));
   {
     // drift layout: whole-strip staging where it fits (VLS_DRIFT=window, 48,
-    // 64 or -48 selects one for measurements)
+    // 64, -48, -49, 50 or 51 selects one for measurements)
     const char *dv = std::getenv("VLS_DRIFT");
     const std::string d = dv ? dv : "";
-    const int want = d == "48" ? 48 : d == "64" ? 64 : d == "-48" ? -48 : d == "-49" ? -49 : 0;
+    const int want = d == "48"    ? 48
+                     : d == "64"  ? 64
+                     : d == "-48" ? -48
+                     : d == "-49" ? -49
+                     : d == "50"  ? 50
+                     : d == "51"  ? 51
+                                  : 0;
     h->strip_w = d == "window" ? 0
                  : h->esize == 4 ? drift_strip_width<float>(c.nu, want)
                                  : drift_strip_width<double>(c.nu, want);

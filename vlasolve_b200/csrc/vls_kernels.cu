@@ -1365,12 +1365,14 @@ __global__ void __launch_bounds__(32 * NW, MINB)
 
 // strip layouts: 48 (48 columns, 8 warps, two blocks per SM), 64 (64
 // columns, 16 warps, one block per SM), -48 (48 columns, 16 warps, two blocks
-// per SM), -49 (as -48, every box awaited before the first cell); 0: none,
-// the windowed kernel is used.  `want` != 0 asks for one layout, returned
-// only if it fits.  The default is -49 for FP32 storage where two blocks fit
-// (4 % faster than -48 on the 513 x 513 x 256 case: the other block on the SM
-// computes while this one's strip lands), else the windowed kernel (FP64
-// strips fit one block per SM only, which measured slower).
+// per SM), -49 (as -48, every box awaited before the first cell), 50 (48
+// columns, 32 warps, one block per SM), 51 (as 50, every box awaited first);
+// 0: none, the windowed kernel is used.  `want` != 0 asks for one layout,
+// returned only if it fits.  The default for FP32 storage is -49 where two
+// blocks fit (4 % faster than -48 on the 513 x 513 x 256 case: the other
+// block on the SM computes while this one's strip lands), else 51 where one
+// fits, else the windowed kernel; FP64 takes the windowed kernel (its strips
+// fit one block per SM only, which measured slower).
 template <typename T>
 int drift_strip_width(int nu, int want) {
   const int nch = (nu + 3 + DS_ROWS - 1) / DS_ROWS;
@@ -1381,11 +1383,19 @@ int drift_strip_width(int nu, int want) {
   const bool fit48x8 = 2 * (dyn(48) + 8 * 32 * 8 + 1024) <= 233472;
   const bool fit48x16 = 2 * (dyn(48) + 16 * 32 * 8 + 1024) <= 233472;
   const bool fit64 = dyn(64) + 16 * 32 * 8 <= 232448;
+  // one block of 32 warps per SM (strips of up to 1028 rows in FP32)
+  const bool fit48x32 = dyn(48) + 32 * 32 * 8 <= 232448;
   if (want == 48) return fit48x8 ? 48 : 0;
   if (want == 64) return fit64 ? 64 : 0;
   if (want == -48) return fit48x16 ? -48 : 0;
   if (want == -49) return fit48x16 ? -49 : 0;
-  return (sizeof(T) == 4 && fit48x16) ? -49 : 0;
+  if (want == 50) return fit48x32 ? 50 : 0;
+  if (want == 51) return fit48x32 ? 51 : 0;
+  if (sizeof(T) != 4) return 0;
+  // strips too tall for two blocks per SM (1025 rows) take one block of 32
+  // warps, every box awaited first: 14 % faster than the windowed drift on
+  // the 1025 x 1025 x 512 case (the per-cell waits of 50 gained nothing)
+  return fit48x16 ? -49 : fit48x32 ? 51 : 0;
 }
 
 template <typename T, int WC, int NW, int MINB, bool WAITALL = false>
@@ -1432,6 +1442,12 @@ cudaError_t launch_drift_strip(const CUtensorMap *tmS, int width, const T *C, T 
     case -48:
       return drift_strip_go<T, 48, 16, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
                                           ndrift, mt, partial, farsum, err, g, st);
+    case 50:  // 48 columns, 32 warps, one block per SM, per-cell box waits
+      return drift_strip_go<T, 48, 32, 1>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
+                                          ndrift, mt, partial, farsum, err, g, st);
+    case 51:  // 50 with every box awaited before the first cell
+      return drift_strip_go<T, 48, 32, 1, true>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len,
+                                                ch_val, ndrift, mt, partial, farsum, err, g, st);
     default:
       return cudaErrorInvalidValue;
   }
