@@ -15,6 +15,7 @@ pytestmark = pytest.mark.gpu
 # vertices; chunks of 31 rows: 4 -> 1 chunk, 32 -> 2 chunks with a last
 # chunk of one row, 62 -> 2 full chunks, 63 -> 3 chunks, 94 -> 4 chunks;
 # chunks of 23 rows: 47 -> 2 full chunks and one row, 69 -> 3 full chunks;
+# chunks of 19 rows: 47 -> 2 full chunks and 9 rows;
 # 701 u vertices: lines too long for 16-line blocks of 15-row chunks, which
 # take 23-row chunks by default; 1001 r vertices: FP64 rows whose four
 # persistent r-solve tiles exceed a block's shared memory (the plain kernel
@@ -43,6 +44,7 @@ IMPLS = {
     "rcB": {"VLS_RC": "B"},
     "rcC": {"VLS_RC": "C"},
     "rcD": {"VLS_RC": "D"},
+    "rcF": {"VLS_RC": "F"},
     "strip48": {"VLS_DRIFT": "48"},
     "strip64": {"VLS_DRIFT": "64"},
     "strip-48": {"VLS_DRIFT": "-48"},

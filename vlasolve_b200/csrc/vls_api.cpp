@@ -653,14 +653,20 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   h->tu = thomas_tables(c.nu, c.sstep_inv[1]);
   {
     // prefilter kernels: register chunks (VLS_PREFILTER=segment selects the
-    // shared-memory segment kernels; VLS_RC=A|B|C a chunk layout)
+    // shared-memory segment kernels; VLS_RC=A|B|C|D|F a chunk layout for
+    // both directions, VLS_RC_U / VLS_RC_R for one)
     const char *pf = std::getenv("VLS_PREFILTER");
     const bool seg = pf && std::string(pf) == "segment";
     const char *lay = std::getenv("VLS_RC");
+    const char *lay_u = std::getenv("VLS_RC_U"), *lay_r = std::getenv("VLS_RC_R");
+    if (!lay_u) lay_u = lay;
+    if (!lay_r) lay_r = lay;
     const bool r64 = h->prec == VLS_FP64 || h->prec == VLS_FP32_BULK;
     if (!seg) {
-      h->rcu_cfg = r64 ? rc_config<double>(h->tu, lay, true) : rc_config<float>(h->tu, lay, true);
-      h->rcr_cfg = r64 ? rc_config<double>(h->tr, lay, false) : rc_config<float>(h->tr, lay, false);
+      h->rcu_cfg =
+          r64 ? rc_config<double>(h->tu, lay_u, true) : rc_config<float>(h->tu, lay_u, true);
+      h->rcr_cfg =
+          r64 ? rc_config<double>(h->tr, lay_r, false) : rc_config<float>(h->tr, lay_r, false);
     }
     h->rcu_d = rc_dir<double>(h->tu, h->rcu_cfg);
     h->rcr_d = rc_dir<double>(h->tr, h->rcr_cfg);

@@ -60,6 +60,8 @@ using CfgB = RcCfg<15, 8, 320, 3>;    // 15-row chunks, 8 lines, three blocks pe
 using CfgB1 = RcCfg<15, 8, 640, 1>;   // the same for up to 77 chunks
 using CfgC = RcCfg<15, 16, 576, 2>;   // 15-row chunks, 16 lines, two blocks per SM
 using CfgD = RcCfg<23, 8, 384, 2>;    // 23-row chunks, 8 lines, two blocks per SM (up to 45 chunks)
+using CfgF = RcCfg<19, 8, 256, 3>;    // 19-row chunks, 8 lines, three blocks per SM (up to 29 chunks)
+using CfgI = RcCfg<17, 16, 512, 2>;   // 17-row chunks, 16 lines, two blocks per SM (up to 31 chunks)
 
 template <typename R>
 struct Dev;
@@ -1282,10 +1284,10 @@ using CfgAdjR2 = RcCfg<15, 8, 640, 1>;
 
 // ------------------------------------------------------------- host side
 // configuration for one direction (u_lines: the ucol kernel's columns, else
-// the prer kernel's rows): `pref` "A", "B", "C" or "D" (31-row chunks of 16
-// lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines; 23-row chunks
-// of 8 lines) or empty for the default; -1 when no configuration takes the
-// shape
+// the prer kernel's rows): `pref` "A", "B", "C", "D" or "F" (31-row chunks
+// of 16 lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines; 23-row
+// chunks of 8 lines; 19-row chunks of 8 lines) or empty for the default; -1
+// when no configuration takes the shape
 template <typename R>
 int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
   const int N = t.M - 2;
@@ -1296,17 +1298,37 @@ int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
   if (p == "B") return b;
   if (p == "C") return cfg2_fits<CfgC>(N, kc) ? 4 : -1;
   if (p == "D") return cfg2_fits<CfgD>(N, kc) ? 5 : -1;
-  // default (fastest measured on 513 x 513 x 256): 16-line blocks for the u
-  // lines, 8-line blocks for the r lines; lines too long for those take
-  // 23-row chunks with two blocks per SM (1025-row lines: ucol 2.85 -> 1.85
-  // ms, prer 1.17 -> 0.97 ms against 15-row chunks at one block per SM)
+  if (p == "F") return cfg2_fits<CfgF>(N, kc) ? 6 : -1;
+  if (p == "I") return cfg2_fits<CfgI>(N, kc) ? 7 : -1;
+  // default (fastest measured on 513 x 513 x 256): 16-line blocks of 15-row
+  // chunks for the u lines (19- and 23-row chunks measured 3 % and 28 %
+  // slower), 8-line blocks of 19-row chunks for the r lines (prer 0.142 ->
+  // 0.120 ms against 15-row chunks; 17 and 21 rows 0.130 and 0.128 ms);
+  // lines too long for those take 23-row chunks with two blocks per SM
+  // (1025-row lines: ucol 2.85 -> 1.85 ms, prer 1.17 -> 0.97 ms against
+  // 15-row chunks at one block per SM)
   if (u_lines && cfg2_fits<CfgC>(N, kc)) return 4;
+  if (!u_lines && cfg2_fits<CfgF>(N, kc)) return 6;
   if (cfg2_fits<CfgB>(N, kc)) return 2;
   if (cfg2_fits<CfgD>(N, kc)) return 5;
   return b;
 }
 
-static int cfg_L(int cfg) { return cfg <= 1 ? CfgA::L : cfg == 5 ? CfgD::L : CfgB::L; }
+static int cfg_L(int cfg) {
+  switch (cfg) {
+    case 0:
+    case 1:
+      return CfgA::L;
+    case 5:
+      return CfgD::L;
+    case 6:
+      return CfgF::L;
+    case 7:
+      return CfgI::L;
+    default:
+      return CfgB::L;
+  }
+}
 
 template <typename R>
 RcDir<R> rc_dir(const HostDirTables &t, int cfg) {
@@ -1372,6 +1394,8 @@ cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *s
     VLS_UCOL_CFG(3, CfgB1)
     VLS_UCOL_CFG(4, CfgC)
     VLS_UCOL_CFG(5, CfgD)
+    VLS_UCOL_CFG(6, CfgF)
+    VLS_UCOL_CFG(7, CfgI)
     default:
       return cudaErrorInvalidValue;
   }
@@ -1394,6 +1418,10 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
       return prer_rc_go<T, R, CfgC>(G, C, g, tr, err, st);
     case 5:
       return prer_rc_go<T, R, CfgD>(G, C, g, tr, err, st);
+    case 6:
+      return prer_rc_go<T, R, CfgF>(G, C, g, tr, err, st);
+    case 7:
+      return prer_rc_go<T, R, CfgI>(G, C, g, tr, err, st);
     default:
       return cudaErrorInvalidValue;
   }
