@@ -45,6 +45,7 @@ IMPLS = {
     "rcC": {"VLS_RC": "C"},
     "rcD": {"VLS_RC": "D"},
     "rcF": {"VLS_RC": "F"},
+    "rcI": {"VLS_RC": "I"},
     "strip48": {"VLS_DRIFT": "48"},
     "strip64": {"VLS_DRIFT": "64"},
     "strip-48": {"VLS_DRIFT": "-48"},

@@ -653,7 +653,7 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   h->tu = thomas_tables(c.nu, c.sstep_inv[1]);
   {
     // prefilter kernels: register chunks (VLS_PREFILTER=segment selects the
-    // shared-memory segment kernels; VLS_RC=A|B|C|D|F a chunk layout for
+    // shared-memory segment kernels; VLS_RC=A|B|C|D|F|I a chunk layout for
     // both directions, VLS_RC_U / VLS_RC_R for one)
     const char *pf = std::getenv("VLS_PREFILTER");
     const bool seg = pf && std::string(pf) == "segment";

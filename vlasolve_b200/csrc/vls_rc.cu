@@ -1284,10 +1284,10 @@ using CfgAdjR2 = RcCfg<15, 8, 640, 1>;
 
 // ------------------------------------------------------------- host side
 // configuration for one direction (u_lines: the ucol kernel's columns, else
-// the prer kernel's rows): `pref` "A", "B", "C", "D" or "F" (31-row chunks
-// of 16 lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines; 23-row
-// chunks of 8 lines; 19-row chunks of 8 lines) or empty for the default; -1
-// when no configuration takes the shape
+// the prer kernel's rows): `pref` "A", "B", "C", "D", "F" or "I" (31-row
+// chunks of 16 lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines;
+// 23-row chunks of 8 lines; 19-row chunks of 8 lines; 17-row chunks of 16
+// lines) or empty for the default; -1 when no configuration takes the shape
 template <typename R>
 int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
   const int N = t.M - 2;
@@ -1300,13 +1300,14 @@ int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
   if (p == "D") return cfg2_fits<CfgD>(N, kc) ? 5 : -1;
   if (p == "F") return cfg2_fits<CfgF>(N, kc) ? 6 : -1;
   if (p == "I") return cfg2_fits<CfgI>(N, kc) ? 7 : -1;
-  // default (fastest measured on 513 x 513 x 256): 16-line blocks of 15-row
-  // chunks for the u lines (19- and 23-row chunks measured 3 % and 28 %
+  // default (fastest measured on 513 x 513 x 256): 16-line blocks of 17-row
+  // chunks for the u lines (15, 19 and 23 rows measured 1 %, 3 % and 28 %
   // slower), 8-line blocks of 19-row chunks for the r lines (prer 0.142 ->
   // 0.120 ms against 15-row chunks; 17 and 21 rows 0.130 and 0.128 ms);
   // lines too long for those take 23-row chunks with two blocks per SM
   // (1025-row lines: ucol 2.85 -> 1.85 ms, prer 1.17 -> 0.97 ms against
   // 15-row chunks at one block per SM)
+  if (u_lines && cfg2_fits<CfgI>(N, kc)) return 7;
   if (u_lines && cfg2_fits<CfgC>(N, kc)) return 4;
   if (!u_lines && cfg2_fits<CfgF>(N, kc)) return 6;
   if (cfg2_fits<CfgB>(N, kc)) return 2;
