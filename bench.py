@@ -154,6 +154,23 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest of the ranks' values of x (every rank takes the same
+    collective); x itself without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, cells, steps, seconds):
+    """Whole-job cell updates/s of `world` replicas that each advanced `cells`
+    cells `steps` times, the slowest in `seconds`."""
+    return world * cells * steps / seconds
+
+
 def time_steps(solver, steps, warmup, torch, dist):
     """Device time of `steps` steps on the solver's stream (CUDA events)."""
     stream = torch.cuda.ExternalStream(solver.stream_ptr())
@@ -172,9 +189,7 @@ def time_steps(solver, steps, warmup, torch, dist):
     ms = e0.elapsed_time(e1)
     launches = solver.kernel_launches() - l0
     if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist)
         dist.barrier()
     return ms, launches
 
@@ -239,7 +254,7 @@ def gpu_arm(args):
 
     main = res[args.precision]
     ms = main["ms"]
-    value = world * cells * K / (ms * 1e-3)
+    value = replica_value(world, cells, K, ms * 1e-3)
     esize = 8 if args.precision == "fp64" else 4
     # dominant kernel and its roofline: algorithmic bytes = one read of its input
     # field + one write of its output field per cell (8 B FP32 / 16 B FP64)
@@ -272,11 +287,8 @@ def gpu_arm(args):
     s.get_f_into(hnp)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * cells * K / e2e_s
+    e2e_s = max_over_ranks(e2e_s, dist)
+    e2e = replica_value(world, cells, K, e2e_s)
     s.close()
 
     if rank != 0:
