@@ -562,6 +562,14 @@ def large_block(nsteps, K):
     s.sync()
     out["step_adjoint_s"] = time.perf_counter() - ta
     out["step_adjoint_ms_per_step"] = 1e3 * out["step_adjoint_s"] / nsteps
+    # per-kernel device times of a 4-step backward pass (3 recomputed forward
+    # steps and 4 transposed steps)
+    s.adjoint_forward(4, 4)
+    s.set_profiling(True)
+    s.adjoint_backward(dbins)
+    prof = s.profile_read()
+    s.set_profiling(False)
+    out["adjoint_pass_4_steps_kernel_ms"] = {k: v[0] for k, v in prof.items() if v[1]}
     out["grad"] = th.grad.numpy().tolist()
     out["loss_value"] = float(L.detach())
     out["forward_checkpointed_s"] = t2 - t1

@@ -173,7 +173,13 @@ int vls_stream(const vls_handle *h, void **stream);
    (VLS_K_* below, nk entries) and clears the record.  Diagnostic only. */
 enum { VLS_K_UCOL_KICK = 0, VLS_K_UCOL = 1, VLS_K_PRER = 2, VLS_K_TAILS = 3,
        VLS_K_DRIFT = 4, VLS_K_SCAN = 5, VLS_K_MOMENT = 6, VLS_K_STATS = 7,
-       VLS_K_CONVERT = 8, VLS_K_COUNT = 9 };
+       VLS_K_CONVERT = 8,
+       /* adjoint step: drift transpose, chain fronts and tails, r-solve and
+          u-solves + kick transposed, the step's shift (moment + scan), the
+          moment and shift transposed */
+       VLS_K_ADJ_DRIFT = 9, VLS_K_ADJ_TAILS = 10, VLS_K_ADJ_PRER = 11,
+       VLS_K_ADJ_UCOL = 12, VLS_K_ADJ_SHIFT = 13, VLS_K_ADJ_MOMENT = 14,
+       VLS_K_COUNT = 15 };
 int vls_set_profiling(vls_handle *h, int32_t on);
 int vls_profile_read(vls_handle *h, double *ms, int64_t *count, int32_t nk);
 

@@ -201,3 +201,40 @@ def test_chunked_adjoint_lines_match_one_thread_per_line(monkeypatch):
     p = problem("fp64")
     _, g = loss_and_grad(p, target)
     np.testing.assert_allclose(g, g_ref, rtol=1e-10)
+
+
+def _solver_backward(precision, env, monkeypatch, far=False):
+    from vlasolve_b200 import VlasovSolver21Spline
+    if far:
+        monkeypatch.setenv("VLS_FAR", "1")
+    s = VlasovSolver21Spline(cfg(pres=40, ures=(28, 10)), precision=precision)
+    s.adjoint_forward(7, 3)
+    dbins = np.cos(0.3 * np.arange(s.nr, dtype=np.float64))
+    out = []
+    for mode in env:
+        if mode:
+            monkeypatch.setenv("VLS_DRIFT_ADJ", mode)
+        else:
+            monkeypatch.delenv("VLS_DRIFT_ADJ", raising=False)
+        df0, dch = s.adjoint_backward(dbins)
+        out.append((df0.copy(), dch.copy()))
+    return out
+
+
+@pytest.mark.parametrize("precision,far", [("fp64", False), ("fp32", False), ("fp32", True)])
+def test_gather_drift_transpose_matches_atomic_scatter(precision, far, monkeypatch):
+    """The drift transposed as a gather over the inverse footpoint map against
+    the scatter with FP64 atomics: the same sums in another order, on every
+    cell of dL/df0 and every ring slot of dL/d(chains)."""
+    (g0, gc), (a0, ac) = _solver_backward(precision, ["", "atomic"], monkeypatch, far)
+    assert np.max(np.abs(a0)) > 0
+    np.testing.assert_allclose(g0, a0, rtol=1e-11, atol=1e-13 * np.max(np.abs(a0)))
+    assert gc.size == ac.size and gc.size > 0
+    np.testing.assert_allclose(gc, ac, rtol=1e-11, atol=1e-13 * max(np.max(np.abs(ac)), 1e-300))
+
+
+def test_gather_drift_transpose_is_deterministic(monkeypatch):
+    """Two backward passes through the gather give the same bits."""
+    (a0, ac), (b0, bc) = _solver_backward("fp32", ["", ""], monkeypatch)
+    np.testing.assert_array_equal(a0, b0)
+    np.testing.assert_array_equal(ac, bc)

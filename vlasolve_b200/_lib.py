@@ -34,7 +34,8 @@ EXPORTED = [
     "vls_restart_info", "vls_read_restart",
 ]
 KERNEL_KINDS = ["ucol_kick", "ucol", "prer", "tails", "drift", "scan", "moment",
-                "stats", "convert"]
+                "stats", "convert", "adj_drift", "adj_tails", "adj_prer", "adj_ucol",
+                "adj_shift", "adj_moment"]
 
 
 class VlsError(RuntimeError):

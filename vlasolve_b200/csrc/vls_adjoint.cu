@@ -3,8 +3,9 @@
 //
 // The reference has no derivative code; this is the transpose of the step as
 // the forward kernels compute it (vls_kernels.cu, vls_rc.cu):
-//   drift D       f(cell) = sum_ab wy_a wx_b C[uI+a][rI+b] / 36   -> scatter-add
-//   tails E       ring[tail] = same gather at the chain's end    -> scatter-add
+//   drift D       f(cell) = sum_ab wy_a wx_b C[uI+a][rI+b] / 36   -> gather over
+//                 the inverse footpoint map (or scatter-add)
+//   tails E       ring[tail] = same gather at the chain's end    -> the same
 //   prefilter P   natural-BC Thomas solve of each line           -> transposed
 //                 recurrences (localSpline.hxx:953-1182 read backwards)
 //   kick          per column: gather at y = u + s_r hu           -> transposed
@@ -12,8 +13,10 @@
 //   shift s       s_r = Rcoef_r sum_{r' < r} bins_r'             -> reverse scan
 //   moment        bins_r = dR_r/4 (T_r + T_{r+1}), T_r = sum_j w_j sum_u b_u f
 // Adjoint values are FP64 in every precision mode; the forward state they
-// linearise around is read in the handle's storage type.  Scatter-adds use
-// FP64 atomics (their summation order is not deterministic).
+// linearise around is read in the handle's storage type.  The default drift
+// transpose is a gather with a fixed summation order (deterministic); the
+// scatter-add form (FP64 atomics, order not deterministic) remains for
+// comparison and for grids with N_u >= 2^15.
 #include <cuda_runtime.h>
 
 #include "vls_internal.h"
@@ -274,23 +277,42 @@ __global__ void ucol_adj_kernel(const T *__restrict__ f, double *__restrict__ Gb
 }
 
 // shift, transposed: sbar (per slice) -> beta_r' = sum_{r > r'} Rcoef_r sum_j sbar[j][r]
-// (one block: the slice sums in parallel, the N_r-long reverse scan in one
-// thread)
-__global__ void shift_adj_kernel(const double *__restrict__ sbar, double *__restrict__ beta,
-                                 MomentTables mt, Geometry g) {
+// (beta[0..N_r)), and the moment's transpose per radius to beta[N_r..2 N_r)
+// (one block of 1024 threads: 32 slice groups x 32 radii sum in parallel,
+// in a fixed order; the N_r-long reverse scan in one thread)
+__global__ void __launch_bounds__(1024) shift_adj_kernel(const double *__restrict__ sbar,
+                                                         double *__restrict__ beta,
+                                                         MomentTables mt, Geometry g) {
   extern __shared__ double ssum[];
-  for (int r = threadIdx.x; r < g.nr; r += blockDim.x) {
+  __shared__ double part[32][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int r0 = 0; r0 < g.nr; r0 += 32) {
+    const int r = r0 + lane;
     double s = 0.0;
-    for (int j = 0; j < g.nj; ++j) s += sbar[(size_t)j * g.nr + r];
-    ssum[r] = s * mt.Rcoef[r];
+    if (r < g.nr)
+      for (int j = w; j < g.nj; j += 32) s += sbar[(size_t)j * g.nr + r];
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && r < g.nr) {
+      double t = 0.0;
+      for (int k = 0; k < 32; ++k) t += part[k][lane];
+      ssum[r] = t * mt.Rcoef[r];
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (threadIdx.x == 0) {
     double acc = 0.0;
     for (int r = g.nr - 1; r >= 0; --r) {
       beta[r] = acc;  // exclusive: bins_r' enters s_r for r > r'
       acc += ssum[r];
     }
+  }
+  // the moment's transpose per radius: mB_r = beta_r dR4_r + beta_{r-1} dR4_{r-1}
+  __syncthreads();
+  for (int r = threadIdx.x; r < g.nr; r += blockDim.x) {
+    double b = beta[r] * mt.dR4[r];
+    if (r > 0) b += beta[r - 1] * mt.dR4[r - 1];
+    beta[g.nr + r] = b;
   }
 }
 
@@ -315,7 +337,355 @@ unsigned grid_for(size_t n, int threads) {
   return (unsigned)(b ? b : 1);
 }
 
+// ---------------------------------------------------------------------------
+// The drift transposed as a gather over the inverse footpoint map.  The
+// footpoints are fixed for the run, so the cells (and chain tails) whose 4 x 4
+// stencil starts at base node (uI, rI) of slice j are listed once: bucket key
+// uI * N_r + rI, per slice, entries ascending by id within a bucket (u << 16
+// | r of the cell, N_u < 2^15, or INV_TAIL | chain id).  Every C node then
+// sums the contributions of the 16 buckets that reach it, in a fixed order:
+// the result does not depend on scheduling, and no FP64 atomics are issued.
+//
+// The moment's transpose (lam += w_j b_u B_r, B_r = beta_r dR_r/4 +
+// beta_{r-1} dR_{r-1}/4) is not applied to lam as a pass of its own: the
+// readers of lam in the next transposed step (this gather and the chain
+// fronts) add it to the values they read (mB = B, or null for none).
+
+constexpr uint32_t INV_TAIL = 0x80000000u;
+
+// base node of cell i's stencil; false for cells outside the box and chain
+// fronts (the forward drift's decode, vls_kernels.cu)
+template <typename T>
+__device__ __forceinline__ bool cell_base(size_t i, const int32_t *__restrict__ idx,
+                                          const uint2 *__restrict__ fp2,
+                                          const uint2 *__restrict__ far_w, int &rI, int &uI,
+                                          uint2 &w) {
+  if (sizeof(T) == 8) {
+    const int code = idx[i];
+    if (code < 0) return false;
+    rI = code & 0xffff;
+    uI = code >> 16;
+    return true;
+  }
+  w = fp2[i];
+  if (w.x == AFP_FAR) w = far_w[w.y];
+  if (w.x >= AFP_FAR) return false;
+  rI = (int)(w.x >> AFP_FBITS);
+  uI = (int)(w.y >> AFP_FBITS);
+  return true;
+}
+
+// one pass over the cells and chain tails: count (ent == nullptr) or place
+// each into its bucket (ends then hold the bucket starts and end as the
+// bucket ends)
+template <typename T>
+__global__ void inv_fill_kernel(const int32_t *__restrict__ idx, const uint2 *__restrict__ fp2,
+                                const uint2 *__restrict__ far_w, const int32_t *__restrict__ t_idx,
+                                int64_t nch, uint32_t *__restrict__ ends,
+                                uint32_t *__restrict__ ent, const int64_t *__restrict__ ebase,
+                                Geometry g) {
+  const size_t S = (size_t)g.nr * g.nu, n = S * g.nj;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n + (size_t)nch;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int rI, uI, j;
+    uint32_t id;
+    if (i < n) {
+      uint2 w;
+      if (!cell_base<T>(i, idx, fp2, far_w, rI, uI, w)) continue;
+      j = (int)(i / S);
+      const uint32_t within = (uint32_t)(i - (size_t)j * S);
+      id = (within / (uint32_t)g.nr) << 16 | (within % (uint32_t)g.nr);
+    } else {
+      const int64_t c = (int64_t)(i - n);
+      const int code = t_idx[c];
+      if (code < 0) continue;
+      rI = code & 0xffff;
+      uI = code >> 16;
+      j = t_idx[nch + c];
+      id = INV_TAIL | (uint32_t)c;
+    }
+    uint32_t *b = ends + (size_t)j * S + (size_t)uI * g.nr + rI;
+    if (!ent) {
+      atomicAdd(b, 1u);
+    } else {
+      const uint32_t pos = atomicAdd(b, 1u);
+      ent[ebase[j] + pos] = id;
+    }
+  }
+}
+
+// exclusive scan of each slice's bucket counts in place (one block of 1024
+// threads per slice); the slice's entry count to totals[j]
+__global__ void __launch_bounds__(1024) inv_scan_kernel(uint32_t *__restrict__ ends,
+                                                        uint32_t *__restrict__ totals,
+                                                        int64_t S) {
+  __shared__ uint32_t wsum[32];
+  uint32_t *e = ends + (size_t)blockIdx.x * S;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t carry = 0;
+  for (int64_t t0 = 0; t0 < S; t0 += 1024) {
+    const int64_t i = t0 + threadIdx.x;
+    const uint32_t v = i < S ? e[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      uint32_t s = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+      }
+      wsum[lane] = s;
+    }
+    __syncthreads();
+    if (i < S) e[i] = carry + (w ? wsum[w - 1] : 0u) + x - v;
+    carry += wsum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+// order each bucket's entries by id (the placement's atomics leave them in
+// any order)
+__global__ void inv_sort_kernel(const uint32_t *__restrict__ ends, uint32_t *__restrict__ ent,
+                                const int64_t *__restrict__ ebase, int64_t S, int64_t nkeys) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nkeys;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = k / S;
+    const uint32_t s = k - j * S ? ends[k - 1] : 0u, e = ends[k];
+    uint32_t *p = ent + ebase[j];
+    for (uint32_t a = s + 1; a < e; ++a) {
+      const uint32_t v = p[a];
+      uint32_t b = a;
+      while (b > s && p[b - 1] > v) {
+        p[b] = p[b - 1];
+        --b;
+      }
+      p[b] = v;
+    }
+  }
+}
+
+// chain fronts and tails, transposed, one thread per chain: the front slot
+// takes the adjoint of the cell that read it; the tail slot's adjoint (the
+// value this step's tails wrote) moves to tv for the gather and is cleared.
+// In the forward the tails write before the drift reads, so with L = 1 the
+// front add comes first here.
+__global__ void chain_adj_kernel(const double *__restrict__ lam, const double *__restrict__ mB,
+                                 MomentTables mt, double *__restrict__ ringb,
+                                 double *__restrict__ tv, const int64_t *__restrict__ ch_cell,
+                                 const int64_t *__restrict__ ch_start,
+                                 const int32_t *__restrict__ ch_len, int64_t nch,
+                                 int64_t ndrift, Geometry g) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  const int L = ch_len[c];
+  double *ring = ringb + ch_start[c];
+  const int64_t i = ch_cell[c];
+  double v = lam[i];
+  if (mB) {
+    const int r = (int)(i % g.nr);
+    const int64_t ju = i / g.nr;
+    v += mt.wj[ju / g.nu] * mt.bu[ju % g.nu] * mB[r];
+  }
+  ring[ndrift % L] += v;
+  double *slot = ring + (ndrift + L - 1) % L;
+  tv[c] = *slot;
+  *slot = 0.0;
+}
+
+// weight m of the cubic B-spline at fraction t (times 6): m = 0..3 are
+// BV2(1-t), BV1(1-t), BV1(t), BV2(t), as scatter16 computes them
+__device__ __forceinline__ double bweight(int m, double t) {
+  const double s = m < 2 ? 1.0 - t : t;
+  return (m == 0 || m == 3) ? bv2d(s) : bv1d(s);
+}
+
+// one entry of the inverse map: its value (cells: lam plus the pending
+// moment term), base column and fractions
+template <typename T>
+__device__ __forceinline__ void inv_entry(uint32_t id, const double *__restrict__ lam,
+                                          const double *__restrict__ mB, const MomentTables &mt,
+                                          double wjj, const double *__restrict__ tv,
+                                          size_t cbase, const T *__restrict__ fx,
+                                          const T *__restrict__ fy,
+                                          const int32_t *__restrict__ idx,
+                                          const uint2 *__restrict__ fp2,
+                                          const uint2 *__restrict__ far_w,
+                                          const int32_t *__restrict__ t_idx,
+                                          const double *__restrict__ t_x,
+                                          const double *__restrict__ t_y, int nr, double &v,
+                                          double &x, double &y, int &rI) {
+  if (id & INV_TAIL) {
+    const uint32_t c = id & ~INV_TAIL;
+    v = tv[c];
+    rI = t_idx[c] & 0xffff;
+    x = t_x[c];
+    y = t_y[c];
+    return;
+  }
+  const int u = (int)(id >> 16), r = (int)(id & 0xffffu);
+  const size_t i = cbase + (size_t)u * nr + r;
+  v = lam[i];
+  if (mB) v += wjj * mt.bu[u] * mB[r];
+  if (sizeof(T) == 8) {
+    rI = idx[i] & 0xffff;
+    x = (double)fx[i];
+    y = (double)fy[i];
+  } else {
+    uint2 w = fp2[i];
+    if (w.x == AFP_FAR) w = far_w[w.y];
+    rI = (int)(w.x >> AFP_FBITS);
+    const uint32_t m = (1u << AFP_FBITS) - 1u;
+    x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
+    y = (double)(__uint_as_float(0x3F800000u | ((w.y & m) << 2)) - 1.0f);
+  }
+}
+
+// Cb[j][p][q] = sum over the buckets (p - a, q - b), a, b = 0..3, of
+// lam * w_a(y) w_b(x) / 36.  One thread sums the nodes of R rows p0..p0+R-1
+// and Q columns q0..q0+Q-1: it visits the base rows p0-3 .. p0+R-1 once
+// each, and an entry found there adds to up to four of its rows (a static
+// row offset for each unrolled base row, so the sums stay in registers).
+// The buckets of one base row reaching the Q columns are adjacent, one
+// contiguous run of entries.  Writes every node of Cb.
+template <typename T, int R, int Q>
+__global__ void __launch_bounds__(128)
+    drift_adj_gather_kernel(const double *__restrict__ lam, const double *__restrict__ mB,
+                            MomentTables mt, const double *__restrict__ tv,
+                            double *__restrict__ Cb, const uint32_t *__restrict__ ends,
+                            const uint32_t *__restrict__ ent, const int64_t *__restrict__ ebase,
+                            const T *__restrict__ fx, const T *__restrict__ fy,
+                            const int32_t *__restrict__ idx, const uint2 *__restrict__ fp2,
+                            const uint2 *__restrict__ far_w, const int32_t *__restrict__ t_idx,
+                            const double *__restrict__ t_x, const double *__restrict__ t_y,
+                            Geometry g) {
+  const int q0 = (blockIdx.x * 32 + threadIdx.x) * Q;
+  const int p0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
+  const int j = blockIdx.z;
+  if (q0 >= g.pc || p0 >= g.nu + 3) return;
+  const size_t S = (size_t)g.nr * g.nu;
+  const uint32_t *endj = ends + (size_t)j * S;
+  const uint32_t *entj = ent + ebase[j];
+  const size_t cbase = (size_t)j * S;
+  const double wjj = mB ? mt.wj[j] : 0.0;
+  const int qlo = max(q0 - 3, 0), qhi = min(q0 + Q - 1, g.nr - 1);
+  double acc[R][Q];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int k = 0; k < Q; ++k) acc[r][k] = 0.0;
+  if (qlo <= qhi) {
+#pragma unroll
+    for (int t = 0; t < R + 3; ++t) {
+      const int pb = p0 - 3 + t;
+      if (pb < 0 || pb >= g.nu) continue;
+      const size_t k0 = (size_t)pb * g.nr + qlo, k1 = (size_t)pb * g.nr + qhi;
+      const uint32_t e1 = endj[k1];
+      for (uint32_t e = k0 ? endj[k0 - 1] : 0u; e < e1; ++e) {
+        double v, x, y;
+        int rI;
+        inv_entry<T>(entj[e], lam, mB, mt, wjj, tv, cbase, fx, fy, idx, fp2, far_w, t_idx, t_x,
+                     t_y, g.nr, v, x, y, rI);
+        const double s = 1.0 - y;
+        const double wy[4] = {bv2d(s), bv1d(s), bv1d(y), bv2d(y)};
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+          const int b = q0 + k - rI;
+          const double c = (b >= 0 && b <= 3) ? v * bweight(b, x) : 0.0;
+          // node row pb + a is acc[t - 3 + a]
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const int rr = t - 3 + a;
+            if (rr >= 0 && rr < R) acc[rr >= 0 && rr < R ? rr : 0][k] += c * wy[a];
+          }
+        }
+      }
+    }
+  }
+  double *out = Cb + ((size_t)j * (g.nu + 3) + p0) * g.pc + q0;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int k = 0; k < Q; ++k)
+      if (p0 + r < g.nu + 3 && q0 + k < g.pc) out[(size_t)r * g.pc + k] = acc[r][k] * (1.0 / 36.0);
+}
+
 }  // namespace
+
+template <typename T>
+cudaError_t launch_inv_fill(const int32_t *idx, const uint2 *fp2, const uint2 *far_w,
+                            const int32_t *t_idx, int64_t nch, uint32_t *ends, uint32_t *ent,
+                            const int64_t *ebase, const Geometry &g, cudaStream_t st) {
+  const size_t n = (size_t)g.nr * g.nu * g.nj + (size_t)nch;
+  inv_fill_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(idx, fp2, far_w, t_idx, nch, ends, ent,
+                                                        ebase, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inv_scan(uint32_t *ends, uint32_t *totals, const Geometry &g,
+                            cudaStream_t st) {
+  inv_scan_kernel<<<g.nj, 1024, 0, st>>>(ends, totals, (int64_t)g.nr * g.nu);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inv_sort(const uint32_t *ends, uint32_t *ent, const int64_t *ebase,
+                            const Geometry &g, cudaStream_t st) {
+  const int64_t S = (int64_t)g.nr * g.nu;
+  inv_sort_kernel<<<grid_for((size_t)S * g.nj, 256), 256, 0, st>>>(ends, ent, ebase, S,
+                                                                   S * g.nj);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chain_adj(const double *lam, const double *mB, const MomentTables &mt,
+                             double *ringb, double *tv, const int64_t *ch_cell,
+                             const int64_t *ch_start, const int32_t *ch_len, int64_t nch,
+                             int64_t ndrift, const Geometry &g, cudaStream_t st) {
+  if (nch <= 0) return cudaSuccess;
+  chain_adj_kernel<<<(unsigned)((nch + 255) / 256), 256, 0, st>>>(
+      lam, mB, mt, ringb, tv, ch_cell, ch_start, ch_len, nch, ndrift, g);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const MomentTables &mt,
+                                    const double *tv, double *Cb, const uint32_t *ends,
+                                    const uint32_t *ent, const int64_t *ebase, const T *fx,
+                                    const T *fy, const int32_t *idx, const uint2 *fp2,
+                                    const uint2 *far_w, const int32_t *t_idx, const double *t_x,
+                                    const double *t_y, int rows, int cols, const Geometry &g,
+                                    cudaStream_t st) {
+  auto go = [&](auto kernel, int R, int Q) {
+    const int per_block = 4 * R, cols_per_block = 32 * Q;
+    const dim3 grid((unsigned)((g.pc + cols_per_block - 1) / cols_per_block),
+                    (unsigned)((g.nu + 3 + per_block - 1) / per_block), (unsigned)g.nj);
+    kernel<<<grid, dim3(32, 4), 0, st>>>(lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2,
+                                         far_w, t_idx, t_x, t_y, g);
+    return cudaGetLastError();
+  };
+  if (cols == 1) return go(drift_adj_gather_kernel<T, 8, 1>, 8, 1);
+  if (rows == 4) return go(drift_adj_gather_kernel<T, 4, 2>, 4, 2);
+  return go(drift_adj_gather_kernel<T, 8, 2>, 8, 2);
+}
+
+#define VLS_INV_INST(T)                                                                       \
+  template cudaError_t launch_inv_fill<T>(const int32_t *, const uint2 *, const uint2 *,       \
+                                          const int32_t *, int64_t, uint32_t *, uint32_t *,    \
+                                          const int64_t *, const Geometry &, cudaStream_t);    \
+  template cudaError_t launch_drift_adj_gather<T>(                                            \
+      const double *, const double *, const MomentTables &, const double *, double *,         \
+      const uint32_t *, const uint32_t *, const int64_t *, const T *, const T *,              \
+      const int32_t *, const uint2 *, const uint2 *, const int32_t *, const double *,         \
+      const double *, int, int, const Geometry &, cudaStream_t);
+VLS_INV_INST(float)
+VLS_INV_INST(double)
+#undef VLS_INV_INST
 
 template <typename T>
 cudaError_t launch_drift_adj(const double *lam, double *Cb, const int32_t *idx, const T *fx,
@@ -358,7 +728,13 @@ cudaError_t launch_ucol_adj(const T *f, double *Gb, double *A, double *B, double
 
 cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTables &mt,
                              const Geometry &g, cudaStream_t st) {
-  shift_adj_kernel<<<1, 256, (size_t)g.nr * sizeof(double), st>>>(sbar, beta, mt, g);
+  const size_t smem = (size_t)g.nr * sizeof(double);
+  if (smem > (32u << 10)) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        shift_adj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  shift_adj_kernel<<<1, 1024, smem, st>>>(sbar, beta, mt, g);
   return cudaGetLastError();
 }
 

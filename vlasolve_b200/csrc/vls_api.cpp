@@ -130,6 +130,14 @@ struct vls_handle {
          *ab_B = nullptr, *ab_ringb = nullptr, *ab_sbar = nullptr, *ab_beta = nullptr;
   bool ab_rc = false;
   std::vector<void *> ab_stash;
+  double *ab_shifts = nullptr;  // shift of each stashed state (ab_nshift x N_r)
+  int ab_nshift = 0;
+  // inverse footpoint map of the drift's transpose (built for footpoint set
+  // fp_gen; see launch_inv_fill), the chain cells and tail adjoints
+  uint64_t fp_gen = 0, inv_gen = ~(uint64_t)0;
+  uint32_t *inv_ends = nullptr, *inv_ent = nullptr, *inv_tot = nullptr;
+  int64_t *inv_ebase = nullptr, *inv_chc = nullptr;
+  double *inv_tv = nullptr;
   bool adj_ready = false;
   std::vector<void *> adj_allocs;
 };
@@ -443,6 +451,7 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
     }
   }
   if (h->far_mode) TRY(upload_far(h, fh));
+  h->fp_gen++;
   return VLS_OK;
 }
 
@@ -592,6 +601,12 @@ static void free_all(vls_handle *h) {
   h->ab_lam = h->ab_Cb = h->ab_Gb = h->ab_A = h->ab_B = nullptr;
   h->ab_ringb = h->ab_sbar = h->ab_beta = nullptr;
   h->ab_stash.clear();
+  h->ab_shifts = nullptr;
+  h->ab_nshift = 0;
+  h->inv_ends = h->inv_ent = h->inv_tot = nullptr;
+  h->inv_ebase = h->inv_chc = nullptr;
+  h->inv_tv = nullptr;
+  h->inv_gen = ~(uint64_t)0;
   for (void *p : {(void *)h->far_w, (void *)h->far_cell, (void *)h->far_col,
                   (void *)h->far_prod})
     if (p) cudaFree(p);
@@ -1121,6 +1136,7 @@ extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
     }
     TRY(upload(h, h->fp2, p.data(), sizeof(uint2) * h->cells));
   }
+  h->fp_gen++;
   return VLS_OK;
 }
 
@@ -1631,37 +1647,111 @@ struct AdjBufs {
   std::vector<int64_t> ndrift;
   // chunked line kernels (else one thread per line through A and B)
   bool rc = false;
+  // drift transposed as a gather over the inverse footpoint map (else the
+  // scatter with FP64 atomics)
+  bool gather = true;
+  int gather_rows = 8, gather_cols = 2;  // C nodes per thread of the gather
+  bool pending = false;  // lam still lacks the moment term in beta[N_r..2 N_r)
+  bool lazy_moment = true;  // leave the moment term to the readers of lam
+  // shift of each stashed state (N_r per state), saved by the recomputation
+  double *shifts = nullptr;
   RcDir<double> rcu{}, rcr{};
 };
 }  // namespace
 
+// The inverse footpoint map of the current footpoints for the drift's
+// transpose (launch_inv_fill), built once per footpoint set: count, scan,
+// place, order.
 template <typename T>
-static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift) {
+static int ensure_inv(vls_handle *h) {
+  if (h->inv_gen == h->fp_gen) return VLS_OK;
+  const Geometry g = geometry(h);
+  const int64_t nch = h->nch;
+  if (!h->inv_ends) {
+    TRY(adj_alloc(h, &h->inv_ends, h->cells * sizeof(uint32_t)));
+    TRY(adj_alloc(h, &h->inv_ent, (h->cells + (size_t)nch) * sizeof(uint32_t)));
+    TRY(adj_alloc(h, &h->inv_tot, (size_t)g.nj * sizeof(uint32_t)));
+    TRY(adj_alloc(h, &h->inv_ebase, (size_t)(g.nj + 1) * sizeof(int64_t)));
+    TRY(adj_alloc(h, &h->inv_chc, (size_t)std::max<int64_t>(nch, 1) * sizeof(int64_t)));
+    TRY(adj_alloc(h, &h->inv_tv, (size_t)std::max<int64_t>(nch, 1) * sizeof(double)));
+  }
+  if (nch) TRY(upload(h, h->inv_chc, h->ch_cell_h.data(), sizeof(int64_t) * nch));
+  CK(h, cudaMemsetAsync(h->inv_ends, 0, h->cells * sizeof(uint32_t), h->st));
+  CK(h, launch_inv_fill<T>(h->idx, h->fp2, h->far_w, h->t_idx, nch, h->inv_ends, nullptr,
+                           nullptr, g, h->st));
+  CK(h, launch_inv_scan(h->inv_ends, h->inv_tot, g, h->st));
+  std::vector<uint32_t> tot((size_t)g.nj);
+  CK(h, cudaMemcpyAsync(tot.data(), h->inv_tot, sizeof(uint32_t) * g.nj, cudaMemcpyDeviceToHost,
+                        h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  std::vector<int64_t> eb((size_t)g.nj + 1, 0);
+  for (int j = 0; j < g.nj; ++j) eb[j + 1] = eb[j] + tot[j];
+  if ((size_t)eb[g.nj] > h->cells + (size_t)nch)
+    return fail(h, VLS_ECUDA, "adjoint: inverse footpoint map larger than its cells");
+  TRY(upload(h, h->inv_ebase, eb.data(), sizeof(int64_t) * eb.size()));
+  CK(h, launch_inv_fill<T>(h->idx, h->fp2, h->far_w, h->t_idx, nch, h->inv_ends, h->inv_ent,
+                           h->inv_ebase, g, h->st));
+  CK(h, launch_inv_sort(h->inv_ends, h->inv_ent, h->inv_ebase, g, h->st));
+  h->launches += 4;
+  h->inv_gen = h->fp_gen;
+  return VLS_OK;
+}
+
+template <typename T>
+// the transposed step n: state f_n, its drift count and its shift s(f_n)
+static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift,
+                    const double *shift) {
   const Geometry g = geometry(h);
   const MomentTables mt = moment_tables(h);
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
   const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
-  // the shift of this step, from f_n
-  CK(h, launch_moment<T>((const T *)fn, mt, h->partial, g, h->st));
-  CK(h, launch_scan(h->partial, mt, h->T2, h->bins, h->Mr, h->shift, h->mtot, h->count, g,
-                    h->st));
-  const size_t cbn = (size_t)g.nj * (g.nu + 3) * g.pc;
-  CK(h, cudaMemsetAsync(b.Cb, 0, cbn * sizeof(double), h->st));
-  CK(h, launch_drift_adj<T>(b.lam, b.Cb, h->idx, (const T *)h->fx, (const T *)h->fy, h->fp2,
-                            h->ch_start, h->ch_len, b.ringb, h->far_w, ndrift, g, h->st));
-  CK(h, launch_tails_adj(b.Cb, b.ringb, h->ch_start, h->ch_len, h->t_idx, h->t_x, h->t_y,
-                         h->nch, ndrift, g, h->st));
-  if (b.rc) {
-    CK(h, launch_prer_adj_rc(b.Cb, b.Gb, g, b.rcr, h->st));
-    CK(h, launch_ucol_adj_rc<T>((const T *)fn, b.Gb, b.lam, b.sbar, h->shift, g, b.rcu, h->st));
+  if (b.gather) {
+    // lam of this step is lam + the moment term of the step after it, when
+    // that was left pending
+    const double *mB = b.pending ? b.beta + g.nr : nullptr;
+    if (h->nch > 0)
+      CK(h, timed(h, VLS_K_ADJ_TAILS, [&] {
+        return launch_chain_adj(b.lam, mB, mt, b.ringb, h->inv_tv, h->inv_chc, h->ch_start,
+                                h->ch_len, h->nch, ndrift, g, h->st);
+      }));
+    CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
+      return launch_drift_adj_gather<T>(b.lam, mB, mt, h->inv_tv, b.Cb, h->inv_ends,
+                                        h->inv_ent, h->inv_ebase, (const T *)h->fx,
+                                        (const T *)h->fy, h->idx, h->fp2, h->far_w, h->t_idx,
+                                        h->t_x, h->t_y, b.gather_rows, b.gather_cols, g, h->st);
+    }));
   } else {
-    CK(h, launch_prer_adj(b.Cb, b.Gb, g, tr, h->st));
-    CK(h, launch_ucol_adj<T>((const T *)fn, b.Gb, b.A, b.B, b.lam, b.sbar, h->shift, g, tu,
-                             h->st));
+    const size_t cbn = (size_t)g.nj * (g.nu + 3) * g.pc;
+    CK(h, cudaMemsetAsync(b.Cb, 0, cbn * sizeof(double), h->st));
+    CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
+      return launch_drift_adj<T>(b.lam, b.Cb, h->idx, (const T *)h->fx, (const T *)h->fy,
+                                 h->fp2, h->ch_start, h->ch_len, b.ringb, h->far_w, ndrift, g,
+                                 h->st);
+    }));
+    if (h->nch > 0)
+      CK(h, timed(h, VLS_K_ADJ_TAILS, [&] {
+        return launch_tails_adj(b.Cb, b.ringb, h->ch_start, h->ch_len, h->t_idx, h->t_x,
+                                h->t_y, h->nch, ndrift, g, h->st);
+      }));
   }
-  CK(h, launch_shift_adj(b.sbar, b.beta, mt, g, h->st));
-  CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
-  h->launches += 9;
+  CK(h, timed(h, VLS_K_ADJ_PRER, [&] {
+    return b.rc ? launch_prer_adj_rc(b.Cb, b.Gb, g, b.rcr, h->st)
+                : launch_prer_adj(b.Cb, b.Gb, g, tr, h->st);
+  }));
+  CK(h, timed(h, VLS_K_ADJ_UCOL, [&] {
+    return b.rc ? launch_ucol_adj_rc<T>((const T *)fn, b.Gb, b.lam, b.sbar, shift, g, b.rcu,
+                                        h->st)
+                : launch_ucol_adj<T>((const T *)fn, b.Gb, b.A, b.B, b.lam, b.sbar, shift, g, tu,
+                                     h->st);
+  }));
+  CK(h, timed(h, VLS_K_ADJ_MOMENT, [&] { return launch_shift_adj(b.sbar, b.beta, mt, g, h->st); }));
+  if (b.gather && b.lazy_moment) {
+    b.pending = true;  // added by the next step's readers of lam, or at the end
+  } else {
+    CK(h, timed(h, VLS_K_ADJ_MOMENT, [&] {
+      return launch_moment_adj(b.lam, b.beta, mt, g, h->st);
+    }));
+  }
   return VLS_OK;
 }
 
@@ -1678,7 +1768,16 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
     b.rc = rc_adj_supported(h->tu, h->tr) && !(pf && std::string(pf) == "segment");
     b.rcu = rc_dir<double>(h->tu, 2);
     b.rcr = rc_dir<double>(h->tr, 2);
+    const char *da = std::getenv("VLS_DRIFT_ADJ");
+    b.gather = !(da && std::string(da) == "atomic");
+    if (const char *gr = std::getenv("VLS_ADJ_GATHER_R")) b.gather_rows = std::atoi(gr);
+    if (const char *gq = std::getenv("VLS_ADJ_GATHER_Q")) b.gather_cols = std::atoi(gq);
+    const char *mp = std::getenv("VLS_ADJ_MOMENT");
+    b.lazy_moment = !(mp && std::string(mp) == "pass");
+    // the inverse map's ids hold u in 15 bits
+    if (h->co.nu >= (1 << 15)) b.gather = false;
   }
+  if (b.gather) TRY(ensure_inv<T>(h));
   if (!h->ab_lam || (h->ab_rc != b.rc && !b.rc)) {
     if (!h->ab_lam) {
       TRY(adj_alloc(h, &h->ab_lam, cells * sizeof(double)));
@@ -1686,7 +1785,7 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
       TRY(adj_alloc(h, &h->ab_Gb, gn * sizeof(double)));
       TRY(adj_alloc(h, &h->ab_ringb, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double)));
       TRY(adj_alloc(h, &h->ab_sbar, (size_t)g.nj * g.nr * sizeof(double)));
-      TRY(adj_alloc(h, &h->ab_beta, (size_t)g.nr * sizeof(double)));
+      TRY(adj_alloc(h, &h->ab_beta, (size_t)2 * g.nr * sizeof(double)));
     }
     // scratch of the one-thread-per-line kernels
     TRY(adj_alloc(h, &h->ab_A, (b.rc ? 1 : gn) * sizeof(double)));
@@ -1734,6 +1833,11 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
     h->adj_sub.resize((K + K2 - 1) / K2);  // entries allocate on first save
   b.stash.assign(h->ab_stash.begin(), h->ab_stash.begin() + K2);
   b.ndrift.assign(K2, 0);
+  if (h->ab_nshift < K2) {
+    TRY(adj_alloc(h, &h->ab_shifts, (size_t)K2 * g.nr * sizeof(double)));
+    h->ab_nshift = K2;
+  }
+  b.shifts = h->ab_shifts;
   // seed: the derivative of the loss with respect to the final radial bins
   TRY(upload(h, b.beta, dbins, (size_t)g.nr * sizeof(double)));
   CK(h, cudaMemsetAsync(b.lam, 0, cells * sizeof(double), h->st));
@@ -1746,9 +1850,15 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
       CK(h, cudaMemcpyAsync(b.stash[n - a], h->f, h->esize * cells, cudaMemcpyDeviceToDevice,
                             h->st));
       b.ndrift[n - a] = h->ndrift;
+      // the shift of step n, as the step computes it from f_n
+      TRY(ensure_moments<T>(h));
+      TRY(scan_once(h));
+      CK(h, cudaMemcpyAsync(b.shifts + (size_t)(n - a) * g.nr, h->shift, g.nr * sizeof(double),
+                            cudaMemcpyDeviceToDevice, h->st));
       if (n + 1 < e) TRY(vls_step(h, 1));
     }
-    for (int64_t n = e - 1; n >= a; --n) TRY(adj_step<T>(h, b, b.stash[n - a], b.ndrift[n - a]));
+    for (int64_t n = e - 1; n >= a; --n)
+      TRY(adj_step<T>(h, b, b.stash[n - a], b.ndrift[n - a], b.shifts + (size_t)(n - a) * g.nr));
     return VLS_OK;
   };
   const int ncp = h->adj_ncp;
@@ -1774,6 +1884,7 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
     }
   }
   h->adj_last_inner = two_level ? K2 : 0;
+  if (b.pending) CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
   // results: the derivative with respect to the initial grid and the initial
   // chain values (logical ring order at the first step)
   CK(h, cudaMemcpyAsync(df0, b.lam, cells * sizeof(double), cudaMemcpyDeviceToHost, h->st));

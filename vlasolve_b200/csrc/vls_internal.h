@@ -162,12 +162,40 @@ cudaError_t launch_tails_adj(double *Cb, double *ringb, const int64_t *ch_start,
                              const int32_t *ch_len, const int32_t *t_idx, const double *t_x,
                              const double *t_y, int64_t nch, int64_t ndrift, const Geometry &g,
                              cudaStream_t st);
+// the drift transposed as a gather over the inverse footpoint map: buckets of
+// cells and chain tails by the base node of their stencil (ends: [nj][nr*nu]
+// bucket ends within the slice's entries; ent: ids, ascending per bucket;
+// ebase: first entry of each slice).  inv_fill counts (ent == nullptr) or
+// places; inv_scan turns counts into starts and writes each slice's total.
+template <typename T>
+cudaError_t launch_inv_fill(const int32_t *idx, const uint2 *fp2, const uint2 *far_w,
+                            const int32_t *t_idx, int64_t nch, uint32_t *ends, uint32_t *ent,
+                            const int64_t *ebase, const Geometry &g, cudaStream_t st);
+cudaError_t launch_inv_scan(uint32_t *ends, uint32_t *totals, const Geometry &g,
+                            cudaStream_t st);
+cudaError_t launch_inv_sort(const uint32_t *ends, uint32_t *ent, const int64_t *ebase,
+                            const Geometry &g, cudaStream_t st);
+// chain fronts and tails transposed; mB: pending moment term (or null)
+cudaError_t launch_chain_adj(const double *lam, const double *mB, const MomentTables &mt,
+                             double *ringb, double *tv, const int64_t *ch_cell,
+                             const int64_t *ch_start, const int32_t *ch_len, int64_t nch,
+                             int64_t ndrift, const Geometry &g, cudaStream_t st);
+// rows x cols C nodes per thread (8 x 2 by default; 8 x 1, 4 x 2)
+template <typename T>
+cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const MomentTables &mt,
+                                    const double *tv, double *Cb, const uint32_t *ends,
+                                    const uint32_t *ent, const int64_t *ebase, const T *fx,
+                                    const T *fy, const int32_t *idx, const uint2 *fp2,
+                                    const uint2 *far_w, const int32_t *t_idx, const double *t_x,
+                                    const double *t_y, int rows, int cols, const Geometry &g,
+                                    cudaStream_t st);
 cudaError_t launch_prer_adj(const double *Cb, double *Gb, const Geometry &g,
                             const DirTables &tr, cudaStream_t st);
 template <typename T>
 cudaError_t launch_ucol_adj(const T *f, double *Gb, double *A, double *B, double *lam,
                             double *sbar, const double *shift, const Geometry &g,
                             const DirTables &tu, cudaStream_t st);
+// beta: 2 N_r values (beta, then the moment's transpose per radius)
 cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTables &mt,
                              const Geometry &g, cudaStream_t st);
 cudaError_t launch_moment_adj(double *lam, const double *beta, const MomentTables &mt,
