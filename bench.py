@@ -562,6 +562,7 @@ def large_block(nsteps, K):
     s.sync()
     out["step_adjoint_s"] = time.perf_counter() - ta
     out["step_adjoint_ms_per_step"] = 1e3 * out["step_adjoint_s"] / nsteps
+    out["inner_every_used"] = s.adjoint_inner_used()
     # per-kernel device times of a 4-step backward pass (3 recomputed forward
     # steps and 4 transposed steps)
     s.adjoint_forward(4, 4)
@@ -574,7 +575,6 @@ def large_block(nsteps, K):
     out["loss_value"] = float(L.detach())
     out["forward_checkpointed_s"] = t2 - t1
     out["backward_s"] = t3 - t2
-    out["inner_every_used"] = s.adjoint_inner_used()
     out["hbm_gb"] = {"step_handle_forward": fwd_bytes / 1e9,
                      "step_handle_with_adjoint": s.device_bytes() / 1e9,
                      "initial_state_handle_fp64": p.ic.device_bytes() / 1e9,
@@ -602,6 +602,30 @@ def large_block(nsteps, K):
                         "fp32_vs_fp64_rel": float(np.max(np.abs(grads["fp32"] - grads["fp64"]))
                                                   / np.max(np.abs(grads["fp64"])))}
     out["seconds"] = time.perf_counter() - t_all
+    return out
+
+
+def adjoint_kernels_block(grid, nsteps, precision):
+    """Per-kernel device times of one backward pass of `nsteps` steps
+    (checkpoint every nsteps) on the PLDF case of the large block at grid
+    (N_r - 1, N_u - 1, N_J): the recomputed forward steps and the transposed
+    steps, divided by nsteps.  A first backward pass builds the inverse
+    footpoint map and is not timed."""
+    import numpy as np
+    from vlasolve_b200 import VlasovSolver21Spline
+    s = VlasovSolver21Spline(dict(LARGE, Pres=grid[0], Ures=(grid[1], grid[2])),
+                             precision=precision)
+    s.adjoint_forward(nsteps, nsteps)
+    dbins = np.cos(0.01 * np.arange(s.nr))
+    s.adjoint_backward(dbins)
+    s.set_profiling(True)
+    s.adjoint_backward(dbins)
+    prof = s.profile_read()
+    s.set_profiling(False)
+    out = {"workload": "pldf_%dx%dx%d" % tuple(grid), "grid": [s.nr, s.nu, s.nj],
+           "precision": precision, "steps": nsteps,
+           "kernel_ms_per_step": {k: v[0] / nsteps for k, v in prof.items() if v[1]}}
+    s.close()
     return out
 
 
@@ -659,11 +683,18 @@ def main():
                     help="only the 1025 x 1025 x 512 PLDF forward + adjoint block")
     ap.add_argument("--large-steps", type=int, default=1000)
     ap.add_argument("--large-every", type=int, default=100)
+    ap.add_argument("--adjoint-kernels", metavar="PRES,NU,NJ",
+                    help="only the per-kernel times of a backward pass on this PLDF grid")
+    ap.add_argument("--adjoint-kernel-steps", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         reference_arm(args)
+    elif args.adjoint_kernels:
+        grid = [int(x) for x in args.adjoint_kernels.split(",")]
+        print(json.dumps({"adjoint_kernels": adjoint_kernels_block(
+            grid, args.adjoint_kernel_steps, args.precision)}), flush=True)
     elif args.large:
         print(json.dumps({"large": large_block(args.large_steps, args.large_every)}), flush=True)
     else:
