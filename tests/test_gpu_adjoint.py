@@ -175,13 +175,15 @@ def test_far_cell_layout_keeps_the_adjoint(monkeypatch):
     np.testing.assert_allclose(g, g_ref, rtol=1e-6)
 
 
-def test_long_line_adjoint_layout_keeps_the_gradient(monkeypatch):
-    """The 8-line chunk layouts the transposed solves take for lines too long
-    for the default ones (1025 rows), forced here on short lines."""
+@pytest.mark.parametrize("layout", ["long", "short"])
+def test_other_adjoint_line_layouts_keep_the_gradient(layout, monkeypatch):
+    """The chunk layouts the transposed solves take besides the default ones:
+    the r layout of lines too long for the default (1025 rows), forced here
+    on short lines ("long"), and the 16-line u layout ("short")."""
     p_ref = problem("fp64")
     target = p_ref.run(THETA + DTHETA)
     _, g_ref = loss_and_grad(p_ref, target)
-    monkeypatch.setenv("VLS_ADJ_RC", "long")
+    monkeypatch.setenv("VLS_ADJ_RC", layout)
     for prec in ("fp64", "fp32"):
         p = problem(prec)
         _, g = loss_and_grad(p, target)
@@ -238,3 +240,32 @@ def test_gather_drift_transpose_is_deterministic(monkeypatch):
     (a0, ac), (b0, bc) = _solver_backward("fp32", ["", ""], monkeypatch)
     np.testing.assert_array_equal(a0, b0)
     np.testing.assert_array_equal(ac, bc)
+
+
+def test_inverse_map_follows_new_footpoints(monkeypatch):
+    """vls_set_footpoints after a backward pass: the next gather uses the
+    inverse map of the new footpoints (base columns moved by one), checked
+    against the atomic scatter, which reads the footpoints directly."""
+    import ctypes
+    from vlasolve_b200 import VlasovSolver21Spline
+    s = VlasovSolver21Spline(cfg(pres=40, ures=(28, 10)), precision="fp32")
+    dbins = np.cos(0.3 * np.arange(s.nr, dtype=np.float64))
+    s.adjoint_forward(4, 2)
+    monkeypatch.delenv("VLS_DRIFT_ADJ", raising=False)
+    s.adjoint_backward(dbins)
+    fp = s.footpoints()
+    rI = fp["rI"].copy()
+    move = (fp["out"] == 0) & (rI >= 1)
+    rI[move] -= 1
+    i32, u8 = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint8)
+    d = ctypes.POINTER(ctypes.c_double)
+    assert s._L.vls_set_footpoints(
+        s._h, rI.ctypes.data_as(i32), fp["rF"].ctypes.data_as(d),
+        fp["uI"].ctypes.data_as(i32), fp["uF"].ctypes.data_as(d),
+        fp["out"].ctypes.data_as(u8), fp["driftR"].ctypes.data_as(d)) == 0
+    s.adjoint_forward(4, 2)
+    g0, gc = s.adjoint_backward(dbins)
+    monkeypatch.setenv("VLS_DRIFT_ADJ", "atomic")
+    a0, ac = s.adjoint_backward(dbins)
+    np.testing.assert_allclose(g0, a0, rtol=1e-11, atol=1e-13 * np.max(np.abs(a0)))
+    np.testing.assert_allclose(gc, ac, rtol=1e-11, atol=1e-13 * max(np.max(np.abs(ac)), 1e-300))

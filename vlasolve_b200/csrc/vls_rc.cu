@@ -1428,16 +1428,17 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
   }
 }
 
-// adjoint line kernels (FP64): u lines with 15-row chunks of 16 lines, r
-// lines with 15-row chunks of 8 lines; lines too long for those in 8-line
-// blocks of up to 70 / 78 chunks (VLS_ADJ_RC=long takes those for every
-// length, for tests); tables from rc_dir<double>(t, 2)
-static bool adj_long_forced() {
-  static const bool f = [] {
-    const char *e = std::getenv("VLS_ADJ_RC");
-    return e && std::string(e) == "long";
-  }();
-  return f;
+// adjoint line kernels (FP64): u lines with 15-row chunks in 8-line blocks
+// (up to 70 chunks; 12 % faster than 16-line blocks on 513-row lines), r
+// lines with 15-row chunks of 8 lines and lines too long for those in
+// 8-line blocks of up to 78 chunks.  VLS_ADJ_RC=long takes the long-line r
+// layout for every length, VLS_ADJ_RC=short the 16-line u layout where it
+// fits (read at each launch, for tests); tables from rc_dir<double>(t, 2)
+static int adj_rc_forced() {
+  const char *e = std::getenv("VLS_ADJ_RC");
+  if (!e) return 0;
+  const std::string v(e);
+  return v == "long" ? 1 : v == "short" ? 2 : 0;
 }
 bool rc_adj_supported(const HostDirTables &tu, const HostDirTables &tr) {
   return tu.M - 2 > CfgAdjU::L && tr.M - 2 > CfgAdjR::L &&
@@ -1466,7 +1467,7 @@ template <typename T>
 cudaError_t launch_ucol_adj_rc(const T *f, const double *Gb, double *lam, double *sbar,
                                const double *shift, const Geometry &g, const RcDir<double> &tu,
                                cudaStream_t st) {
-  if (tu.S <= rc_maxs<CfgAdjU>() && !adj_long_forced())
+  if (tu.S <= rc_maxs<CfgAdjU>() && adj_rc_forced() == 2)
     return ucol_adj_go<T, CfgAdjU>(f, Gb, lam, sbar, shift, g, tu, st);
   return ucol_adj_go<T, CfgAdjU2>(f, Gb, lam, sbar, shift, g, tu, st);
 }
@@ -1489,7 +1490,7 @@ static cudaError_t prer_adj_go(const double *Cb, double *Gb, const Geometry &g,
 
 cudaError_t launch_prer_adj_rc(const double *Cb, double *Gb, const Geometry &g,
                                const RcDir<double> &tr, cudaStream_t st) {
-  if (tr.S <= rc_maxs<CfgAdjR>() && !adj_long_forced())
+  if (tr.S <= rc_maxs<CfgAdjR>() && adj_rc_forced() != 1)
     return prer_adj_go<CfgAdjR>(Cb, Gb, g, tr, st);
   return prer_adj_go<CfgAdjR2>(Cb, Gb, g, tr, st);
 }
