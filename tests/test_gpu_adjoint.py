@@ -269,3 +269,23 @@ def test_inverse_map_follows_new_footpoints(monkeypatch):
     a0, ac = s.adjoint_backward(dbins)
     np.testing.assert_allclose(g0, a0, rtol=1e-11, atol=1e-13 * np.max(np.abs(a0)))
     np.testing.assert_allclose(gc, ac, rtol=1e-11, atol=1e-13 * max(np.max(np.abs(ac)), 1e-300))
+
+
+@pytest.mark.parametrize("far", [False, True])
+def test_entry_ordered_gather_matches_cell_ordered_gather(far, monkeypatch):
+    """FP32 handles: the gather over entry-ordered values and packed words
+    against the gather that reads lam and the footpoints through each
+    entry's cell index (with the far-cell layout too)."""
+    from vlasolve_b200 import VlasovSolver21Spline
+    if far:
+        monkeypatch.setenv("VLS_FAR", "1")
+    s = VlasovSolver21Spline(cfg(pres=40, ures=(28, 10)), precision="fp32")
+    s.adjoint_forward(7, 3)
+    dbins = np.cos(0.3 * np.arange(s.nr, dtype=np.float64))
+    monkeypatch.delenv("VLS_DRIFT_ADJ", raising=False)
+    monkeypatch.setenv("VLS_ADJ_GATHER_PERM", "0")
+    a0, ac = s.adjoint_backward(dbins)
+    monkeypatch.setenv("VLS_ADJ_GATHER_PERM", "1")
+    p0, pc = s.adjoint_backward(dbins)
+    np.testing.assert_allclose(p0, a0, rtol=1e-13, atol=1e-15 * np.max(np.abs(a0)))
+    np.testing.assert_allclose(pc, ac, rtol=1e-13, atol=1e-15 * max(np.max(np.abs(ac)), 1e-300))

@@ -19,6 +19,8 @@
 // comparison and for grids with N_u >= 2^15.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "vls_internal.h"
 
 namespace vls {
@@ -617,6 +619,131 @@ __global__ void __launch_bounds__(128)
       if (p0 + r < g.nu + 3 && q0 + k < g.pc) out[(size_t)r * g.pc + k] = acc[r][k] * (1.0 / 36.0);
 }
 
+// Entry-ordered form of the gather (FP32 handles).  The packed footpoint
+// word of each entry (far cells resolved; a chain tail is GEO_TAIL, chain
+// id) is stored once in entry order when the map is built, and each
+// transposed step first permutes its values into entry order (vperm: lam
+// plus the pending moment term, or the tail's ring adjoint), so that a
+// visit of the gather reads two arrays at the same index.  For FP64
+// handles the entry-ordered fractions (16 B) cost more than they save, and
+// the cell-ordered gather above is used.
+constexpr uint32_t GEO_TAIL = 0xFFFFFFFFu;
+
+__global__ void inv_geo_kernel(const uint32_t *__restrict__ ent,
+                               const int64_t *__restrict__ ebase, const uint2 *__restrict__ fp2,
+                               const uint2 *__restrict__ far_w, uint2 *__restrict__ geo,
+                               Geometry g) {
+  const int j = blockIdx.y;
+  const int64_t e0 = ebase[j], e1 = ebase[j + 1];
+  const size_t cbase = (size_t)j * g.nr * g.nu;
+  for (int64_t e = e0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < e1;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t id = ent[e];
+    if (id & INV_TAIL) {
+      geo[e] = make_uint2(GEO_TAIL, id & ~INV_TAIL);
+      continue;
+    }
+    uint2 w = fp2[cbase + (size_t)(id >> 16) * g.nr + (id & 0xffffu)];
+    if (w.x == AFP_FAR) w = far_w[w.y];
+    geo[e] = w;
+  }
+}
+
+// values of this transposed step in entry order
+__global__ void inv_perm_kernel(const uint32_t *__restrict__ ent,
+                                const int64_t *__restrict__ ebase, const double *__restrict__ lam,
+                                const double *__restrict__ mB, MomentTables mt,
+                                const double *__restrict__ tv, double *__restrict__ vperm,
+                                Geometry g) {
+  const int j = blockIdx.y;
+  const int64_t e0 = ebase[j], e1 = ebase[j + 1];
+  const size_t cbase = (size_t)j * g.nr * g.nu;
+  const double wjj = mB ? mt.wj[j] : 0.0;
+  for (int64_t e = e0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < e1;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t id = ent[e];
+    double v;
+    if (id & INV_TAIL) {
+      v = tv[id & ~INV_TAIL];
+    } else {
+      const int u = (int)(id >> 16), r = (int)(id & 0xffffu);
+      v = lam[cbase + (size_t)u * g.nr + r];
+      if (mB) v += wjj * mt.bu[u] * mB[r];
+    }
+    vperm[e] = v;
+  }
+}
+
+// the gather of drift_adj_gather_kernel over entry-ordered values and
+// packed words (same nodes per thread, same summation order)
+template <int R, int Q>
+__global__ void __launch_bounds__(128)
+    drift_adj_gather_perm_kernel(const double *__restrict__ vperm, const uint2 *__restrict__ geo,
+                                 double *__restrict__ Cb, const uint32_t *__restrict__ ends,
+                                 const int64_t *__restrict__ ebase,
+                                 const int32_t *__restrict__ t_idx,
+                                 const double *__restrict__ t_x, const double *__restrict__ t_y,
+                                 Geometry g) {
+  const int q0 = (blockIdx.x * 32 + threadIdx.x) * Q;
+  const int p0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
+  const int j = blockIdx.z;
+  if (q0 >= g.pc || p0 >= g.nu + 3) return;
+  const size_t S = (size_t)g.nr * g.nu;
+  const uint32_t *endj = ends + (size_t)j * S;
+  const int64_t eb = ebase[j];
+  const double *vj = vperm + eb;
+  const uint2 *gj = geo + eb;
+  const int qlo = max(q0 - 3, 0), qhi = min(q0 + Q - 1, g.nr - 1);
+  double acc[R][Q];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int k = 0; k < Q; ++k) acc[r][k] = 0.0;
+  if (qlo <= qhi) {
+#pragma unroll
+    for (int t = 0; t < R + 3; ++t) {
+      const int pb = p0 - 3 + t;
+      if (pb < 0 || pb >= g.nu) continue;
+      const size_t k0 = (size_t)pb * g.nr + qlo, k1 = (size_t)pb * g.nr + qhi;
+      const uint32_t e1 = endj[k1];
+      for (uint32_t e = k0 ? endj[k0 - 1] : 0u; e < e1; ++e) {
+        const double v = vj[e];
+        const uint2 w = gj[e];
+        double x, y;
+        int rI;
+        if (w.x == GEO_TAIL) {
+          rI = t_idx[w.y] & 0xffff;
+          x = t_x[w.y];
+          y = t_y[w.y];
+        } else {
+          rI = (int)(w.x >> AFP_FBITS);
+          const uint32_t m = (1u << AFP_FBITS) - 1u;
+          x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
+          y = (double)(__uint_as_float(0x3F800000u | ((w.y & m) << 2)) - 1.0f);
+        }
+        const double s = 1.0 - y;
+        const double wy[4] = {bv2d(s), bv1d(s), bv1d(y), bv2d(y)};
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+          const int b = q0 + k - rI;
+          const double c = (b >= 0 && b <= 3) ? v * bweight(b, x) : 0.0;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const int rr = t - 3 + a;
+            if (rr >= 0 && rr < R) acc[rr >= 0 && rr < R ? rr : 0][k] += c * wy[a];
+          }
+        }
+      }
+    }
+  }
+  double *out = Cb + ((size_t)j * (g.nu + 3) + p0) * g.pc + q0;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int k = 0; k < Q; ++k)
+      if (p0 + r < g.nu + 3 && q0 + k < g.pc) out[(size_t)r * g.pc + k] = acc[r][k] * (1.0 / 36.0);
+}
+
 }  // namespace
 
 template <typename T>
@@ -659,19 +786,43 @@ cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const M
                                     const uint32_t *ent, const int64_t *ebase, const T *fx,
                                     const T *fy, const int32_t *idx, const uint2 *fp2,
                                     const uint2 *far_w, const int32_t *t_idx, const double *t_x,
-                                    const double *t_y, int rows, int cols, const Geometry &g,
-                                    cudaStream_t st) {
-  auto go = [&](auto kernel, int R, int Q) {
-    const int per_block = 4 * R, cols_per_block = 32 * Q;
-    const dim3 grid((unsigned)((g.pc + cols_per_block - 1) / cols_per_block),
-                    (unsigned)((g.nu + 3 + per_block - 1) / per_block), (unsigned)g.nj);
-    kernel<<<grid, dim3(32, 4), 0, st>>>(lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2,
-                                         far_w, t_idx, t_x, t_y, g);
-    return cudaGetLastError();
-  };
-  if (cols == 1) return go(drift_adj_gather_kernel<T, 8, 1>, 8, 1);
-  if (rows == 4) return go(drift_adj_gather_kernel<T, 4, 2>, 4, 2);
-  return go(drift_adj_gather_kernel<T, 8, 2>, 8, 2);
+                                    const double *t_y, const Geometry &g, cudaStream_t st) {
+  constexpr int R = 8, Q = 2;
+  const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
+                  (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
+  drift_adj_gather_kernel<T, R, Q><<<grid, dim3(32, 4), 0, st>>>(
+      lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2, far_w, t_idx, t_x, t_y, g);
+  return cudaGetLastError();
+}
+
+static dim3 slice_grid(const Geometry &g) {
+  const size_t per = ((size_t)g.nr * g.nu + 255) / 256;
+  return dim3((unsigned)std::min<size_t>(per ? per : 1, 64), (unsigned)g.nj);
+}
+
+cudaError_t launch_inv_geo(const uint32_t *ent, const int64_t *ebase, const uint2 *fp2,
+                           const uint2 *far_w, uint2 *geo, const Geometry &g, cudaStream_t st) {
+  inv_geo_kernel<<<slice_grid(g), 256, 0, st>>>(ent, ebase, fp2, far_w, geo, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inv_perm(const uint32_t *ent, const int64_t *ebase, const double *lam,
+                            const double *mB, const MomentTables &mt, const double *tv,
+                            double *vperm, const Geometry &g, cudaStream_t st) {
+  inv_perm_kernel<<<slice_grid(g), 256, 0, st>>>(ent, ebase, lam, mB, mt, tv, vperm, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_drift_adj_gather_perm(const double *vperm, const uint2 *geo, double *Cb,
+                                         const uint32_t *ends, const int64_t *ebase,
+                                         const int32_t *t_idx, const double *t_x,
+                                         const double *t_y, const Geometry &g, cudaStream_t st) {
+  constexpr int R = 8, Q = 2;
+  const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
+                  (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
+  drift_adj_gather_perm_kernel<R, Q><<<grid, dim3(32, 4), 0, st>>>(vperm, geo, Cb, ends, ebase,
+                                                                    t_idx, t_x, t_y, g);
+  return cudaGetLastError();
 }
 
 #define VLS_INV_INST(T)                                                                       \
@@ -682,8 +833,9 @@ cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const M
       const double *, const double *, const MomentTables &, const double *, double *,         \
       const uint32_t *, const uint32_t *, const int64_t *, const T *, const T *,              \
       const int32_t *, const uint2 *, const uint2 *, const int32_t *, const double *,         \
-      const double *, int, int, const Geometry &, cudaStream_t);
+      const double *, const Geometry &, cudaStream_t);
 VLS_INV_INST(float)
+
 VLS_INV_INST(double)
 #undef VLS_INV_INST
 

@@ -138,6 +138,10 @@ struct vls_handle {
   uint32_t *inv_ends = nullptr, *inv_ent = nullptr, *inv_tot = nullptr;
   int64_t *inv_ebase = nullptr, *inv_chc = nullptr;
   double *inv_tv = nullptr;
+  // FP32 handles: the entries' packed words and each step's values in entry
+  // order
+  uint2 *inv_geo = nullptr;
+  double *inv_vperm = nullptr;
   bool adj_ready = false;
   std::vector<void *> adj_allocs;
 };
@@ -606,6 +610,8 @@ static void free_all(vls_handle *h) {
   h->inv_ends = h->inv_ent = h->inv_tot = nullptr;
   h->inv_ebase = h->inv_chc = nullptr;
   h->inv_tv = nullptr;
+  h->inv_geo = nullptr;
+  h->inv_vperm = nullptr;
   h->inv_gen = ~(uint64_t)0;
   for (void *p : {(void *)h->far_w, (void *)h->far_cell, (void *)h->far_col,
                   (void *)h->far_prod})
@@ -1650,9 +1656,9 @@ struct AdjBufs {
   // drift transposed as a gather over the inverse footpoint map (else the
   // scatter with FP64 atomics)
   bool gather = true;
-  int gather_rows = 8, gather_cols = 2;  // C nodes per thread of the gather
   bool pending = false;  // lam still lacks the moment term in beta[N_r..2 N_r)
   bool lazy_moment = true;  // leave the moment term to the readers of lam
+  bool perm = true;  // FP32 handles: the gather over entry-ordered values
   // shift of each stashed state (N_r per state), saved by the recomputation
   double *shifts = nullptr;
   RcDir<double> rcu{}, rcr{};
@@ -1674,6 +1680,11 @@ static int ensure_inv(vls_handle *h) {
     TRY(adj_alloc(h, &h->inv_ebase, (size_t)(g.nj + 1) * sizeof(int64_t)));
     TRY(adj_alloc(h, &h->inv_chc, (size_t)std::max<int64_t>(nch, 1) * sizeof(int64_t)));
     TRY(adj_alloc(h, &h->inv_tv, (size_t)std::max<int64_t>(nch, 1) * sizeof(double)));
+    if (sizeof(T) == 4) {
+      const size_t ne = h->cells + (size_t)nch;
+      TRY(adj_alloc(h, &h->inv_geo, ne * sizeof(uint2)));
+      TRY(adj_alloc(h, &h->inv_vperm, ne * sizeof(double)));
+    }
   }
   if (nch) TRY(upload(h, h->inv_chc, h->ch_cell_h.data(), sizeof(int64_t) * nch));
   CK(h, cudaMemsetAsync(h->inv_ends, 0, h->cells * sizeof(uint32_t), h->st));
@@ -1692,6 +1703,10 @@ static int ensure_inv(vls_handle *h) {
   CK(h, launch_inv_fill<T>(h->idx, h->fp2, h->far_w, h->t_idx, nch, h->inv_ends, h->inv_ent,
                            h->inv_ebase, g, h->st));
   CK(h, launch_inv_sort(h->inv_ends, h->inv_ent, h->inv_ebase, g, h->st));
+  if (h->inv_geo) {
+    CK(h, launch_inv_geo(h->inv_ent, h->inv_ebase, h->fp2, h->far_w, h->inv_geo, g, h->st));
+    h->launches++;
+  }
   h->launches += 4;
   h->inv_gen = h->fp_gen;
   return VLS_OK;
@@ -1714,11 +1729,21 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift,
         return launch_chain_adj(b.lam, mB, mt, b.ringb, h->inv_tv, h->inv_chc, h->ch_start,
                                 h->ch_len, h->nch, ndrift, g, h->st);
       }));
+    if (b.perm) {
+      CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
+        return launch_inv_perm(h->inv_ent, h->inv_ebase, b.lam, mB, mt, h->inv_tv, h->inv_vperm,
+                               g, h->st);
+      }));
+      CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
+        return launch_drift_adj_gather_perm(h->inv_vperm, h->inv_geo, b.Cb, h->inv_ends,
+                                            h->inv_ebase, h->t_idx, h->t_x, h->t_y, g, h->st);
+      }));
+    } else
     CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
       return launch_drift_adj_gather<T>(b.lam, mB, mt, h->inv_tv, b.Cb, h->inv_ends,
                                         h->inv_ent, h->inv_ebase, (const T *)h->fx,
                                         (const T *)h->fy, h->idx, h->fp2, h->far_w, h->t_idx,
-                                        h->t_x, h->t_y, b.gather_rows, b.gather_cols, g, h->st);
+                                        h->t_x, h->t_y, g, h->st);
     }));
   } else {
     const size_t cbn = (size_t)g.nj * (g.nu + 3) * g.pc;
@@ -1770,8 +1795,8 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
     b.rcr = rc_dir<double>(h->tr, 2);
     const char *da = std::getenv("VLS_DRIFT_ADJ");
     b.gather = !(da && std::string(da) == "atomic");
-    if (const char *gr = std::getenv("VLS_ADJ_GATHER_R")) b.gather_rows = std::atoi(gr);
-    if (const char *gq = std::getenv("VLS_ADJ_GATHER_Q")) b.gather_cols = std::atoi(gq);
+    const char *pp = std::getenv("VLS_ADJ_GATHER_PERM");
+    b.perm = sizeof(T) == 4 && !(pp && std::string(pp) == "0");
     const char *mp = std::getenv("VLS_ADJ_MOMENT");
     b.lazy_moment = !(mp && std::string(mp) == "pass");
     // the inverse map's ids hold u in 15 bits

@@ -180,15 +180,25 @@ cudaError_t launch_chain_adj(const double *lam, const double *mB, const MomentTa
                              double *ringb, double *tv, const int64_t *ch_cell,
                              const int64_t *ch_start, const int32_t *ch_len, int64_t nch,
                              int64_t ndrift, const Geometry &g, cudaStream_t st);
-// rows x cols C nodes per thread (8 x 2 by default; 8 x 1, 4 x 2)
+// cell-ordered gather (FP64 handles; 8 x 2 C nodes per thread)
 template <typename T>
 cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const MomentTables &mt,
                                     const double *tv, double *Cb, const uint32_t *ends,
                                     const uint32_t *ent, const int64_t *ebase, const T *fx,
                                     const T *fy, const int32_t *idx, const uint2 *fp2,
                                     const uint2 *far_w, const int32_t *t_idx, const double *t_x,
-                                    const double *t_y, int rows, int cols, const Geometry &g,
-                                    cudaStream_t st);
+                                    const double *t_y, const Geometry &g, cudaStream_t st);
+// entry-ordered form (FP32 handles): packed words of the entries once per
+// map, values permuted into entry order each step, gather
+cudaError_t launch_inv_geo(const uint32_t *ent, const int64_t *ebase, const uint2 *fp2,
+                           const uint2 *far_w, uint2 *geo, const Geometry &g, cudaStream_t st);
+cudaError_t launch_inv_perm(const uint32_t *ent, const int64_t *ebase, const double *lam,
+                            const double *mB, const MomentTables &mt, const double *tv,
+                            double *vperm, const Geometry &g, cudaStream_t st);
+cudaError_t launch_drift_adj_gather_perm(const double *vperm, const uint2 *geo, double *Cb,
+                                         const uint32_t *ends, const int64_t *ebase,
+                                         const int32_t *t_idx, const double *t_x,
+                                         const double *t_y, const Geometry &g, cudaStream_t st);
 cudaError_t launch_prer_adj(const double *Cb, double *Gb, const Geometry &g,
                             const DirTables &tr, cudaStream_t st);
 template <typename T>
