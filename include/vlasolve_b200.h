@@ -33,7 +33,12 @@ enum {
   VLS_OK = 0,
   VLS_EINVAL = 1, /* invalid argument or configuration */
   VLS_ECUDA = 2,  /* CUDA runtime error, or the CUDA path is unavailable */
-  VLS_ENAN = 3,   /* non-finite value detected in the grid */
+  VLS_ENAN = 3,   /* non-finite value detected: in a grid loaded from the
+                     host (vls_set_f, vls_read_ndfield, vls_read_restart; the
+                     grid is loaded all the same), in chain values
+                     (vls_set_chain_values), in an adjoint seed, or by a
+                     step's enclosed-mass scan (reported by the next call that
+                     waits for the device, e.g. vls_sync) */
   VLS_EIO = 4,    /* file format / I/O error */
   VLS_ENOMEM = 5, /* device or host allocation failed */
   VLS_ESTATE = 6  /* call out of order (e.g. step before initialisation) */
@@ -108,6 +113,46 @@ int vls_device_ok(int32_t device);
    device buffer of the handle. */
 int vls_create(const vls_grid_desc *grid, const vls_solver_desc *solver,
                vls_handle **out);
+/* Kernel layouts of a handle (no counterpart in the reference, whose step has
+   one CPU code path).  A zero-initialised descriptor, or NULL, selects the
+   defaults, which vls_create uses; the other values serve tests and
+   measurements and never change the arithmetic beyond FP rounding order.
+     prefilter         VLS_PREFILTER_AUTO: register-resident chunked solves
+                       where a line fits them, else shared-memory segments;
+                       VLS_PREFILTER_SEGMENT: segments for every line.
+     drift             VLS_DRIFT_AUTO: FP32 storage stages each block's whole
+                       coefficient strip (two blocks per SM where they fit,
+                       else one block of 32 warps), FP64 storage and strips
+                       too tall for one block take staged 64 x 40 windows;
+                       VLS_DRIFT_WINDOW / _STRIP2 / _STRIP1 ask for one of
+                       those (a strip that does not fit falls back to windows).
+     slices_per_batch  J slices per batch of the prefilter and drift scratch
+                       (0: all slices in one batch); the G and C scratch
+                       holds streams x slices_per_batch slices.
+     streams           batches run on this many streams, each with its own
+                       scratch slot (0 or 1: one stream).
+     drift_wait_spins  polls of each bounded wait of the drift for its staged
+                       coefficients (0: the default, about 2^20; < 0: none,
+                       every such wait gives up at once, which sends every
+                       cell to the gather from global memory and makes
+                       vls_sync report VLS_ECUDA: a test of the timeout path).
+   vls_get_layout reports what a handle uses: prefilter REGISTER or SEGMENT
+   and the chunk length of each direction (0 for segments), the drift kind,
+   the batch size and stream count, and the wait limit. */
+enum { VLS_PREFILTER_AUTO = 0, VLS_PREFILTER_REGISTER = 1, VLS_PREFILTER_SEGMENT = 2 };
+enum { VLS_DRIFT_AUTO = 0, VLS_DRIFT_WINDOW = 1, VLS_DRIFT_STRIP2 = 2, VLS_DRIFT_STRIP1 = 3 };
+typedef struct {
+  int32_t prefilter;
+  int32_t drift;
+  int32_t slices_per_batch;
+  int32_t streams;
+  int32_t drift_wait_spins;
+  int32_t u_chunk_rows; /* reported by vls_get_layout; ignored on input */
+  int32_t r_chunk_rows; /* reported by vls_get_layout; ignored on input */
+} vls_layout_desc;
+int vls_create_layout(const vls_grid_desc *grid, const vls_solver_desc *solver,
+                      const vls_layout_desc *layout, vls_handle **out);
+int vls_get_layout(const vls_handle *h, vls_layout_desc *used);
 /* ~vlasovSolver21_spline: frees the handle and all its device memory */
 int vls_destroy(vls_handle *h);
 /* message of the last failed call on h (or of the last vls_create failure
@@ -286,8 +331,11 @@ int vls_adjoint_inner_used(vls_handle *h, int32_t *inner_every);
    rejected with VLS_EINVAL.  That array is shared by every call, so calls that
    overlap on the GPU race and must be serialised by the caller; the first
    call on a device looks up the array's device address with that device
-   current, so it should come before any stream capture on that device.
-   Errors are reported by vls_noalloc_last_error(). */
+   current, so it should come before any stream capture on that device (after
+   cudaDeviceReset the next call looks it up again).  Every call copies R, U,
+   J and JV from host memory with cudaMemcpyAsync on `stream`.  Errors are
+   reported by vls_noalloc_last_error(), which returns the message of the
+   calling host thread's last failed call. */
 int vls_radial_mass_noalloc(const void *f_dev, int32_t precision, int64_t nr,
                             int64_t nu, int64_t nj, const double *R,
                             const double *U, const double *J, const double *JV,

@@ -14,6 +14,10 @@
 #      (vlasovSolver21.hxx) becomes strcat, so snapshot files get their names;
 #   4. built with _FORTIFY_SOURCE off, because myIO::writeTag writes one byte
 #      past its tag buffer (strcpy of the terminating NUL).
+#
+# The reference tree is taken from VLS_REFERENCE_DIR; unset, the recipe looks
+# in the read-only checkout of this build machine.  Without the tree it
+# builds nothing and exits 0 (a machine that only runs prebuilt files).
 set -euo pipefail
 REF=${VLS_REFERENCE_DIR:-/root/reference}
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"

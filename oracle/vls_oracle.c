@@ -25,6 +25,7 @@ struct vlo_ctx {
   /* spline constants, localSpline.hxx:60-93 */
   double sstart[2], sstep_inv[2];
   double kernelRadius;
+  long halted_cell; /* first cell where the reference would halt, or -1 */
   /* init-profile constants */
   double rho0, sig0, C0, C1, C2, sigR2, sigO2, Vg;
   /* state */
@@ -180,8 +181,10 @@ static double profile_value(const vlo_ctx *c, double r, double u, double j) {
 
 /* vlasovSolver21::advanceParticleDrift, vlasovSolver21.hxx:328-408 */
 static void advance_particle_drift(double R, double U, double J, double dt,
-                                   double R0, double *outR, double *outU) {
+                                   double R0, double *outR, double *outU,
+                                   int *halted) {
   double H0, newU, newR, tlim, tR0, sgn, deltaT;
+  if (halted) *halted = 0;
   H0 = 0.5 * (U * U + (J * J) / (R * R));
   sgn = (U <= 0) ? -1 : 1;
   deltaT = dt;
@@ -229,8 +232,11 @@ static void advance_particle_drift(double R, double U, double J, double dt,
     deltaT -= tlim;
     tR0 -= tlim;
     tlim = 10 * dt;
-    /* the reference exits the process on tR0<deltaT here (:389-391); that
-       branch is unreachable after the reflection update above */
+    /* the reference prints and exits the process on tR0<deltaT here
+       (:389-391).  Reached with a reflection radius R0 > 0 only, by cells
+       inside R0 (reflective kernel, kernelBufferSize > 0); *halted reports
+       it and vlo_create then fails, as the reference run ends there */
+    if (tR0 < deltaT && halted) *halted = 1;
   }
   newR = sqrt(pow(fabs(newR * newU) - 2 * sgn * H0 * deltaT, 2) + J * J) *
          pow(2 * H0, -0.5);
@@ -272,7 +278,9 @@ static void generate_displacement(vlo_ctx *c, double dt, int reflective) {
       for (r = 0; r < c->nr; r++) {
         long i = (j * c->nu + u) * c->nr + r;
         double dR, dU;
-        advance_particle_drift(c->R[r], c->U[u], J, dth, R0, &dR, &dU);
+        int halted = 0;
+        advance_particle_drift(c->R[r], c->U[u], J, dth, R0, &dR, &dU, &halted);
+        if (halted && c->halted_cell < 0) c->halted_cell = i;
         c->driftR[i] = dR;
         c->driftU[i] = dU;
         c->driftOut[i] = ((dR >= c->R[c->nr - 1]) || (dR <= c->R[0]) ||
@@ -331,11 +339,11 @@ static int setup_chains(vlo_ctx *c, double dt) {
         c->cell2ch[i] = c->nch;
         c->nch++;
         deltaT = dth;
-        advance_particle_drift(c->R[r], c->U[u], J, deltaT, -1, &nR, &nU);
+        advance_particle_drift(c->R[r], c->U[u], J, deltaT, -1, &nR, &nU, NULL);
         while (nR < c->kernelRadius) {
           chain_push(c, nR, nU, profile_value(c, nR, nU, J));
           deltaT += dth;
-          advance_particle_drift(c->R[r], c->U[u], J, deltaT, -1, &nR, &nU);
+          advance_particle_drift(c->R[r], c->U[u], J, deltaT, -1, &nR, &nU, NULL);
         }
         chain_push(c, nR, nU, 0.0);
       }
@@ -790,7 +798,13 @@ vlo_ctx *vlo_create(const vlo_params *p) {
 
   {
     double dtd = p->noLinking ? p->dt : p->dt * 2;
+    c->halted_cell = -1;
     generate_displacement(c, dtd, p->kernelType == VLO_REFLECTIVE);
+    if (c->halted_cell >= 0) {
+      /* the reference terminates in generateDisplacement for this set-up */
+      vlo_destroy(c);
+      return NULL;
+    }
     setup_chains(c, dtd);
   }
   /* renormalize(init->getMass(0), 0) */

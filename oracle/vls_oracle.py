@@ -123,12 +123,21 @@ def make_params(cfg: dict) -> _Params:
     return p
 
 
+class ReferenceHalt(RuntimeError):
+    """The reference run ends during set-up for this configuration."""
+
+
 class Oracle:
     """One oracle solver instance (FP64 CPU restatement of the reference)."""
 
     def __init__(self, cfg: dict):
         self._p = make_params(cfg)
         self._c = lib().vlo_create(ctypes.byref(self._p))
+        if not self._c:
+            # advanceParticleDrift reached the branch where the reference
+            # prints and exits (vlasovSolver21.hxx:389-391)
+            raise ReferenceHalt("the reference terminates in generateDisplacement "
+                                "for this set-up (vlasovSolver21.hxx:389-391)")
         nr, nu, nj = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
         lib().vlo_dims(self._c, ctypes.byref(nr), ctypes.byref(nu), ctypes.byref(nj))
         self.nr, self.nu, self.nj = nr.value, nu.value, nj.value

@@ -12,7 +12,8 @@ order) and records:
 * the ``statistics.txt`` rows;
 * the delayed-kernel chains (cell, R, U, values) from the restart file written
   at step 0 and from the final restart file;
-* two .vls restart files of the smallest case, byte for byte (``restart``).
+* two .vls restart files of the smallest case, byte for byte (``restart``);
+* one NDfield snapshot of the smallest case, byte for byte (``ndfield``).
 
 Usage:  python tests/golden/make_golden.py [case ...]
 """
@@ -70,7 +71,19 @@ CASES = [
     case("plummer_linr", ["-init.type", "Plummer"]
          + _grid(20, 16, 8, 0.05, 20, -3, 3, 0, 2, pscale="linear"),
          4, [0, 1, 4], dt=0.01),
-    # BASELINE configurations at their full sizes (sampled)
+    # reflective kernel (kernelType reflective): footpoints that cross the
+    # kernel radius R_Val[0] are reflected there (vlasovSolver21.hxx:343-377,
+    # :434); with kernelBufferSize > 0 the reference terminates during set-up
+    # (:389-391), so the radius stays at the first vertex
+    case("udf_reflect", ["-init.type", "UDF", "-solver.kernelType", "reflective"]
+         + _grid(20, 18, 6, 0.01, 25, -2, 2, 0, 1.6), 4, [0, 1, 4], dt=0.02),
+    # lines of 1025 vertices along r and along v_r (the layouts the
+    # 1024 x 1024 x 512 PLDF configuration takes), three J slices (sampled)
+    case("pldf_1025", ["-init.type", "PLDF", "-init.alpha", "1", "-init.eta", "0.1",
+                       "-init.n", "1", "-init.smoothingRadius", "0.5"]
+         + _grid(1024, 1024, 3, 0.01, 200, -3, 3, 0, 1.6), 2, [0, 1, 2], full_f=False,
+         dt=0.005),
+    # the north-star configurations at their full sizes (sampled)
     case("udf_cfg1", ["-init.type", "UDF"] + _grid(200, 200, 200, 0.01, 25, -2, 2, 0, 1.6),
          10, [0, 1, 10], full_f=False, dt=0.005),
     case("plummer_cfg2", ["-init.type", "Plummer"] + _grid(256, 256, 128, 0.01, 25, -3, 3, 0, 2),
@@ -216,11 +229,33 @@ def make_restart_fixtures():
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+# an NDfield snapshot written by the reference (Save_NDfield, NDfield.hxx:308-363),
+# kept byte for byte: the udf_tiny case after one step
+NDFIELD_FILE = ("snapshot_0.0050.ND", "udf_tiny_snapshot_step1.ND")
+
+
+def make_ndfield_fixture():
+    tmp = tempfile.mkdtemp(prefix="vls_golden_")
+    try:
+        c = CASES[0]
+        args = [REF_BIN, "-threads_per_node", "1", "-verbose", "0"] + c["args"] + [
+            "-solver.dt", "0.005", "-solver.Tmax", "0.005", "-solver.restartEvery", "100000",
+            "-solver.statsEvery", "-1", "-solver.snapshotEvery", "1"]
+        with open(os.path.join(tmp, "log.txt"), "w") as log:
+            subprocess.check_call(args, cwd=tmp, stdout=log, stderr=subprocess.STDOUT)
+        shutil.copyfile(os.path.join(tmp, NDFIELD_FILE[0]), os.path.join(HERE, NDFIELD_FILE[1]))
+        return "ndfield", "ok"
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main(names):
     if not os.path.exists(REF_BIN):
         sys.exit("reference binary missing: run oracle/build_ref.sh first")
     if not names or "restart" in names:
         print(*make_restart_fixtures(), flush=True)
+    if not names or "ndfield" in names:
+        print(*make_ndfield_fixture(), flush=True)
     todo = [c for c in CASES if not names or c["name"] in names]
     if not todo:
         return

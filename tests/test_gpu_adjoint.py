@@ -163,129 +163,143 @@ def test_reinitialising_a_stepped_handle_restores_the_initial_state():
     np.testing.assert_array_equal(s.f, fresh.f)
 
 
-def test_far_cell_layout_keeps_the_adjoint(monkeypatch):
-    """With the far-cell pass (packed words FP_FAR + list index) the drift's
-    transpose reads the original footpoints from the far list."""
-    p_ref = problem("fp32")
-    target = p_ref.run(THETA + DTHETA)
-    _, g_ref = loss_and_grad(p_ref, target)
-    monkeypatch.setenv("VLS_FAR", "1")
-    p = problem("fp32")
-    _, g = loss_and_grad(p, target)
-    np.testing.assert_allclose(g, g_ref, rtol=1e-6)
-
-
-@pytest.mark.parametrize("layout", ["long", "short"])
-def test_other_adjoint_line_layouts_keep_the_gradient(layout, monkeypatch):
-    """The chunk layouts the transposed solves take besides the default ones:
-    the r layout of lines too long for the default (1025 rows), forced here
-    on short lines ("long"), and the 16-line u layout ("short")."""
-    p_ref = problem("fp64")
-    target = p_ref.run(THETA + DTHETA)
-    _, g_ref = loss_and_grad(p_ref, target)
-    monkeypatch.setenv("VLS_ADJ_RC", layout)
-    for prec in ("fp64", "fp32"):
-        p = problem(prec)
-        _, g = loss_and_grad(p, target)
-        if prec == "fp64":
-            np.testing.assert_allclose(g, g_ref, rtol=1e-10)
-        else:
-            assert np.all(np.abs(g - g_ref) <= FP32_RTOL * np.max(np.abs(g_ref)))
-
-
-def test_chunked_adjoint_lines_match_one_thread_per_line(monkeypatch):
+def test_chunked_adjoint_lines_match_one_thread_per_line():
     """The chunked-register transposed solves against the one-thread-per-line
-    kernels (VLS_PREFILTER=segment selects those for both directions)."""
+    kernels (the segment prefilter layout selects those for both
+    directions)."""
     p_ref = problem("fp64")
     target = p_ref.run(THETA + DTHETA)
     _, g_ref = loss_and_grad(p_ref, target)
-    monkeypatch.setenv("VLS_PREFILTER", "segment")
-    p = problem("fp64")
+    from vlasolve_b200.adjoint import DensityProblem
+    p = DensityProblem(cfg(), precision="fp64", nsteps=12, checkpoint_every=5,
+                       layout={"prefilter": "segment"})
+    assert p.solver.layout()["prefilter"] == "segment"
     _, g = loss_and_grad(p, target)
     np.testing.assert_allclose(g, g_ref, rtol=1e-10)
 
 
-def _solver_backward(precision, env, monkeypatch, far=False):
+def _kbuf_solver(precision):
+    """A small grid with delayed-kernel chains (kernel radius at the third r
+    vertex) and footpoints far enough to leave the drift strips."""
     from vlasolve_b200 import VlasovSolver21Spline
-    if far:
-        monkeypatch.setenv("VLS_FAR", "1")
-    s = VlasovSolver21Spline(cfg(pres=40, ures=(28, 10)), precision=precision)
+    c = dict(cfg(pres=40, ures=(28, 10)), kernelBufferSize=2)
+    return VlasovSolver21Spline(c, precision=precision)
+
+
+def _loss(s, f, chv, nsteps, dbins):
+    """L = <dbins, bins(f_N)>: the radial bins after nsteps steps from (f, chv)."""
+    s.f = f
+    s.set_chain_values(chv)
+    s.step(nsteps)
+    return float(np.dot(dbins, s.moments()[0]))
+
+
+def test_adjoint_random_directions_match_central_differences():
+    """Cell by cell rather than through three parameters: for seeded random
+    directions v over the initial grid and w over the initial chain values,
+    <dL/df0, v> + <dL/dchain0, w> equals the central difference
+    (L(f0 + h v, c0 + h w) - L(f0 - h v, c0 - h w)) / 2h of FP64 forward runs
+    (h = 1e-5), to 1e-6 relative.  The grid has chains, so the ring buffers'
+    transposes and the chain tails' gathers enter every direction."""
+    nsteps, K = 7, 3
+    s = _kbuf_solver("fp64")
+    f0, c0 = s.f, s.chains()["val"].copy()
+    assert len(c0) > 0
+    rng = np.random.default_rng(20261203)
+    dbins = rng.standard_normal(s.nr)
+    s.f = f0
+    s.set_chain_values(c0)
+    s.adjoint_forward(nsteps, K)
+    df0, dch = s.adjoint_backward(dbins)
+    df0 = np.asarray(df0).reshape(f0.shape)
+    h = 1e-5
+    for trial in range(3):
+        v = f0 * rng.standard_normal(f0.shape)
+        w = c0 * rng.standard_normal(c0.shape)
+        pred = float(np.sum(df0 * v) + np.dot(dch, w))
+        Lp = _loss(s, f0 + h * v, c0 + h * w, nsteps, dbins)
+        Lm = _loss(s, f0 - h * v, c0 - h * w, nsteps, dbins)
+        fd = (Lp - Lm) / (2 * h)
+        print(f"direction {trial}: adjoint {pred:.12e} fd {fd:.12e}")
+        assert abs(pred - fd) <= 1e-6 * abs(fd), (trial, pred, fd)
+    # the chain part alone, so that a wrong ring transpose cannot hide behind
+    # the much larger grid part
+    w = c0 * rng.standard_normal(c0.shape)
+    pred = float(np.dot(dch, w))
+    fd = (_loss(s, f0, c0 + h * w, nsteps, dbins) - _loss(s, f0, c0 - h * w, nsteps, dbins)) / (2 * h)
+    print(f"chains only: adjoint {pred:.12e} fd {fd:.12e}")
+    assert abs(pred - fd) <= 1e-6 * abs(fd), (pred, fd)
+
+
+def test_fp32_adjoint_matches_fp64_adjoint_cell_by_cell():
+    """The FP32-storage handle's transposed step (the entry-ordered gather)
+    against the FP64 handle's (the cell-ordered gather) on every cell of
+    dL/df0 and every chain element: the two differ only by the FP32 rounding
+    of the forward states they linearise around."""
+    out = []
+    for prec in ("fp64", "fp32"):
+        s = _kbuf_solver(prec)
+        s.adjoint_forward(7, 3)
+        dbins = np.cos(0.3 * np.arange(s.nr, dtype=np.float64))
+        df0, dch = s.adjoint_backward(dbins)
+        out.append((np.asarray(df0).ravel().copy(), dch.copy()))
+    (a0, ac), (b0, bc) = out
+    assert np.max(np.abs(a0)) > 0 and ac.size > 0
+    assert np.max(np.abs(b0 - a0)) <= 1e-4 * np.max(np.abs(a0))
+    assert np.max(np.abs(bc - ac)) <= 1e-4 * max(np.max(np.abs(ac)), 1e-300)
+
+
+def _backward_twice(precision):
+    s = _kbuf_solver(precision)
     s.adjoint_forward(7, 3)
     dbins = np.cos(0.3 * np.arange(s.nr, dtype=np.float64))
     out = []
-    for mode in env:
-        if mode:
-            monkeypatch.setenv("VLS_DRIFT_ADJ", mode)
-        else:
-            monkeypatch.delenv("VLS_DRIFT_ADJ", raising=False)
+    for _ in range(2):
         df0, dch = s.adjoint_backward(dbins)
-        out.append((df0.copy(), dch.copy()))
+        out.append((np.asarray(df0).copy(), dch.copy()))
     return out
 
 
-@pytest.mark.parametrize("precision,far", [("fp64", False), ("fp32", False), ("fp32", True)])
-def test_gather_drift_transpose_matches_atomic_scatter(precision, far, monkeypatch):
-    """The drift transposed as a gather over the inverse footpoint map against
-    the scatter with FP64 atomics: the same sums in another order, on every
-    cell of dL/df0 and every ring slot of dL/d(chains)."""
-    (g0, gc), (a0, ac) = _solver_backward(precision, ["", "atomic"], monkeypatch, far)
-    assert np.max(np.abs(a0)) > 0
-    np.testing.assert_allclose(g0, a0, rtol=1e-11, atol=1e-13 * np.max(np.abs(a0)))
-    assert gc.size == ac.size and gc.size > 0
-    np.testing.assert_allclose(gc, ac, rtol=1e-11, atol=1e-13 * max(np.max(np.abs(ac)), 1e-300))
-
-
-def test_gather_drift_transpose_is_deterministic(monkeypatch):
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gather_drift_transpose_is_deterministic(precision):
     """Two backward passes through the gather give the same bits."""
-    (a0, ac), (b0, bc) = _solver_backward("fp32", ["", ""], monkeypatch)
+    (a0, ac), (b0, bc) = _backward_twice(precision)
     np.testing.assert_array_equal(a0, b0)
     np.testing.assert_array_equal(ac, bc)
 
 
-def test_inverse_map_follows_new_footpoints(monkeypatch):
-    """vls_set_footpoints after a backward pass: the next gather uses the
-    inverse map of the new footpoints (base columns moved by one), checked
-    against the atomic scatter, which reads the footpoints directly."""
+def _set_footpoints(s, fp, rI):
     import ctypes
-    from vlasolve_b200 import VlasovSolver21Spline
-    s = VlasovSolver21Spline(cfg(pres=40, ures=(28, 10)), precision="fp32")
-    dbins = np.cos(0.3 * np.arange(s.nr, dtype=np.float64))
-    s.adjoint_forward(4, 2)
-    monkeypatch.delenv("VLS_DRIFT_ADJ", raising=False)
-    s.adjoint_backward(dbins)
-    fp = s.footpoints()
-    rI = fp["rI"].copy()
-    move = (fp["out"] == 0) & (rI >= 1)
-    rI[move] -= 1
     i32, u8 = ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint8)
     d = ctypes.POINTER(ctypes.c_double)
     assert s._L.vls_set_footpoints(
         s._h, rI.ctypes.data_as(i32), fp["rF"].ctypes.data_as(d),
         fp["uI"].ctypes.data_as(i32), fp["uF"].ctypes.data_as(d),
         fp["out"].ctypes.data_as(u8), fp["driftR"].ctypes.data_as(d)) == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_inverse_map_follows_new_footpoints(precision):
+    """vls_set_footpoints after a backward pass: the next gather uses the
+    inverse map of the new footpoints (base columns moved by one), as a
+    handle that never saw the old footpoints does."""
+    dbins = np.cos(0.3 * np.arange(41, dtype=np.float64))
+    s = _kbuf_solver(precision)
+    f0, c0 = s.f, s.chains()["val"].copy()
+    s.adjoint_forward(4, 2)
+    s.adjoint_backward(dbins)
+    fp = s.footpoints()
+    rI = fp["rI"].copy()
+    move = (fp["out"] == 0) & (rI >= 1)
+    rI[move] -= 1
+    _set_footpoints(s, fp, rI)
+    s.f = f0
+    s.set_chain_values(c0)
     s.adjoint_forward(4, 2)
     g0, gc = s.adjoint_backward(dbins)
-    monkeypatch.setenv("VLS_DRIFT_ADJ", "atomic")
-    a0, ac = s.adjoint_backward(dbins)
-    np.testing.assert_allclose(g0, a0, rtol=1e-11, atol=1e-13 * np.max(np.abs(a0)))
-    np.testing.assert_allclose(gc, ac, rtol=1e-11, atol=1e-13 * max(np.max(np.abs(ac)), 1e-300))
-
-
-@pytest.mark.parametrize("far", [False, True])
-def test_entry_ordered_gather_matches_cell_ordered_gather(far, monkeypatch):
-    """FP32 handles: the gather over entry-ordered values and packed words
-    against the gather that reads lam and the footpoints through each
-    entry's cell index (with the far-cell layout too)."""
-    from vlasolve_b200 import VlasovSolver21Spline
-    if far:
-        monkeypatch.setenv("VLS_FAR", "1")
-    s = VlasovSolver21Spline(cfg(pres=40, ures=(28, 10)), precision="fp32")
-    s.adjoint_forward(7, 3)
-    dbins = np.cos(0.3 * np.arange(s.nr, dtype=np.float64))
-    monkeypatch.delenv("VLS_DRIFT_ADJ", raising=False)
-    monkeypatch.setenv("VLS_ADJ_GATHER_PERM", "0")
-    a0, ac = s.adjoint_backward(dbins)
-    monkeypatch.setenv("VLS_ADJ_GATHER_PERM", "1")
-    p0, pc = s.adjoint_backward(dbins)
-    np.testing.assert_allclose(p0, a0, rtol=1e-13, atol=1e-15 * np.max(np.abs(a0)))
-    np.testing.assert_allclose(pc, ac, rtol=1e-13, atol=1e-15 * max(np.max(np.abs(ac)), 1e-300))
+    t = _kbuf_solver(precision)
+    _set_footpoints(t, fp, rI)
+    t.adjoint_forward(4, 2)
+    a0, ac = t.adjoint_backward(dbins)
+    assert np.max(np.abs(np.asarray(g0) - np.asarray(a0))) == 0.0
+    np.testing.assert_array_equal(gc, ac)

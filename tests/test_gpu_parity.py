@@ -148,8 +148,11 @@ def test_full_config_fp64_sampled(name):
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp32all"])
-def test_full_config_fp32_hernquist_sampled(prec):
-    g, cfg = load_golden("hernquist_cfg3")
+@pytest.mark.parametrize("name", LARGE)
+def test_full_config_fp32_sampled(name, prec):
+    """Every full-size configuration (the 1025-vertex r and v_r lines of
+    pldf_1025 included) in both FP32 modes, with the default kernel layouts."""
+    g, cfg = load_golden(name)
     s = solver(cfg, prec)
     idx = g["sample_idx"]
     cur = 0
@@ -159,7 +162,7 @@ def test_full_config_fp32_hernquist_sampled(prec):
         fs = s.f.ravel()[idx]
         ref = g["fs_%d" % st]
         err = np.abs(fs - ref).max() / np.abs(ref).max()
-        print(f"hernquist_cfg3 {prec} step {st}: max rel err {err:.3e}")
+        print(f"{name} {prec} step {st}: max rel err {err:.3e}")
         assert err <= FP32_MAX, st
 
 
@@ -202,6 +205,93 @@ def test_ndfield_roundtrip_and_layout():
         np.testing.assert_array_equal(s2.f, f)
 
 
+def test_ndfield_writer_matches_reference_file_bytes():
+    """The reference's own snapshot of udf_tiny after one step
+    (tests/golden/udf_tiny_snapshot_step1.ND): read into a handle, written back
+    by vls_write_ndfield, the two files are identical byte for byte."""
+    ref_path = os.path.join(os.path.dirname(__file__), "golden", "udf_tiny_snapshot_step1.ND")
+    ref = open(ref_path, "rb").read()
+    g, cfg = load_golden("udf_tiny")
+    s = solver(cfg)
+    s.load_snapshot(ref_path)
+    np.testing.assert_array_equal(s.f, g["f_1"])
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "snap.ND")
+        s.snapshot(p)
+        assert open(p, "rb").read() == ref
+
+
+def test_ndfield_record_marker_above_2gib():
+    """1025 x 1025 x 256 cells: 2.15 GB of FP64 data, whose int record marker
+    wraps exactly as the reference's (NDfield.hxx:355); the file reads back."""
+    import struct
+    cfg = {"type": "Hernquist", "Pmin": 0.01, "Pmax": 50.0, "Pres": 1024,
+           "Pscale": "logarithmic", "Umin": (-3.0, 0.0), "Umax": (3.0, 3.0),
+           "Ures": (1024, 256), "Uscale": ("linear", "quadratic"), "dt": 0.0025}
+    s = solver(cfg, "fp32")
+    n = 1025 * 1025 * 256
+    wrapped = struct.unpack("<i", struct.pack("<I", (8 * n) % 2 ** 32))[0]
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "big.ND")
+        s.snapshot(p)
+        assert os.path.getsize(p) == 688 + 8 * n + 4
+        with open(p, "rb") as fh:
+            fh.seek(684)
+            assert struct.unpack("<i", fh.read(4))[0] == wrapped
+            fh.seek(688 + 8 * n)
+            assert struct.unpack("<i", fh.read(4))[0] == wrapped
+            fh.seek(688 + 8 * (n - 3))
+            tail = np.frombuffer(fh.read(24), "<f8")
+        f = s.f
+        np.testing.assert_array_equal(tail, f.ravel()[-3:])
+        s.f = np.zeros_like(f)
+        s.load_snapshot(p)
+        np.testing.assert_array_equal(s.f, f)
+
+
+def test_reflective_kernel_where_the_reference_halts_is_an_error():
+    """kernelBufferSize > 0 with the reflective kernel reaches the branch
+    where the reference terminates (vlasovSolver21.hxx:389-391); vls_create
+    returns VLS_EINVAL naming it instead."""
+    from vlasolve_b200 import _lib
+    g, cfg = load_golden("udf_reflect")
+    with pytest.raises(_lib.VlsError) as e:
+        solver(cfg, kernelBufferSize=2)
+    assert e.value.code == _lib.VLS_EINVAL
+    assert "reflect" in str(e.value)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_nonfinite_grid_is_reported(prec):
+    """A NaN placed in the host grid: vls_set_f loads it and returns VLS_ENAN;
+    a step from that state is reported by the enclosed-mass scan at the next
+    vls_sync; a clean grid clears the state; an infinity in the chain values
+    is reported by vls_set_chain_values."""
+    from vlasolve_b200 import _lib
+    g, cfg = load_golden("udf_rect_kbuf")
+    s = solver(cfg, prec)
+    f = s.f
+    bad = f.copy()
+    bad[2, 5, 7] = np.nan
+    with pytest.raises(_lib.VlsError) as e:
+        s.f = bad
+    assert e.value.code == _lib.VLS_ENAN
+    s.step(1)
+    with pytest.raises(_lib.VlsError) as e:
+        s.sync()
+    assert e.value.code == _lib.VLS_ENAN
+    assert "total mass" in str(e.value)
+    s.f = f  # clean again
+    s.step(1)
+    s.sync()
+    ch = s.chains()["val"].copy()
+    assert len(ch) > 0
+    ch[0] = np.inf
+    with pytest.raises(_lib.VlsError) as e:
+        s.set_chain_values(ch)
+    assert e.value.code == _lib.VLS_ENAN
+
+
 def test_bad_inputs_report_errors():
     from vlasolve_b200 import _lib
     g, cfg = load_golden("udf_tiny")
@@ -215,16 +305,60 @@ def test_bad_inputs_report_errors():
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 @pytest.mark.parametrize("name", ["udf_tiny", "udf_rect_kbuf", "udf_nolink"])
-def test_slice_batches_on_streams_are_bit_identical(name, prec, monkeypatch):
+def test_slice_batches_on_streams_are_bit_identical(name, prec):
     """Splitting the J slices into batches on several streams (each with its
     own scratch slot) changes no arithmetic: the grid after several steps is
     bit-identical to the single-batch run."""
+    from vlasolve_b200 import VlasovSolver21Spline
     g, cfg = load_golden(name)
     a = solver(cfg, prec)
-    monkeypatch.setenv("VLS_BATCH", "3")
-    monkeypatch.setenv("VLS_STREAMS", "2")
-    b = solver(cfg, prec)
+    b = VlasovSolver21Spline(cfg, precision=prec, layout={"slices_per_batch": 3, "streams": 2})
+    assert b.layout()["slices_per_batch"] == 3 and b.layout()["streams"] == 2
     a.step(4)
     b.step(4)
     np.testing.assert_array_equal(a.f, b.f)
     np.testing.assert_array_equal(a.chains()["val"], b.chains()["val"])
+
+
+@pytest.mark.parametrize("prec,drift", [("fp64", "window"), ("fp32", "window"),
+                                        ("fp32", "strip2"), ("fp32", "strip1")])
+def test_drift_wait_timeout_reports_and_falls_back(prec, drift):
+    """drift_wait_spins < 0: every bounded wait of the drift for its staged
+    coefficients gives up at once (the copies still land; the block's last
+    wait, before its shared memory is released, keeps the full limit).  The
+    step reports it (vls_sync returns VLS_ECUDA, naming the drift) and its
+    cells read C from global memory, so f still matches the reference."""
+    from vlasolve_b200 import VlasovSolver21Spline, _lib
+    g, cfg = load_golden("udf_rect_kbuf")
+    s = VlasovSolver21Spline(cfg, precision=prec,
+                             layout={"drift": drift, "drift_wait_spins": -1})
+    lay = s.layout()
+    assert lay["drift"] == drift and lay["drift_wait_spins"] == 0
+    cur = 0
+    for st in _saved_steps(g, "f_")[1:]:
+        s.step(st - cur)
+        cur = st
+        with pytest.raises(_lib.VlsError) as e:
+            s.sync()
+        assert e.value.code == _lib.VLS_ECUDA and "drift" in str(e.value)
+        ref = g["f_%d" % st]
+        d = s.f - ref
+        if prec == "fp64":
+            assert np.abs(d).max() <= FP64_TOL * np.abs(ref).max()
+        else:
+            assert np.linalg.norm(d) / np.linalg.norm(ref) <= FP32_L2
+    s.sync()  # the report cleared the flag; nothing ran since
+
+
+def test_default_layouts_of_the_1025_vertex_grid():
+    """The kernels the 1025 x 1025 lines take by default (the ones the
+    pldf_1025 parity tests run): 23-row chunks along both directions, the
+    one-block strip drift in FP32, the windowed drift in FP64."""
+    g, cfg = load_golden("pldf_1025")
+    a = solver(cfg, "fp32").layout()
+    assert a["prefilter"] == "register" and a["u_chunk_rows"] == 23 and a["r_chunk_rows"] == 23
+    assert a["drift"] == "strip1"
+    b = solver(cfg, "fp64").layout()
+    assert b["drift"] == "window" and b["u_chunk_rows"] == 23
+    c = solver(load_golden("hernquist_cfg3")[1], "fp32").layout()
+    assert c["drift"] == "strip2" and c["u_chunk_rows"] == 17 and c["r_chunk_rows"] == 19

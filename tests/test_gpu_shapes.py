@@ -2,7 +2,6 @@
 (one chunk, a last chunk of one row, exactly full chunks, odd sizes) and the
 drift's strip boxes against the oracle, for every prefilter / drift layout
 and all three precisions."""
-import os
 
 import numpy as np
 import pytest
@@ -34,34 +33,20 @@ def cfg_for(pres, ures0):
             "Ures": (ures0, 6), "Uscale": ("linear", "quadratic"), "dt": 0.02}
 
 
-# environment of each implementation choice: the defaults, the shared-memory
-# segment prefilter with the windowed drift, each register chunk layout, and
-# each whole-strip drift layout
+# layout of each kernel choice (vls_layout_desc): the defaults, the
+# shared-memory segment prefilter with the windowed drift, and each drift
+# kind forced (a strip that does not fit falls back to windows)
 IMPLS = {
-    "default": {},
-    "segment-window": {"VLS_PREFILTER": "segment", "VLS_DRIFT": "window"},
-    "rcA": {"VLS_RC": "A"},
-    "rcB": {"VLS_RC": "B"},
-    "rcC": {"VLS_RC": "C"},
-    "rcD": {"VLS_RC": "D"},
-    "rcF": {"VLS_RC": "F"},
-    "rcI": {"VLS_RC": "I"},
-    "strip48": {"VLS_DRIFT": "48"},
-    "strip64": {"VLS_DRIFT": "64"},
-    "strip-48": {"VLS_DRIFT": "-48"},
-    "strip-49": {"VLS_DRIFT": "-49"},
-    "strip50": {"VLS_DRIFT": "50"},
-    "strip51": {"VLS_DRIFT": "51"},
-    "far": {"VLS_FAR": "1"},
+    "default": None,
+    "segment-window": {"prefilter": "segment", "drift": "window"},
+    "window": {"drift": "window"},
+    "strip2": {"drift": "strip2"},
+    "strip1": {"drift": "strip1"},
 }
 
 
 @pytest.fixture(params=sorted(IMPLS))
-def impl(request, monkeypatch):
-    for k in ("VLS_PREFILTER", "VLS_DRIFT", "VLS_RC", "VLS_FAR"):
-        monkeypatch.delenv(k, raising=False)
-    for k, v in IMPLS[request.param].items():
-        monkeypatch.setenv(k, v)
+def impl(request):
     return request.param
 
 
@@ -70,7 +55,7 @@ def impl(request, monkeypatch):
 def test_shape_steps_match_oracle(shape, precision, impl):
     from vlasolve_b200 import VlasovSolver21Spline
     cfg = cfg_for(*shape)
-    s = VlasovSolver21Spline(cfg, precision=precision)
+    s = VlasovSolver21Spline(cfg, precision=precision, layout=IMPLS[impl])
     o = Oracle(cfg)
     for _ in range(3):
         s.step(1)

@@ -101,3 +101,15 @@ def test_planted_error_is_caught():
     o.f = f
     o.step(1)
     assert not np.array_equal(o.f, g["f_1"])
+
+
+def test_oracle_halts_where_the_reference_terminates():
+    """With the reflective kernel and kernelBufferSize > 0 the cells inside the
+    reflection radius reach the branch of advanceParticleDrift where the
+    reference prints and exits (vlasovSolver21.hxx:389-391; its run of this
+    set-up ends there).  The oracle refuses the set-up the same way."""
+    from oracle.vls_oracle import ReferenceHalt
+    g, cfg = load_golden("udf_reflect")
+    cfg = dict(cfg, kernelBufferSize=2)
+    with pytest.raises(ReferenceHalt):
+        Oracle(cfg)

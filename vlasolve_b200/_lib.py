@@ -22,7 +22,8 @@ PRECISIONS = {"fp64": 0, "fp32": 1, "fp32all": 2}
 
 # every symbol include/vlasolve_b200.h declares
 EXPORTED = [
-    "vls_version", "vls_device_ok", "vls_create", "vls_destroy", "vls_last_error",
+    "vls_version", "vls_device_ok", "vls_create", "vls_create_layout", "vls_get_layout",
+    "vls_destroy", "vls_last_error",
     "vls_dims", "vls_coords", "vls_init_profile", "vls_set_f", "vls_get_f",
     "vls_get_footpoints", "vls_set_footpoints", "vls_get_chains",
     "vls_set_chain_values", "vls_step", "vls_sync", "vls_kernel_launches",
@@ -57,6 +58,18 @@ class SolverDesc(ctypes.Structure):
                 ("noLinking", ctypes.c_int32), ("kernelType", ctypes.c_int32),
                 ("kernelBufferSize", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("device", ctypes.c_int32)]
+
+
+# vls_layout_desc: kernel layouts of a handle (zeroes = the defaults)
+PREFILTERS = {"auto": 0, "register": 1, "segment": 2}
+DRIFTS = {"auto": 0, "window": 1, "strip2": 2, "strip1": 3}
+
+
+class LayoutDesc(ctypes.Structure):
+    _fields_ = [("prefilter", ctypes.c_int32), ("drift", ctypes.c_int32),
+                ("slices_per_batch", ctypes.c_int32), ("streams", ctypes.c_int32),
+                ("drift_wait_spins", ctypes.c_int32), ("u_chunk_rows", ctypes.c_int32),
+                ("r_chunk_rows", ctypes.c_int32)]
 
 
 class InitDesc(ctypes.Structure):
@@ -95,6 +108,8 @@ def load(path: str = LIB_PATH):
         "vls_version": [P(i32), P(i32)],
         "vls_device_ok": [i32],
         "vls_create": [P(GridDesc), P(SolverDesc), P(H)],
+        "vls_create_layout": [P(GridDesc), P(SolverDesc), P(LayoutDesc), P(H)],
+        "vls_get_layout": [H, P(LayoutDesc)],
         "vls_destroy": [H],
         "vls_dims": [H, P(i64), P(i64), P(i64)],
         "vls_coords": [H, P(d), P(d), P(d), P(d)],

@@ -29,8 +29,10 @@ class DensityProblem:
 
     def __init__(self, cfg, precision: str = "fp64", nsteps: int = 1,
                  checkpoint_every: int = 1, params=("R0", "alpha", "smoothingRadius"),
-                 ic_step: float = 1e-6, device: int = 0, inner_every: int = 0):
-        self.solver = VlasovSolver21Spline(cfg, precision=precision, device=device, init=False)
+                 ic_step: float = 1e-6, device: int = 0, inner_every: int = 0,
+                 layout: dict | None = None):
+        self.solver = VlasovSolver21Spline(cfg, precision=precision, device=device, init=False,
+                                           layout=layout)
         # second-level checkpoint spacing of the backward pass (0: chosen from
         # free device memory)
         self.solver.adjoint_set_inner(inner_every)

@@ -4,7 +4,7 @@
 // The reference has no derivative code; this is the transpose of the step as
 // the forward kernels compute it (vls_kernels.cu, vls_rc.cu):
 //   drift D       f(cell) = sum_ab wy_a wx_b C[uI+a][rI+b] / 36   -> gather over
-//                 the inverse footpoint map (or scatter-add)
+//                 the inverse footpoint map
 //   tails E       ring[tail] = same gather at the chain's end    -> the same
 //   prefilter P   natural-BC Thomas solve of each line           -> transposed
 //                 recurrences (localSpline.hxx:953-1182 read backwards)
@@ -13,10 +13,9 @@
 //   shift s       s_r = Rcoef_r sum_{r' < r} bins_r'             -> reverse scan
 //   moment        bins_r = dR_r/4 (T_r + T_{r+1}), T_r = sum_j w_j sum_u b_u f
 // Adjoint values are FP64 in every precision mode; the forward state they
-// linearise around is read in the handle's storage type.  The default drift
-// transpose is a gather with a fixed summation order (deterministic); the
-// scatter-add form (FP64 atomics, order not deterministic) remains for
-// comparison and for grids with N_u >= 2^15.
+// linearise around is read in the handle's storage type.  The drift's
+// transpose is a gather with a fixed summation order, so the gradient is
+// bitwise reproducible.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -102,95 +101,8 @@ __device__ void solve_line_adj(const double *__restrict__ cb, int cst, double *_
   }
 }
 
-__device__ __forceinline__ void scatter16(double *Cbj, int pc, int rI, double x, int uI,
-                                          double y, double v) {
-  const double wx[4] = {bv2d(1.0 - x), bv1d(1.0 - x), bv1d(x), bv2d(x)};
-  const double wy[4] = {bv2d(1.0 - y), bv1d(1.0 - y), bv1d(y), bv2d(y)};
-  const double s = v * (1.0 / 36.0);
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    double *row = Cbj + (size_t)(uI + a) * pc + rI;
-    const double sa = s * wy[a];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) atomicAdd(row + b, sa * wx[b]);
-  }
-}
-
-constexpr uint32_t AFP_CHAIN = 0xFFFFFFFEu, AFP_FAR = 0xFFFFFFFDu;
+constexpr uint32_t AFP_CHAIN = 0xFFFFFFFEu;
 constexpr int AFP_FBITS = 21;
-
-// drift, transposed: lam (cells) -> Cb (C layout, all slices), chain fronts
-// -> ring adjoint
-template <typename T>
-__global__ void drift_adj_kernel(const double *__restrict__ lam, double *__restrict__ Cb,
-                                 const int32_t *__restrict__ idx, const T *__restrict__ fx,
-                                 const T *__restrict__ fy, const uint2 *__restrict__ fp2,
-                                 const int64_t *__restrict__ ch_start,
-                                 const int32_t *__restrict__ ch_len, double *__restrict__ ringb,
-                                 const uint2 *__restrict__ far_w, int64_t ndrift, Geometry g) {
-  const size_t n = (size_t)g.nr * g.nu * g.nj;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const double v = lam[i];
-    if (v == 0.0) continue;
-    const int j = (int)(i / ((size_t)g.nr * g.nu));
-    int kind, rI = 0, uI = 0;
-    uint32_t ch = 0;
-    double x = 0, y = 0;
-    if (sizeof(T) == 8) {
-      const int code = idx[i];
-      kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
-      ch = (uint32_t)(-2 - code);
-      if (code >= 0) {
-        rI = code & 0xffff;
-        uI = code >> 16;
-        x = (double)fx[i];
-        y = (double)fy[i];
-      }
-    } else {
-      uint2 w = fp2[i];
-      // far cells of the strip layout keep their footpoint in the far list
-      if (w.x == AFP_FAR) w = far_w[w.y];
-      kind = w.x < AFP_FAR ? 0 : (w.x == AFP_CHAIN ? 2 : 1);
-      ch = w.y;
-      if (kind == 0) {
-        rI = (int)(w.x >> AFP_FBITS);
-        uI = (int)(w.y >> AFP_FBITS);
-        const uint32_t m = (1u << AFP_FBITS) - 1u;
-        // the forward decodes the fraction to float exactly (21 bits)
-        x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
-        y = (double)(__uint_as_float(0x3F800000u | ((w.y & m) << 2)) - 1.0f);
-      }
-    }
-    if (kind == 0) {
-      scatter16(Cb + (size_t)j * (g.nu + 3) * g.pc, g.pc, rI, x, uI, y, v);
-    } else if (kind == 2) {
-      const int L = ch_len[ch];
-      atomicAdd(ringb + ch_start[ch] + ndrift % L, v);
-    }
-  }
-}
-
-// chain tails, transposed: ring adjoint of each chain's tail slot -> Cb
-// (the slot's value was written by this step's tails, so its adjoint is
-// consumed and cleared)
-__global__ void tails_adj_kernel(double *__restrict__ Cb, double *__restrict__ ringb,
-                                 const int64_t *__restrict__ ch_start,
-                                 const int32_t *__restrict__ ch_len,
-                                 const int32_t *__restrict__ t_idx, const double *__restrict__ t_x,
-                                 const double *__restrict__ t_y, const int32_t *__restrict__ t_j,
-                                 int64_t nch, int64_t ndrift, Geometry g) {
-  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= nch) return;
-  const int L = ch_len[c];
-  double *slot = ringb + ch_start[c] + (ndrift + L - 1) % L;
-  const double v = *slot;
-  *slot = 0.0;
-  const int code = t_idx[c];
-  if (code >= 0 && v != 0.0)
-    scatter16(Cb + (size_t)t_j[c] * (g.nu + 3) * g.pc, g.pc, code & 0xffff, t_x[c], code >> 16,
-              t_y[c], v);
-}
 
 // r-solve, transposed: each row k of every slice, Cb[j][k][0..M_r-1] ->
 // Gb[j][k][0..N_r-1]
@@ -359,8 +271,7 @@ constexpr uint32_t INV_TAIL = 0x80000000u;
 // fronts (the forward drift's decode, vls_kernels.cu)
 template <typename T>
 __device__ __forceinline__ bool cell_base(size_t i, const int32_t *__restrict__ idx,
-                                          const uint2 *__restrict__ fp2,
-                                          const uint2 *__restrict__ far_w, int &rI, int &uI,
+                                          const uint2 *__restrict__ fp2, int &rI, int &uI,
                                           uint2 &w) {
   if (sizeof(T) == 8) {
     const int code = idx[i];
@@ -370,8 +281,7 @@ __device__ __forceinline__ bool cell_base(size_t i, const int32_t *__restrict__ 
     return true;
   }
   w = fp2[i];
-  if (w.x == AFP_FAR) w = far_w[w.y];
-  if (w.x >= AFP_FAR) return false;
+  if (w.x >= AFP_CHAIN) return false;
   rI = (int)(w.x >> AFP_FBITS);
   uI = (int)(w.y >> AFP_FBITS);
   return true;
@@ -382,7 +292,7 @@ __device__ __forceinline__ bool cell_base(size_t i, const int32_t *__restrict__ 
 // bucket ends)
 template <typename T>
 __global__ void inv_fill_kernel(const int32_t *__restrict__ idx, const uint2 *__restrict__ fp2,
-                                const uint2 *__restrict__ far_w, const int32_t *__restrict__ t_idx,
+                                const int32_t *__restrict__ t_idx,
                                 int64_t nch, uint32_t *__restrict__ ends,
                                 uint32_t *__restrict__ ent, const int64_t *__restrict__ ebase,
                                 Geometry g) {
@@ -393,7 +303,7 @@ __global__ void inv_fill_kernel(const int32_t *__restrict__ idx, const uint2 *__
     uint32_t id;
     if (i < n) {
       uint2 w;
-      if (!cell_base<T>(i, idx, fp2, far_w, rI, uI, w)) continue;
+      if (!cell_base<T>(i, idx, fp2, rI, uI, w)) continue;
       j = (int)(i / S);
       const uint32_t within = (uint32_t)(i - (size_t)j * S);
       id = (within / (uint32_t)g.nr) << 16 | (within % (uint32_t)g.nr);
@@ -519,7 +429,6 @@ __device__ __forceinline__ void inv_entry(uint32_t id, const double *__restrict_
                                           const T *__restrict__ fy,
                                           const int32_t *__restrict__ idx,
                                           const uint2 *__restrict__ fp2,
-                                          const uint2 *__restrict__ far_w,
                                           const int32_t *__restrict__ t_idx,
                                           const double *__restrict__ t_x,
                                           const double *__restrict__ t_y, int nr, double &v,
@@ -541,8 +450,7 @@ __device__ __forceinline__ void inv_entry(uint32_t id, const double *__restrict_
     x = (double)fx[i];
     y = (double)fy[i];
   } else {
-    uint2 w = fp2[i];
-    if (w.x == AFP_FAR) w = far_w[w.y];
+    const uint2 w = fp2[i];
     rI = (int)(w.x >> AFP_FBITS);
     const uint32_t m = (1u << AFP_FBITS) - 1u;
     x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
@@ -565,7 +473,7 @@ __global__ void __launch_bounds__(128)
                             const uint32_t *__restrict__ ent, const int64_t *__restrict__ ebase,
                             const T *__restrict__ fx, const T *__restrict__ fy,
                             const int32_t *__restrict__ idx, const uint2 *__restrict__ fp2,
-                            const uint2 *__restrict__ far_w, const int32_t *__restrict__ t_idx,
+                            const int32_t *__restrict__ t_idx,
                             const double *__restrict__ t_x, const double *__restrict__ t_y,
                             Geometry g) {
   const int q0 = (blockIdx.x * 32 + threadIdx.x) * Q;
@@ -593,7 +501,7 @@ __global__ void __launch_bounds__(128)
       for (uint32_t e = k0 ? endj[k0 - 1] : 0u; e < e1; ++e) {
         double v, x, y;
         int rI;
-        inv_entry<T>(entj[e], lam, mB, mt, wjj, tv, cbase, fx, fy, idx, fp2, far_w, t_idx, t_x,
+        inv_entry<T>(entj[e], lam, mB, mt, wjj, tv, cbase, fx, fy, idx, fp2, t_idx, t_x,
                      t_y, g.nr, v, x, y, rI);
         const double s = 1.0 - y;
         const double wy[4] = {bv2d(s), bv1d(s), bv1d(y), bv2d(y)};
@@ -620,8 +528,7 @@ __global__ void __launch_bounds__(128)
 }
 
 // Entry-ordered form of the gather (FP32 handles).  The packed footpoint
-// word of each entry (far cells resolved; a chain tail is GEO_TAIL, chain
-// id) is stored once in entry order when the map is built, and each
+// word of each entry (a chain tail is GEO_TAIL, chain id) is stored once in entry order when the map is built, and each
 // transposed step first permutes its values into entry order (vperm: lam
 // plus the pending moment term, or the tail's ring adjoint), so that a
 // visit of the gather reads two arrays at the same index.  For FP64
@@ -631,8 +538,7 @@ constexpr uint32_t GEO_TAIL = 0xFFFFFFFFu;
 
 __global__ void inv_geo_kernel(const uint32_t *__restrict__ ent,
                                const int64_t *__restrict__ ebase, const uint2 *__restrict__ fp2,
-                               const uint2 *__restrict__ far_w, uint2 *__restrict__ geo,
-                               Geometry g) {
+                               uint2 *__restrict__ geo, Geometry g) {
   const int j = blockIdx.y;
   const int64_t e0 = ebase[j], e1 = ebase[j + 1];
   const size_t cbase = (size_t)j * g.nr * g.nu;
@@ -643,9 +549,7 @@ __global__ void inv_geo_kernel(const uint32_t *__restrict__ ent,
       geo[e] = make_uint2(GEO_TAIL, id & ~INV_TAIL);
       continue;
     }
-    uint2 w = fp2[cbase + (size_t)(id >> 16) * g.nr + (id & 0xffffu)];
-    if (w.x == AFP_FAR) w = far_w[w.y];
-    geo[e] = w;
+    geo[e] = fp2[cbase + (size_t)(id >> 16) * g.nr + (id & 0xffffu)];
   }
 }
 
@@ -747,11 +651,11 @@ __global__ void __launch_bounds__(128)
 }  // namespace
 
 template <typename T>
-cudaError_t launch_inv_fill(const int32_t *idx, const uint2 *fp2, const uint2 *far_w,
+cudaError_t launch_inv_fill(const int32_t *idx, const uint2 *fp2,
                             const int32_t *t_idx, int64_t nch, uint32_t *ends, uint32_t *ent,
                             const int64_t *ebase, const Geometry &g, cudaStream_t st) {
   const size_t n = (size_t)g.nr * g.nu * g.nj + (size_t)nch;
-  inv_fill_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(idx, fp2, far_w, t_idx, nch, ends, ent,
+  inv_fill_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(idx, fp2, t_idx, nch, ends, ent,
                                                         ebase, g);
   return cudaGetLastError();
 }
@@ -785,13 +689,13 @@ cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const M
                                     const double *tv, double *Cb, const uint32_t *ends,
                                     const uint32_t *ent, const int64_t *ebase, const T *fx,
                                     const T *fy, const int32_t *idx, const uint2 *fp2,
-                                    const uint2 *far_w, const int32_t *t_idx, const double *t_x,
+                                    const int32_t *t_idx, const double *t_x,
                                     const double *t_y, const Geometry &g, cudaStream_t st) {
   constexpr int R = 8, Q = 2;
   const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
                   (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
   drift_adj_gather_kernel<T, R, Q><<<grid, dim3(32, 4), 0, st>>>(
-      lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2, far_w, t_idx, t_x, t_y, g);
+      lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2, t_idx, t_x, t_y, g);
   return cudaGetLastError();
 }
 
@@ -801,8 +705,8 @@ static dim3 slice_grid(const Geometry &g) {
 }
 
 cudaError_t launch_inv_geo(const uint32_t *ent, const int64_t *ebase, const uint2 *fp2,
-                           const uint2 *far_w, uint2 *geo, const Geometry &g, cudaStream_t st) {
-  inv_geo_kernel<<<slice_grid(g), 256, 0, st>>>(ent, ebase, fp2, far_w, geo, g);
+                           uint2 *geo, const Geometry &g, cudaStream_t st) {
+  inv_geo_kernel<<<slice_grid(g), 256, 0, st>>>(ent, ebase, fp2, geo, g);
   return cudaGetLastError();
 }
 
@@ -826,40 +730,18 @@ cudaError_t launch_drift_adj_gather_perm(const double *vperm, const uint2 *geo, 
 }
 
 #define VLS_INV_INST(T)                                                                       \
-  template cudaError_t launch_inv_fill<T>(const int32_t *, const uint2 *, const uint2 *,       \
+  template cudaError_t launch_inv_fill<T>(const int32_t *, const uint2 *,                      \
                                           const int32_t *, int64_t, uint32_t *, uint32_t *,    \
                                           const int64_t *, const Geometry &, cudaStream_t);    \
   template cudaError_t launch_drift_adj_gather<T>(                                            \
       const double *, const double *, const MomentTables &, const double *, double *,         \
       const uint32_t *, const uint32_t *, const int64_t *, const T *, const T *,              \
-      const int32_t *, const uint2 *, const uint2 *, const int32_t *, const double *,         \
+      const int32_t *, const uint2 *, const int32_t *, const double *,                        \
       const double *, const Geometry &, cudaStream_t);
 VLS_INV_INST(float)
 
 VLS_INV_INST(double)
 #undef VLS_INV_INST
-
-template <typename T>
-cudaError_t launch_drift_adj(const double *lam, double *Cb, const int32_t *idx, const T *fx,
-                             const T *fy, const uint2 *fp2, const int64_t *ch_start,
-                             const int32_t *ch_len, double *ringb, const uint2 *far_w,
-                             int64_t ndrift, const Geometry &g, cudaStream_t st) {
-  const size_t n = (size_t)g.nr * g.nu * g.nj;
-  drift_adj_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(lam, Cb, idx, fx, fy, fp2, ch_start,
-                                                         ch_len, ringb, far_w, ndrift, g);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_tails_adj(double *Cb, double *ringb, const int64_t *ch_start,
-                             const int32_t *ch_len, const int32_t *t_idx, const double *t_x,
-                             const double *t_y, int64_t nch, int64_t ndrift, const Geometry &g,
-                             cudaStream_t st) {
-  if (nch <= 0) return cudaSuccess;
-  const int threads = 256;
-  tails_adj_kernel<<<(unsigned)((nch + threads - 1) / threads), threads, 0, st>>>(
-      Cb, ringb, ch_start, ch_len, t_idx, t_x, t_y, t_idx + nch, nch, ndrift, g);
-  return cudaGetLastError();
-}
 
 cudaError_t launch_prer_adj(const double *Cb, double *Gb, const Geometry &g,
                             const DirTables &tr, cudaStream_t st) {
@@ -897,16 +779,6 @@ cudaError_t launch_moment_adj(double *lam, const double *beta, const MomentTable
   return cudaGetLastError();
 }
 
-template cudaError_t launch_drift_adj<float>(const double *, double *, const int32_t *,
-                                             const float *, const float *, const uint2 *,
-                                             const int64_t *, const int32_t *, double *,
-                                             const uint2 *, int64_t, const Geometry &,
-                                             cudaStream_t);
-template cudaError_t launch_drift_adj<double>(const double *, double *, const int32_t *,
-                                              const double *, const double *, const uint2 *,
-                                              const int64_t *, const int32_t *, double *,
-                                              const uint2 *, int64_t, const Geometry &,
-                                              cudaStream_t);
 template cudaError_t launch_ucol_adj<float>(const float *, double *, double *, double *,
                                             double *, double *, const double *,
                                             const Geometry &, const DirTables &, cudaStream_t);

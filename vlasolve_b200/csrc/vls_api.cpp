@@ -80,23 +80,12 @@ struct vls_handle {
   RcDir<float> rcu_f{}, rcr_f{};
   int rcu_cfg = -1, rcr_cfg = -1;
   // TMA descriptors of each slot of C for the drift's staged windows (tmC)
-  // and strips (tmS, when strip_w != 0: the strip layout in use)
+  // and strips (tmS, when drift_kind is a strip kind)
   CUtensorMap tmC[8];
   CUtensorMap tmS[8];
-  int strip_w = 0;
-  // cells whose taps leave the strip's columns (FP32 strip layout): their
-  // packed word is FP_FAR with the index into far_w / far_cell, sorted by
-  // (slice, column, row); far_col[j * N_r + r] starts column (j, r); farsum
-  // receives each column's moment contribution from the far pass
-  bool far_mode = false;
-  int64_t nfar = 0;
-  uint2 *far_w = nullptr;
-  uint32_t *far_cell = nullptr;
-  int32_t *far_col = nullptr;
-  double *far_prod = nullptr;
-  double *farsum = nullptr;
-  std::vector<int32_t> far_col_h;  // host copy (batch ranges)
-  bool have_tma = false;
+  int drift_kind = DRIFT_WINDOW;
+  uint32_t drift_spins = MBAR_SPIN_LIMIT;  // polls of each bounded wait of the drift
+  vls_layout_desc layout{};                // what vls_get_layout reports
   // opt-in per-kernel event timing
   bool profiling = false;
   struct ProfRec {
@@ -123,7 +112,7 @@ struct vls_handle {
   // chosen from free device memory at the backward pass), kept between calls
   int adj_inner = 0, adj_last_inner = 0;
   // device bytes this handle holds (its allocations are freed by vls_destroy only)
-  size_t dev_bytes = 0, far_bytes = 0;
+  size_t dev_bytes = 0;
   std::vector<Ckpt> adj_sub;
   // backward-pass arrays (FP64) and the segment stash, kept between calls
   double *ab_lam = nullptr, *ab_Cb = nullptr, *ab_Gb = nullptr, *ab_A = nullptr,
@@ -286,7 +275,7 @@ static uint32_t pack_coord(int32_t I, double F, int32_t maxI) {
   if (qi < 0) qi = 0;
   return ((uint32_t)I << 21) | (uint32_t)qi;
 }
-static const uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu, FP_FAR = 0xFFFFFFFDu;
+static const uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu;
 
 static uint2 encode_packed(const Coords &c, int32_t code, double rF, double uF) {
   uint2 w;
@@ -301,75 +290,6 @@ static uint2 encode_packed(const Coords &c, int32_t code, double rF, double uF) 
     w.y = pack_coord(code >> 16, uF, c.nu - 1);
   }
   return w;
-}
-
-// Far cells of one slice (packed words p[0..slice), slice j): words whose
-// taps leave the drift strip's columns are replaced by FP_FAR + list index;
-// their original words and cell indices are appended to the host far list in
-// (column, row) order, and the per-column counts to fcount.
-struct FarHost {
-  std::vector<uint2> w;
-  std::vector<uint32_t> cell;
-  std::vector<int32_t> count;  // per (j, r)
-};
-static void mark_far_slice(const vls_handle *h, int j, uint2 *p, FarHost &fh) {
-  const Coords &c = h->co;
-  const int W = std::abs(h->strip_w) / 16 * 16, XL = (W - 32) / 2;
-  const size_t slice = (size_t)c.nr * c.nu;
-  std::vector<std::pair<uint32_t, uint32_t>> far;  // (r * nu + u, cell within slice)
-  for (size_t i = 0; i < slice; ++i) {
-    const uint2 w = p[i];
-    if (w.x >= FP_FAR) continue;
-    const int r = (int)(i % c.nr), u = (int)(i / c.nr);
-    const int wc = (int)(w.x >> 21) - ((r / 32) * 32 - XL);
-    if (wc < 0 || wc > W - 4) far.push_back({(uint32_t)(r * c.nu + u), (uint32_t)i});
-  }
-  std::sort(far.begin(), far.end());
-  for (auto &e : far) {
-    const size_t i = e.second;
-    const int r = (int)(i % c.nr);
-    fh.count[(size_t)j * c.nr + r]++;
-    const uint32_t idx = (uint32_t)fh.w.size();
-    fh.w.push_back(p[i]);
-    fh.cell.push_back((uint32_t)((size_t)j * slice + i));
-    p[i].x = FP_FAR;
-    p[i].y = idx;
-  }
-}
-
-static int upload_far(vls_handle *h, const FarHost &fh) {
-  auto release = [&](void *q) {
-    if (q) cudaFree(q);
-  };
-  release(h->far_w);
-  release(h->far_cell);
-  release(h->far_col);
-  release(h->far_prod);
-  h->dev_bytes -= h->far_bytes;
-  h->far_bytes = 0;
-  h->far_w = nullptr;
-  h->far_cell = nullptr;
-  h->far_col = nullptr;
-  h->far_prod = nullptr;
-  h->nfar = (int64_t)fh.w.size();
-  const size_t ncol = (size_t)h->co.nj * h->co.nr;
-  std::vector<int32_t> col(ncol + 1, 0);
-  for (size_t k = 0; k < ncol; ++k) col[k + 1] = col[k] + fh.count[k];
-  CK(h, cudaMalloc(&h->far_w, sizeof(uint2) * std::max<size_t>(fh.w.size(), 1)));
-  CK(h, cudaMalloc(&h->far_cell, sizeof(uint32_t) * std::max<size_t>(fh.cell.size(), 1)));
-  CK(h, cudaMalloc(&h->far_col, sizeof(int32_t) * col.size()));
-  CK(h, cudaMalloc(&h->far_prod, sizeof(double) * std::max<size_t>(fh.w.size(), 1)));
-  h->far_bytes = (sizeof(uint2) + sizeof(uint32_t) + sizeof(double)) *
-                     std::max<size_t>(fh.w.size(), 1) +
-                 sizeof(int32_t) * col.size();
-  h->dev_bytes += h->far_bytes;
-  h->far_col_h = col;
-  if (!fh.w.empty()) {
-    TRY(upload(h, h->far_w, fh.w.data(), sizeof(uint2) * fh.w.size()));
-    TRY(upload(h, h->far_cell, fh.cell.data(), sizeof(uint32_t) * fh.cell.size()));
-  }
-  TRY(upload(h, h->far_col, col.data(), sizeof(int32_t) * col.size()));
-  return VLS_OK;
 }
 
 // Encoding of one cell: -1 -> outside the box (value 0), <= -2 -> delayed
@@ -388,8 +308,6 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
   if (h->prec != VLS_FP64) packed.resize(slice * batch);
   std::vector<SliceFootpoints> sfp(batch);
   std::vector<SliceChains> sch(batch);
-  FarHost fh;
-  if (h->far_mode) fh.count.assign((size_t)c.nj * c.nr, 0);
   if (build_chains) {
     h->ch_cell_h.clear();
     h->ch_len_h.clear();
@@ -408,6 +326,13 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
     int64_t chain_base = (int64_t)h->ch_cell_h.size();
     for (int b = 0; b < nb; b++) {
       const SliceFootpoints &fp = sfp[b];
+      if (fp.halted >= 0 && bad.empty()) {
+        const int64_t cell = (int64_t)(j0 + b) * (int64_t)slice + fp.halted;
+        bad = "reflective kernel: the footpoint of cell " + std::to_string(cell) +
+              " reaches the reflection radius a second time, where the reference "
+              "terminates (vlasovSolver21.hxx:389-391); use kernelBufferSize 0 or "
+              "the delayed kernel";
+      }
       int64_t next_chain = chain_base;
       for (size_t i = 0; i < slice; i++) {
         const size_t o = (size_t)b * slice + i;
@@ -449,12 +374,9 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
       TRY(upload(h, (double *)h->fy + off, fy.data(), n * sizeof(double)));
     } else {
       for (size_t i = 0; i < n; i++) packed[i] = encode_packed(c, idx[i], fx[i], fy[i]);
-      if (h->far_mode)
-        for (int b = 0; b < nb; b++) mark_far_slice(h, j0 + b, packed.data() + (size_t)b * slice, fh);
       TRY(upload(h, h->fp2 + off, packed.data(), n * sizeof(uint2)));
     }
   }
-  if (h->far_mode) TRY(upload_far(h, fh));
   h->fp_gen++;
   return VLS_OK;
 }
@@ -518,13 +440,13 @@ static int setup_chain_device(vls_handle *h) {
   return VLS_OK;
 }
 
-// 3D tiled tensor map of C ([N_J][N_u+3][pc], element T): boxes of 64
-// columns x 40 rows x 1 slice for the drift windows.  The encoder is the
-// driver's cuTensorMapEncodeTiled, reached through the runtime (no libcuda
-// link).  Returns false when unavailable (the drift then gathers from global
-// memory directly).
+// 3D tiled tensor maps of C ([N_J][N_u+3][pc], element T): boxes of 64
+// columns x 40 rows x 1 slice for the drift windows, 48 columns x 64 rows x 1
+// slice for the strips.  The encoder is the driver's cuTensorMapEncodeTiled,
+// reached through the runtime (no libcuda link).  Returns false when it is
+// unavailable or refuses a map (vls_create then fails: every drift kernel
+// stages its coefficients by TMA).
 static bool make_tensor_map(vls_handle *h) {
-  if (std::getenv("VLS_NO_TMA")) return false;
   void *fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
@@ -551,14 +473,14 @@ static bool make_tensor_map(vls_handle *h) {
                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
-    if (h->strip_w != 0) {
-      const cuuint32_t sbox[3] = {(cuuint32_t)(std::abs(h->strip_w) / 16 * 16), 64, 1};
+    if (h->drift_kind != DRIFT_WINDOW) {
+      const cuuint32_t sbox[3] = {48, 64, 1};
       if (enc(&h->tmS[s],
               es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
               base, dims, strides, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        h->strip_w = 0;
+        return false;
     }
   }
   return true;
@@ -613,15 +535,7 @@ static void free_all(vls_handle *h) {
   h->inv_geo = nullptr;
   h->inv_vperm = nullptr;
   h->inv_gen = ~(uint64_t)0;
-  for (void *p : {(void *)h->far_w, (void *)h->far_cell, (void *)h->far_col,
-                  (void *)h->far_prod})
-    if (p) cudaFree(p);
   h->dev_bytes = 0;
-  h->far_bytes = 0;
-  h->far_w = nullptr;
-  h->far_cell = nullptr;
-  h->far_col = nullptr;
-  h->far_prod = nullptr;
   for (int k = 0; k < 8; k++) {
     if (h->bst[k]) cudaStreamDestroy(h->bst[k]);
     if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
@@ -636,9 +550,19 @@ static void free_all(vls_handle *h) {
 
 extern "C" int vls_create(const vls_grid_desc *grid,
                           const vls_solver_desc *solver, vls_handle **out) {
+  return vls_create_layout(grid, solver, nullptr, out);
+}
+
+extern "C" int vls_create_layout(const vls_grid_desc *grid, const vls_solver_desc *solver,
+                                 const vls_layout_desc *layout, vls_handle **out) {
   if (!grid || !solver || !out)
     return fail(nullptr, VLS_EINVAL, "vls_create: NULL argument");
   *out = nullptr;
+  const vls_layout_desc lay = layout ? *layout : vls_layout_desc{};
+  if (lay.prefilter < VLS_PREFILTER_AUTO || lay.prefilter > VLS_PREFILTER_SEGMENT ||
+      lay.drift < VLS_DRIFT_AUTO || lay.drift > VLS_DRIFT_STRIP1 || lay.slices_per_batch < 0 ||
+      lay.streams < 0 || lay.streams > 8)
+    return fail(nullptr, VLS_EINVAL, "vls_create: invalid layout descriptor");
   if (solver->precision != VLS_FP64 && solver->precision != VLS_FP32_BULK &&
       solver->precision != VLS_FP32_ALL)
     return fail(nullptr, VLS_EINVAL, "unknown precision");
@@ -673,21 +597,14 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   h->tr = thomas_tables(c.nr, c.sstep_inv[0]);
   h->tu = thomas_tables(c.nu, c.sstep_inv[1]);
   {
-    // prefilter kernels: register chunks (VLS_PREFILTER=segment selects the
-    // shared-memory segment kernels; VLS_RC=A|B|C|D|F|I a chunk layout for
-    // both directions, VLS_RC_U / VLS_RC_R for one)
-    const char *pf = std::getenv("VLS_PREFILTER");
-    const bool seg = pf && std::string(pf) == "segment";
-    const char *lay = std::getenv("VLS_RC");
-    const char *lay_u = std::getenv("VLS_RC_U"), *lay_r = std::getenv("VLS_RC_R");
-    if (!lay_u) lay_u = lay;
-    if (!lay_r) lay_r = lay;
+    // prefilter kernels: register chunks where a line fits them, else the
+    // shared-memory segment kernels (for every line with
+    // VLS_PREFILTER_SEGMENT)
+    const bool seg = lay.prefilter == VLS_PREFILTER_SEGMENT;
     const bool r64 = h->prec == VLS_FP64 || h->prec == VLS_FP32_BULK;
     if (!seg) {
-      h->rcu_cfg =
-          r64 ? rc_config<double>(h->tu, lay_u, true) : rc_config<float>(h->tu, lay_u, true);
-      h->rcr_cfg =
-          r64 ? rc_config<double>(h->tr, lay_r, false) : rc_config<float>(h->tr, lay_r, false);
+      h->rcu_cfg = r64 ? rc_config<double>(h->tu, true) : rc_config<float>(h->tu, true);
+      h->rcr_cfg = r64 ? rc_config<double>(h->tr, false) : rc_config<float>(h->tr, false);
     }
     h->rcu_d = rc_dir<double>(h->tu, h->rcu_cfg);
     h->rcr_d = rc_dir<double>(h->tr, h->rcr_cfg);
@@ -706,13 +623,11 @@ extern "C" int vls_create(const vls_grid_desc *grid,
   };
   const size_t es = h->esize, cells = h->cells;
   {
-    // slice batching (VLS_BATCH slices per batch, VLS_STREAMS streams);
-    // default: one batch of every slice
-    const char *eb = std::getenv("VLS_BATCH");
-    const char *es_ = std::getenv("VLS_STREAMS");
-    h->B = eb ? std::max(1, std::min(c.nj, std::atoi(eb))) : c.nj;
+    // slice batching (slices_per_batch, streams); default: one batch of
+    // every slice
+    h->B = lay.slices_per_batch > 0 ? std::min(c.nj, lay.slices_per_batch) : c.nj;
     h->nbatch = (c.nj + h->B - 1) / h->B;
-    h->NS = es_ ? std::max(1, std::min(8, std::atoi(es_))) : 1;
+    h->NS = std::max(1, lay.streams);
     h->NS = std::min(h->NS, h->nbatch);
     for (int k = 0; k < h->NS; k++)
       if (cudaStreamCreateWithFlags(&h->bst[k], cudaStreamNonBlocking) != cudaSuccess)
@@ -786,33 +701,23 @@ extern "C" int vls_create(const vls_grid_desc *grid,
       cudaMemsetAsync(h->count, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess ||
       cudaMemsetAsync(h->flag, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess)
     return fin(fail(hp, VLS_ECUDA, "cudaMemsetAsync failed"));
-  {
-    // drift layout: whole-strip staging where it fits (VLS_DRIFT=window, 48,
-    // 64, -48, -49, 50 or 51 selects one for measurements)
-    const char *dv = std::getenv("VLS_DRIFT");
-    const std::string d = dv ? dv : "";
-    const int want = d == "48"    ? 48
-                     : d == "64"  ? 64
-                     : d == "-48" ? -48
-                     : d == "-49" ? -49
-                     : d == "50"  ? 50
-                     : d == "51"  ? 51
-                                  : 0;
-    h->strip_w = d == "window" ? 0
-                 : h->esize == 4 ? drift_strip_width<float>(c.nu, want)
-                                 : drift_strip_width<double>(c.nu, want);
-  }
-  h->have_tma = make_tensor_map(hp);
-  // FP32 strip drift: VLS_FAR=1 moves the far cells to their own pass.  Off
-  // by default: on the 513 x 513 x 256 case it measured 7 % slower than
-  // leaving them to the strip kernel's global-memory path.
-  {
-    const char *fv = std::getenv("VLS_FAR");
-    h->far_mode = h->have_tma && h->strip_w != 0 && h->esize == 4 && fv &&
-                  std::string(fv) == "1";
-    if (h->far_mode && dalloc(hp, &h->farsum, sizeof(double) * (size_t)c.nj * c.nr) != VLS_OK)
-      return fin(VLS_ECUDA);
-  }
+  // drift kernel: whole-strip staging where it fits (see vls_layout_desc)
+  h->drift_kind = h->esize == 4 ? drift_strip_width<float>(c.nu, lay.drift)
+                                : drift_strip_width<double>(c.nu, lay.drift);
+  h->drift_spins = lay.drift_wait_spins == 0  ? MBAR_SPIN_LIMIT
+                   : lay.drift_wait_spins < 0 ? 0u
+                                              : (uint32_t)lay.drift_wait_spins;
+  if (!make_tensor_map(hp))
+    return fin(fail(hp, VLS_ECUDA, "TMA tensor maps of the spline coefficients unavailable"));
+  h->layout = lay;
+  h->layout.prefilter =
+      (h->rcu_cfg >= 0 || h->rcr_cfg >= 0) ? VLS_PREFILTER_REGISTER : VLS_PREFILTER_SEGMENT;
+  h->layout.drift = h->drift_kind;
+  h->layout.slices_per_batch = h->B;
+  h->layout.streams = h->NS;
+  h->layout.drift_wait_spins = (int32_t)std::min<uint32_t>(h->drift_spins, 0x7fffffffu);
+  h->layout.u_chunk_rows = rc_chunk_rows(h->rcu_cfg);
+  h->layout.r_chunk_rows = rc_chunk_rows(h->rcr_cfg);
   // tables
   std::vector<double> dR(c.nr), dU(c.nu), Ct1(c.nj), bu(c.nu), wj(c.nj), dR4(c.nr),
       Rcoef(c.nr);
@@ -859,6 +764,12 @@ extern "C" int vls_create(const vls_grid_desc *grid,
     if (fin(st3) != VLS_OK) return st3;
   }
   *out = h.release();
+  return VLS_OK;
+}
+
+extern "C" int vls_get_layout(const vls_handle *h, vls_layout_desc *used) {
+  if (!h || !used) return VLS_EINVAL;
+  *used = h->layout;
   return VLS_OK;
 }
 
@@ -911,10 +822,14 @@ static int put_f(vls_handle *h, const double *host) {
          }));
     }
   }
+  // non-finite values in the uploaded grid: status word bit 0
+  CK(h, h->prec == VLS_FP64
+            ? launch_nonfinite<double>((const double *)h->f, h->cells, h->flag + 2, h->st)
+            : launch_nonfinite<float>((const float *)h->f, h->cells, h->flag + 2, h->st));
   CK(h, cudaStreamSynchronize(h->st));
   h->have_f = true;
   h->moments_valid = false;
-  return VLS_OK;
+  return check_device_flags(h);
 }
 
 static int take_f(vls_handle *h, double *host) {
@@ -1066,6 +981,11 @@ extern "C" int vls_set_chain_values(vls_handle *h, const double *val,
     for (int64_t i = 0; i < h->nel; i++) p32[i] = (float)phys[i];
     TRY(upload(h, h->ch_val, p32.data(), sizeof(float) * h->nel));
   }
+  // the values are loaded either way; a non-finite one is reported
+  for (int64_t i = 0; i < h->nel; i++)
+    if (!std::isfinite(val[i]))
+      return fail(h, VLS_ENAN, "non-finite delayed-kernel chain value at element " +
+                                   std::to_string(i));
   return VLS_OK;
 }
 
@@ -1133,13 +1053,6 @@ extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
   } else {
     std::vector<uint2> p(h->cells);
     for (size_t i = 0; i < h->cells; i++) p[i] = encode_packed(c, idx[i], rF[i], uF[i]);
-    if (h->far_mode) {
-      FarHost fh;
-      fh.count.assign((size_t)c.nj * c.nr, 0);
-      const size_t slice = (size_t)c.nr * c.nu;
-      for (int j = 0; j < c.nj; j++) mark_far_slice(h, j, p.data() + (size_t)j * slice, fh);
-      TRY(upload_far(h, fh));
-    }
     TRY(upload(h, h->fp2, p.data(), sizeof(uint2) * h->cells));
   }
   h->fp_gen++;
@@ -1206,33 +1119,18 @@ static int drift_once(vls_handle *h, bool kick) {
     CK(h, timed(
               h, VLS_K_DRIFT,
               [&] {
-                if (h->have_tma && h->strip_w != 0) {
-                  if (h->far_mode) {
-                    const int c_lo = h->far_col_h[(size_t)g.j0 * h->co.nr];
-                    const int c_hi = h->far_col_h[(size_t)(g.j0 + g.nb) * h->co.nr];
-                    const cudaError_t e = launch_far_drift(
-                        (const float *)C, (float *)h->f, h->far_cell, h->far_w, h->far_col,
-                        c_lo, c_hi, moment_tables(h), h->far_prod, h->farsum, g, bs);
-                    h->launches += c_hi > c_lo ? 2 : 1;  // timed with the drift
-                    if (e != cudaSuccess) return e;
-                  }
-                  return launch_drift_strip<T>(&h->tmS[sl], h->strip_w, C, (T *)h->f, h->idx,
-                                               (const T *)h->fx, (const T *)h->fy, h->fp2,
-                                               h->ch_start, h->ch_len, (const T *)h->ch_val,
-                                               h->ndrift, moment_tables(h), h->partial,
-                                               h->far_mode ? h->farsum : nullptr, h->flag + 1,
-                                               g, bs);
-                }
-                if (h->have_tma)
-                  return launch_drift_tma<T>(&h->tmC[sl], C, (T *)h->f, h->idx,
-                                             (const T *)h->fx, (const T *)h->fy, h->fp2,
-                                             h->ch_start, h->ch_len, (const T *)h->ch_val,
-                                             h->ndrift, moment_tables(h), h->partial,
-                                             h->flag + 1, g, bs);
-                return launch_drift<T>(C, (T *)h->f, h->idx, (const T *)h->fx,
-                                       (const T *)h->fy, h->fp2, h->ch_start, h->ch_len,
-                                       (const T *)h->ch_val, h->ndrift, moment_tables(h),
-                                       h->partial, g, bs);
+                if (h->drift_kind != DRIFT_WINDOW)
+                  return launch_drift_strip<T>(&h->tmS[sl], h->drift_kind, C, (T *)h->f,
+                                               h->idx, (const T *)h->fx, (const T *)h->fy,
+                                               h->fp2, h->ch_start, h->ch_len,
+                                               (const T *)h->ch_val, h->ndrift,
+                                               moment_tables(h), h->partial, h->flag + 1,
+                                               h->drift_spins, g, bs);
+                return launch_drift_tma<T>(&h->tmC[sl], C, (T *)h->f, h->idx,
+                                           (const T *)h->fx, (const T *)h->fy, h->fp2,
+                                           h->ch_start, h->ch_len, (const T *)h->ch_val,
+                                           h->ndrift, moment_tables(h), h->partial,
+                                           h->flag + 1, h->drift_spins, g, bs);
               },
               bs));
   }
@@ -1260,7 +1158,7 @@ static int scan_once(vls_handle *h) {
   const Geometry g = geometry(h);
   CK(h, timed(h, VLS_K_SCAN, [&] {
        return launch_scan(h->partial, moment_tables(h), h->T2, h->bins, h->Mr,
-                          h->shift, h->mtot, h->count, g, h->st);
+                          h->shift, h->mtot, h->count, h->flag + 2, g, h->st);
      }));
   return VLS_OK;
 }
@@ -1293,20 +1191,31 @@ extern "C" int vls_step(vls_handle *h, int32_t nsteps) {
   }
 }
 
-// device-side status words: flag[1] bit 0/1 = a bounded mbarrier wait of the
-// drift timed out (the step then read global memory instead; results stay
-// valid but the hardware path misbehaved); bit 2/3 = the r-solve's bulk row
-// staging timed out (that step's results are not valid)
+// device-side status words, cleared once reported:
+// flag[1] bit 0/1 = a bounded mbarrier wait of the drift timed out (the step
+// then read global memory instead; results stay valid but the hardware path
+// misbehaved); bit 2/3 = the r-solve's bulk row staging timed out (that
+// step's results are not valid);
+// flag[2] bit 0 = a non-finite value in a grid uploaded from the host; bit 1
+// = the enclosed-mass scan of a step found a non-finite total mass (a NaN or
+// an infinity in f at the start of that step)
 static int check_device_flags(vls_handle *h) {
   unsigned int fl[4] = {0, 0, 0, 0};
   CK(h, cudaMemcpyAsync(fl, h->flag, sizeof(fl), cudaMemcpyDeviceToHost, h->st));
   CK(h, cudaStreamSynchronize(h->st));
-  if (fl[1]) {
+  if (fl[1] || fl[2]) {
     CK(h, cudaMemsetAsync(h->flag, 0, sizeof(fl), h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+  }
+  if (fl[1])
     return fail(h, VLS_ECUDA,
                 (fl[1] & 12u) ? "a bounded device wait timed out in the r-solve kernel"
                               : "a bounded device wait timed out in the drift kernel");
-  }
+  if (fl[2])
+    return fail(h, VLS_ENAN,
+                (fl[2] & 1u) ? "non-finite value in the grid loaded from the host"
+                             : "non-finite value in the grid: the total mass of a step "
+                               "is not finite");
   return VLS_OK;
 }
 
@@ -1653,11 +1562,9 @@ struct AdjBufs {
   std::vector<int64_t> ndrift;
   // chunked line kernels (else one thread per line through A and B)
   bool rc = false;
-  // drift transposed as a gather over the inverse footpoint map (else the
-  // scatter with FP64 atomics)
-  bool gather = true;
-  bool pending = false;  // lam still lacks the moment term in beta[N_r..2 N_r)
-  bool lazy_moment = true;  // leave the moment term to the readers of lam
+  // lam still lacks the moment term in beta[N_r..2 N_r): the next step's
+  // readers of lam (chain fronts and the gather) add it, or the end does
+  bool pending = false;
   bool perm = true;  // FP32 handles: the gather over entry-ordered values
   // shift of each stashed state (N_r per state), saved by the recomputation
   double *shifts = nullptr;
@@ -1688,7 +1595,7 @@ static int ensure_inv(vls_handle *h) {
   }
   if (nch) TRY(upload(h, h->inv_chc, h->ch_cell_h.data(), sizeof(int64_t) * nch));
   CK(h, cudaMemsetAsync(h->inv_ends, 0, h->cells * sizeof(uint32_t), h->st));
-  CK(h, launch_inv_fill<T>(h->idx, h->fp2, h->far_w, h->t_idx, nch, h->inv_ends, nullptr,
+  CK(h, launch_inv_fill<T>(h->idx, h->fp2, h->t_idx, nch, h->inv_ends, nullptr,
                            nullptr, g, h->st));
   CK(h, launch_inv_scan(h->inv_ends, h->inv_tot, g, h->st));
   std::vector<uint32_t> tot((size_t)g.nj);
@@ -1700,11 +1607,11 @@ static int ensure_inv(vls_handle *h) {
   if ((size_t)eb[g.nj] > h->cells + (size_t)nch)
     return fail(h, VLS_ECUDA, "adjoint: inverse footpoint map larger than its cells");
   TRY(upload(h, h->inv_ebase, eb.data(), sizeof(int64_t) * eb.size()));
-  CK(h, launch_inv_fill<T>(h->idx, h->fp2, h->far_w, h->t_idx, nch, h->inv_ends, h->inv_ent,
+  CK(h, launch_inv_fill<T>(h->idx, h->fp2, h->t_idx, nch, h->inv_ends, h->inv_ent,
                            h->inv_ebase, g, h->st));
   CK(h, launch_inv_sort(h->inv_ends, h->inv_ent, h->inv_ebase, g, h->st));
   if (h->inv_geo) {
-    CK(h, launch_inv_geo(h->inv_ent, h->inv_ebase, h->fp2, h->far_w, h->inv_geo, g, h->st));
+    CK(h, launch_inv_geo(h->inv_ent, h->inv_ebase, h->fp2, h->inv_geo, g, h->st));
     h->launches++;
   }
   h->launches += 4;
@@ -1720,7 +1627,7 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift,
   const MomentTables mt = moment_tables(h);
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
   const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
-  if (b.gather) {
+  {
     // lam of this step is lam + the moment term of the step after it, when
     // that was left pending
     const double *mB = b.pending ? b.beta + g.nr : nullptr;
@@ -1742,22 +1649,9 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift,
     CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
       return launch_drift_adj_gather<T>(b.lam, mB, mt, h->inv_tv, b.Cb, h->inv_ends,
                                         h->inv_ent, h->inv_ebase, (const T *)h->fx,
-                                        (const T *)h->fy, h->idx, h->fp2, h->far_w, h->t_idx,
+                                        (const T *)h->fy, h->idx, h->fp2, h->t_idx,
                                         h->t_x, h->t_y, g, h->st);
     }));
-  } else {
-    const size_t cbn = (size_t)g.nj * (g.nu + 3) * g.pc;
-    CK(h, cudaMemsetAsync(b.Cb, 0, cbn * sizeof(double), h->st));
-    CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
-      return launch_drift_adj<T>(b.lam, b.Cb, h->idx, (const T *)h->fx, (const T *)h->fy,
-                                 h->fp2, h->ch_start, h->ch_len, b.ringb, h->far_w, ndrift, g,
-                                 h->st);
-    }));
-    if (h->nch > 0)
-      CK(h, timed(h, VLS_K_ADJ_TAILS, [&] {
-        return launch_tails_adj(b.Cb, b.ringb, h->ch_start, h->ch_len, h->t_idx, h->t_x,
-                                h->t_y, h->nch, ndrift, g, h->st);
-      }));
   }
   CK(h, timed(h, VLS_K_ADJ_PRER, [&] {
     return b.rc ? launch_prer_adj_rc(b.Cb, b.Gb, g, b.rcr, h->st)
@@ -1770,13 +1664,7 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift,
                                      h->st);
   }));
   CK(h, timed(h, VLS_K_ADJ_MOMENT, [&] { return launch_shift_adj(b.sbar, b.beta, mt, g, h->st); }));
-  if (b.gather && b.lazy_moment) {
-    b.pending = true;  // added by the next step's readers of lam, or at the end
-  } else {
-    CK(h, timed(h, VLS_K_ADJ_MOMENT, [&] {
-      return launch_moment_adj(b.lam, b.beta, mt, g, h->st);
-    }));
-  }
+  b.pending = true;  // added by the next step's readers of lam, or at the end
   return VLS_OK;
 }
 
@@ -1789,20 +1677,15 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
   const size_t gn = (size_t)g.nj * (g.nu + 2) * g.nr;
   AdjBufs b{};
   {
-    const char *pf = std::getenv("VLS_PREFILTER");
-    b.rc = rc_adj_supported(h->tu, h->tr) && !(pf && std::string(pf) == "segment");
+    // chunked transposed line solves where the forward prefilter uses
+    // register chunks and the lines fit them; the entry-ordered gather for
+    // FP32 handles, the cell-ordered one for FP64
+    b.rc = rc_adj_supported(h->tu, h->tr) && h->layout.prefilter != VLS_PREFILTER_SEGMENT;
     b.rcu = rc_dir<double>(h->tu, 2);
     b.rcr = rc_dir<double>(h->tr, 2);
-    const char *da = std::getenv("VLS_DRIFT_ADJ");
-    b.gather = !(da && std::string(da) == "atomic");
-    const char *pp = std::getenv("VLS_ADJ_GATHER_PERM");
-    b.perm = sizeof(T) == 4 && !(pp && std::string(pp) == "0");
-    const char *mp = std::getenv("VLS_ADJ_MOMENT");
-    b.lazy_moment = !(mp && std::string(mp) == "pass");
-    // the inverse map's ids hold u in 15 bits
-    if (h->co.nu >= (1 << 15)) b.gather = false;
+    b.perm = sizeof(T) == 4;
   }
-  if (b.gather) TRY(ensure_inv<T>(h));
+  TRY(ensure_inv<T>(h));
   if (!h->ab_lam || (h->ab_rc != b.rc && !b.rc)) {
     if (!h->ab_lam) {
       TRY(adj_alloc(h, &h->ab_lam, cells * sizeof(double)));
@@ -1958,6 +1841,9 @@ extern "C" int vls_adjoint_backward(vls_handle *h, const double *dbins, int64_t 
   if (!h->adj_ready) return fail(h, VLS_ESTATE, "adjoint: run vls_adjoint_forward first");
   if (nbins != h->co.nr || ncells != h->cells || (dchain0 && nelems != h->nel))
     return fail(h, VLS_EINVAL, "adjoint: buffer sizes do not match the grid");
+  for (int64_t r = 0; r < nbins; r++)
+    if (!std::isfinite(dbins[r]))
+      return fail(h, VLS_ENAN, "adjoint: non-finite dL/dbins at bin " + std::to_string(r));
   CK(h, cudaSetDevice(h->solver.device));
   const int rc = h->esize == 8 ? adjoint_backward_impl<double>(h, dbins, df0, dchain0)
                                : adjoint_backward_impl<float>(h, dbins, df0, dchain0);

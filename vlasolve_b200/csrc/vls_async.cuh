@@ -7,10 +7,10 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include "vls_internal.h"
+
 namespace vls {
 
-// a wait gives up after ~2^20 polls (tens of milliseconds at most)
-constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 20;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -38,8 +38,9 @@ __device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 // non-blocking polls with a short sleep between them, at most MBAR_SPIN_LIMIT
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (uint32_t i = 0; i < MBAR_SPIN_LIMIT; ++i) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint32_t limit = MBAR_SPIN_LIMIT) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (mbar_test_wait(bar, parity)) return true;
     if (i >= 32) __nanosleep(20);
   }

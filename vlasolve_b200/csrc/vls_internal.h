@@ -14,9 +14,7 @@
 //         fp_x, fp_y [cells] double fractional footpoint offsets
 //   FP32: fp2 [cells] uint2         per direction index<<21 | round(frac*2^21);
 //                                     0xFFFFFFFF = outside, 0xFFFFFFFE = chain
-//                                     (second word = chain id), 0xFFFFFFFD =
-//                                     far cell of the strip layout (second
-//                                     word = index into far_w / far_cell)
+//                                     (second word = chain id)
 //   the footpoint tables end with FOOT_PAD_ROWS zeroed rows of N_r cells and
 //   32 more zeroed cells past the last slice, so that the strip drift
 //   prefetches the next rows of a slice without clamping the row index
@@ -31,6 +29,10 @@
 #include <cuda_runtime.h>
 
 namespace vls {
+
+// a bounded mbarrier wait gives up after ~2^20 polls (tens of milliseconds
+// at most)
+constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 20;
 
 // readable rows past the end of the footpoint tables (the strip drift reads
 // at most 16 warps x 2 rows ahead; 32 cells more cover the lanes past N_r)
@@ -92,42 +94,33 @@ cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
 template <typename T, typename R>
 cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr,
                         cudaStream_t st);
-// footpoints: FP64 handles use idx/fx/fy, FP32 handles the packed fp2 table
-template <typename T>
-cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
-                         const T *fy, const uint2 *fp2, const int64_t *ch_start,
-                         const int32_t *ch_len, const T *ch_val,
-                         int64_t ndrift, const MomentTables &mt, double *partial,
-                         const Geometry &g, cudaStream_t st);
-// drift with the coefficient windows staged by TMA (tmC: 3D map of C, box
-// 64 columns x 40 rows x 1 slice); err receives bit 0 / 1 on a wait timeout
+// drift kernels (the values of the public VLS_DRIFT_* layout choices)
+constexpr int DRIFT_AUTO = 0, DRIFT_WINDOW = 1, DRIFT_STRIP2 = 2, DRIFT_STRIP1 = 3;
+// footpoints: FP64 handles use idx/fx/fy, FP32 handles the packed fp2 table.
+// Drift with the coefficient windows staged by TMA (tmC: 3D map of C, box
+// 64 columns x 40 rows x 1 slice); err receives bit 0 when a wait for a
+// window ran out after `spins` polls (the cells then read C in global
+// memory), bit 1 when a copy had still not landed at the block's end
 template <typename T>
 cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int32_t *idx,
                              const T *fx, const T *fy, const uint2 *fp2,
                              const int64_t *ch_start, const int32_t *ch_len,
                              const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                             double *partial, unsigned int *err, const Geometry &g,
-                             cudaStream_t st);
+                             double *partial, unsigned int *err, uint32_t spins,
+                             const Geometry &g, cudaStream_t st);
 // drift with the block's whole coefficient strip staged by TMA (tmS: 3D map
-// of C with box |width| columns x 64 rows x 1 slice); width from
-// drift_strip_width (48: two blocks per SM; 64, -48: one), 0 = unsupported;
-// want != 0 requests one layout
+// of C with box 48 columns x 64 rows x 1 slice).  drift_strip_width returns
+// the strip kind (DRIFT_STRIP2 / DRIFT_STRIP1) the grid takes, or
+// DRIFT_WINDOW when none fits; want != DRIFT_AUTO requests one kind
 template <typename T>
 int drift_strip_width(int nu, int want);
 template <typename T>
-cudaError_t launch_drift_strip(const CUtensorMap *tmS, int width, const T *C, T *f,
+cudaError_t launch_drift_strip(const CUtensorMap *tmS, int kind, const T *C, T *f,
                                const int32_t *idx, const T *fx, const T *fy, const uint2 *fp2,
                                const int64_t *ch_start, const int32_t *ch_len,
                                const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                               double *partial, const double *farsum, unsigned int *err,
+                               double *partial, unsigned int *err, uint32_t spins,
                                const Geometry &g, cudaStream_t st);
-// far cells of the FP32 strip layout (packed word FP_FAR + list index)
-// (far cells [c_lo, c_hi) belong to the launch's slices; far_prod: one FP64
-// slot per far cell)
-cudaError_t launch_far_drift(const float *C, float *f, const uint32_t *far_cell,
-                             const uint2 *far_w, const int32_t *far_col, int c_lo, int c_hi,
-                             const MomentTables &mt, double *far_prod, double *farsum,
-                             const Geometry &g, cudaStream_t st);
 // chains [c_lo, c_hi) (all of the launch's slices) of nchains in total
 template <typename T>
 cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
@@ -136,11 +129,12 @@ cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,
                                int64_t nchains, int64_t c_lo, int64_t c_hi,
                                int64_t ndrift, const Geometry &g, cudaStream_t st);
 struct HostDirTables;
-// chunk layout of the register kernels for a direction (-1: none takes it;
-// pref "A", "B", "C" or null for the default; u_lines for the ucol kernel)
-// and its tables
+// chunk layout of the register kernels for a direction (-1: none takes it,
+// the shared-memory segment kernels then solve the lines; u_lines for the
+// ucol kernel), its chunk length in rows, and its tables
 template <typename R>
-int rc_config(const HostDirTables &t, const char *pref, bool u_lines);
+int rc_config(const HostDirTables &t, bool u_lines);
+int rc_chunk_rows(int cfg);
 template <typename R>
 RcDir<R> rc_dir(const HostDirTables &t, int cfg);
 template <typename T, typename R>
@@ -153,23 +147,13 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
                            unsigned int *err, cudaStream_t st);
 // adjoint of the step (vls_adjoint.cu); all adjoint arrays FP64: Cb in C
 // layout and Gb, A, B in G layout, each over all J slices
-template <typename T>
-cudaError_t launch_drift_adj(const double *lam, double *Cb, const int32_t *idx, const T *fx,
-                             const T *fy, const uint2 *fp2, const int64_t *ch_start,
-                             const int32_t *ch_len, double *ringb, const uint2 *far_w,
-                             int64_t ndrift, const Geometry &g, cudaStream_t st);
-cudaError_t launch_tails_adj(double *Cb, double *ringb, const int64_t *ch_start,
-                             const int32_t *ch_len, const int32_t *t_idx, const double *t_x,
-                             const double *t_y, int64_t nch, int64_t ndrift, const Geometry &g,
-                             cudaStream_t st);
 // the drift transposed as a gather over the inverse footpoint map: buckets of
 // cells and chain tails by the base node of their stencil (ends: [nj][nr*nu]
 // bucket ends within the slice's entries; ent: ids, ascending per bucket;
 // ebase: first entry of each slice).  inv_fill counts (ent == nullptr) or
 // places; inv_scan turns counts into starts and writes each slice's total.
 template <typename T>
-cudaError_t launch_inv_fill(const int32_t *idx, const uint2 *fp2, const uint2 *far_w,
-                            const int32_t *t_idx, int64_t nch, uint32_t *ends, uint32_t *ent,
+cudaError_t launch_inv_fill(const int32_t *idx, const uint2 *fp2, const int32_t *t_idx, int64_t nch, uint32_t *ends, uint32_t *ent,
                             const int64_t *ebase, const Geometry &g, cudaStream_t st);
 cudaError_t launch_inv_scan(uint32_t *ends, uint32_t *totals, const Geometry &g,
                             cudaStream_t st);
@@ -186,12 +170,12 @@ cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const M
                                     const double *tv, double *Cb, const uint32_t *ends,
                                     const uint32_t *ent, const int64_t *ebase, const T *fx,
                                     const T *fy, const int32_t *idx, const uint2 *fp2,
-                                    const uint2 *far_w, const int32_t *t_idx, const double *t_x,
+                                    const int32_t *t_idx, const double *t_x,
                                     const double *t_y, const Geometry &g, cudaStream_t st);
 // entry-ordered form (FP32 handles): packed words of the entries once per
 // map, values permuted into entry order each step, gather
 cudaError_t launch_inv_geo(const uint32_t *ent, const int64_t *ebase, const uint2 *fp2,
-                           const uint2 *far_w, uint2 *geo, const Geometry &g, cudaStream_t st);
+                           uint2 *geo, const Geometry &g, cudaStream_t st);
 cudaError_t launch_inv_perm(const uint32_t *ent, const int64_t *ebase, const double *lam,
                             const double *mB, const MomentTables &mt, const double *tv,
                             double *vperm, const Geometry &g, cudaStream_t st);
@@ -221,10 +205,11 @@ cudaError_t launch_prer_adj_rc(const double *Cb, double *Gb, const Geometry &g,
 template <typename T>
 cudaError_t launch_moment(const T *f, const MomentTables &mt, double *partial,
                           const Geometry &g, cudaStream_t st);
+// status |= 2 when the total mass is not finite (a NaN or an infinity in f)
 cudaError_t launch_scan(const double *partial, const MomentTables &mt,
                         double *T2, double *bins, double *Mr, double *shift,
-                        double *mtot, unsigned int *count, const Geometry &g,
-                        cudaStream_t st);
+                        double *mtot, unsigned int *count, unsigned int *status,
+                        const Geometry &g, cudaStream_t st);
 template <typename T>
 cudaError_t launch_stats(const T *f, const double *R, const double *U,
                          const double *J, const double *dR, const double *dU,

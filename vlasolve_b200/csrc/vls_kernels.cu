@@ -553,156 +553,16 @@ __device__ __forceinline__ float eval2d<float>(const float *__restrict__ Cj, int
 
 constexpr int DR_W = 8;  // warps per drift block
 
-// footpoint of one cell, decoded: taps at (rI.., uI..) with fractions (x, y);
-// kind 0 = gather, 1 = outside (0), 2 = delayed-kernel chain `ch`
-template <typename T>
-struct Foot {
-  int off, kind;
-  int64_t ch;
-  T x, y;
-};
-
-// FP64 tables: idx = rI | uI<<16, -1 outside, <= -2 chain; FP64 fractions
-__device__ __forceinline__ Foot<double> load_foot(const int32_t *__restrict__ idx,
-                                                  const double *__restrict__ fx,
-                                                  const double *__restrict__ fy,
-                                                  const uint2 *, size_t i, int pc) {
-  Foot<double> p;
-  const int code = __ldg(idx + i);
-  p.kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
-  p.ch = -2 - (int64_t)code;
-  p.off = code >= 0 ? (code >> 16) * pc + (code & 0xffff) : 0;
-  p.x = code >= 0 ? __ldg(fx + i) : 0.0;
-  p.y = code >= 0 ? __ldg(fy + i) : 0.0;
-  return p;
-}
-
 // FP32 tables, 8 bytes per cell: word = index << FP_FBITS | round(frac * 2^FP_FBITS)
 // per direction; FP_OUT / FP_CHAIN in the first word mark the two special kinds
 // (the second word then holds the chain id).  The 21 fraction bits are placed
 // straight into a float mantissa (value 1.frac, minus 1): no int->float convert.
 constexpr int FP_FBITS = 21;
 constexpr uint32_t FP_FMASK = (1u << FP_FBITS) - 1u;
-constexpr uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu, FP_FAR = 0xFFFFFFFDu;
+constexpr uint32_t FP_OUT = 0xFFFFFFFFu, FP_CHAIN = 0xFFFFFFFEu;
 
 __device__ __forceinline__ float frac21(uint32_t w) {
   return __uint_as_float(0x3F800000u | ((w & FP_FMASK) << 2)) - 1.0f;
-}
-
-__device__ __forceinline__ Foot<float> load_foot(const int32_t *, const float *,
-                                                 const float *,
-                                                 const uint2 *__restrict__ fp2,
-                                                 size_t i, int pc) {
-  Foot<float> p;
-  const uint2 w = __ldg(fp2 + i);
-  const bool ok = w.x < FP_CHAIN;
-  p.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
-  p.ch = (int64_t)w.y;
-  p.off = ok ? (int)(w.y >> FP_FBITS) * pc + (int)(w.x >> FP_FBITS) : 0;
-  p.x = frac21(w.x);
-  p.y = frac21(w.y);
-  return p;
-}
-
-template <typename T>
-__device__ __forceinline__ T eval_cell(const T *Cj, int pc, const Foot<T> &p);
-template <>
-__device__ __forceinline__ double eval_cell<double>(const double *Cj, int pc,
-                                                    const Foot<double> &p) {
-  return eval2d<double>(Cj + p.off, pc, 0, p.x, 0, p.y);
-}
-template <>
-__device__ __forceinline__ float eval_cell<float>(const float *Cj, int pc,
-                                                  const Foot<float> &p) {
-  return eval2d_f32x2(Cj, pc, p.off, p.x, p.y);
-}
-
-__device__ __forceinline__ void prefetch_l2(const void *p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
-template <typename T, int CELLS>
-__device__ __forceinline__ void load_group(Foot<T> (&p)[CELLS],
-                                           const int32_t *__restrict__ idx,
-                                           const T *__restrict__ fx,
-                                           const T *__restrict__ fy,
-                                           const uint2 *__restrict__ fp2,
-                                           size_t row0, int nr, int u0, int ue,
-                                           int pc) {
-#pragma unroll
-  for (int c = 0; c < CELLS; ++c) {
-    const int u = u0 + c;
-    p[c] = load_foot(idx, fx, fy, fp2, row0 + (size_t)(u < ue ? u : u0) * nr, pc);
-    if (u >= ue) p[c].kind = 1;
-  }
-}
-
-template <typename T, int CELLS>
-__global__ void __launch_bounds__(32 * DR_W, 4)
-    drift_kernel(const T *__restrict__ C, T *__restrict__ f,
-                 const int32_t *__restrict__ idx, const T *__restrict__ fx,
-                 const T *__restrict__ fy, const uint2 *__restrict__ fp2,
-                 const int64_t *__restrict__ ch_start,
-                 const int32_t *__restrict__ ch_len,
-                 const T *__restrict__ ch_val, int64_t ndrift, MomentTables mt,
-                 double *__restrict__ partial, Geometry g) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int r = blockIdx.x * 32 + lane;
-  const int j = g.j0 + blockIdx.y;
-  const T *Cj = C + (size_t)blockIdx.y * (g.nu + 3) * g.pc;
-  // each warp walks a contiguous band of u rows: consecutive rows have
-  // neighbouring footpoints, so their 4x4 patches overlap in L1
-  const int band = (g.nu + DR_W - 1) / DR_W;
-  const int ub = w * band;
-  const int ue = min(g.nu, ub + band);
-  const size_t row0 = (size_t)j * g.nu * g.nr + r;  // cell (j, u, r) = row0 + u*nr
-  double acc = 0.0;
-  if (r < g.nr && ub < ue) {
-    Foot<T> nxt[CELLS];
-    load_group<T, CELLS>(nxt, idx, fx, fy, fp2, row0, g.nr, ub, ue, g.pc);
-    for (int u0 = ub; u0 < ue; u0 += CELLS) {
-      Foot<T> p[CELLS];
-#pragma unroll
-      for (int c = 0; c < CELLS; ++c) p[c] = nxt[c];
-      // footpoints of the next group are in flight while this one gathers
-      if (u0 + CELLS < ue)
-        load_group<T, CELLS>(nxt, idx, fx, fy, fp2, row0, g.nr, u0 + CELLS, ue, g.pc);
-      // most footpoints lie within a cell of their own node: warm L2 with
-      // the coefficient rows this warp reaches a few iterations from now
-      prefetch_l2(Cj + (size_t)min(u0 + 16, g.nu + 2) * g.pc + r);
-      T v[CELLS];
-#pragma unroll
-      for (int c = 0; c < CELLS; ++c) {
-        // branch-free gather (special cells read a valid patch, then drop it)
-        v[c] = eval_cell<T>(Cj, g.pc, p[c]);
-        if (p[c].kind == 1) v[c] = T(0);
-      }
-      T part = T(0);
-#pragma unroll
-      for (int c = 0; c < CELLS; ++c) {
-        const int u = u0 + c;
-        if (u < ue) {
-          if (p[c].kind == 2) {
-            const int L = __ldg(ch_len + p[c].ch);
-            v[c] = ch_val[__ldg(ch_start + p[c].ch) + ndrift % L];
-          }
-          f[row0 + (size_t)u * g.nr] = v[c];
-          part += (T)__ldg(mt.bu + u) * v[c];
-        }
-      }
-      // moment partial: CELLS products summed in T, then accumulated in FP64
-      acc += (double)part;
-    }
-  }
-  __shared__ double red[DR_W][32];
-  red[w][lane] = acc;
-  __syncthreads();
-  if (w == 0 && r < g.nr) {
-    double s = 0.0;
-#pragma unroll
-    for (int k = 0; k < DR_W; ++k) s += red[k][lane];
-    partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * s;
-  }
 }
 
 // ------------------------------------------------------- TMA-staged drift
@@ -722,35 +582,6 @@ struct Cell {
   uint32_t ch;
   T x, y;
 };
-
-__device__ __forceinline__ Cell<double> load_cell(const int32_t *__restrict__ idx,
-                                                  const double *__restrict__ fx,
-                                                  const double *__restrict__ fy,
-                                                  const uint2 *, size_t i) {
-  Cell<double> c;
-  const int code = __ldg(idx + i);
-  c.kind = code >= 0 ? 0 : (code == -1 ? 1 : 2);
-  c.ch = (uint32_t)(-2 - code);
-  c.rI = code >= 0 ? (code & 0xffff) : 0;
-  c.uI = code >= 0 ? (code >> 16) : 0;
-  c.x = code >= 0 ? __ldg(fx + i) : 0.0;
-  c.y = code >= 0 ? __ldg(fy + i) : 0.0;
-  return c;
-}
-__device__ __forceinline__ Cell<float> load_cell(const int32_t *, const float *,
-                                                 const float *,
-                                                 const uint2 *__restrict__ fp2, size_t i) {
-  Cell<float> c;
-  const uint2 w = __ldg(fp2 + i);
-  const bool ok = w.x < FP_CHAIN;
-  c.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
-  c.ch = w.y;
-  c.rI = ok ? (int)(w.x >> FP_FBITS) : 0;
-  c.uI = ok ? (int)(w.y >> FP_FBITS) : 0;
-  c.x = frac21(w.x);
-  c.y = frac21(w.y);
-  return c;
-}
 
 // Footpoint words as loaded (decoded only where the cell is computed, so that
 // prefetched loads stay in flight)
@@ -782,13 +613,12 @@ __device__ __forceinline__ RawCell<double> load_raw(const int32_t *__restrict__ 
   c.y = __ldg(fy + i);
   return c;
 }
-// kinds: 0 gather, 1 outside (0), 2 delayed-kernel chain front, 3 far cell
-// (computed by the far pass; FP32 strip layout only)
+// kinds: 0 gather, 1 outside (0), 2 delayed-kernel chain front
 __device__ __forceinline__ Cell<float> decode(const RawCell<float> &r) {
   Cell<float> c;
   const uint2 w = r.w;
-  const bool ok = w.x < FP_FAR;
-  c.kind = ok ? 0 : (w.x == FP_OUT ? 1 : (w.x == FP_CHAIN ? 2 : 3));
+  const bool ok = w.x < FP_CHAIN;
+  c.kind = ok ? 0 : (w.x == FP_OUT ? 1 : 2);
   c.ch = w.y;
   c.rI = ok ? (int)(w.x >> FP_FBITS) : 0;
   c.uI = ok ? (int)(w.y >> FP_FBITS) : 0;
@@ -836,7 +666,7 @@ __global__ void __launch_bounds__(DT_THREADS)
                      const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
                      const int32_t *__restrict__ ch_len, const T *__restrict__ ch_val,
                      int64_t ndrift, MomentTables mt, double *__restrict__ partial,
-                     unsigned int *err, Geometry g) {
+                     unsigned int *err, uint32_t spins, Geometry g) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T *win = reinterpret_cast<T *>(smem_raw);  // two windows
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + 2 * DW_COLS * DW_ROWS * sizeof(T));
@@ -883,7 +713,7 @@ __global__ void __launch_bounds__(DT_THREADS)
     }
     const int b = c & 1;
     // after one failed wait this thread waits no more (it reads C globally)
-    const bool have = issuing && mbar_wait_bounded(&bar[b], (uint32_t)((c >> 1) & 1));
+    const bool have = issuing && mbar_wait_bounded(&bar[b], (uint32_t)((c >> 1) & 1), spins);
     if (have) pending &= ~(1u << b);
     if (!have && issuing) {
       issuing = false;  // never stack a second copy onto an unfinished one
@@ -948,8 +778,8 @@ cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int
                              const T *fx, const T *fy, const uint2 *fp2,
                              const int64_t *ch_start, const int32_t *ch_len,
                              const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                             double *partial, unsigned int *err, const Geometry &g,
-                             cudaStream_t st) {
+                             double *partial, unsigned int *err, uint32_t spins,
+                             const Geometry &g, cudaStream_t st) {
   const size_t smem = 2 * DW_COLS * DW_ROWS * sizeof(T) + 2 * sizeof(uint64_t);
   cudaError_t e = cudaFuncSetAttribute(drift_tma_kernel<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -957,21 +787,7 @@ cudaError_t launch_drift_tma(const CUtensorMap *tmC, const T *C, T *f, const int
   dim3 grid((g.nr + 31) / 32, g.nb);
   drift_tma_kernel<T><<<grid, DT_THREADS, smem, st>>>(*tmC, C, f, idx, fx, fy, fp2, ch_start,
                                                        ch_len, ch_val, ndrift, mt, partial,
-                                                       err, g);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_drift(const T *C, T *f, const int32_t *idx, const T *fx,
-                         const T *fy, const uint2 *fp2, const int64_t *ch_start,
-                         const int32_t *ch_len, const T *ch_val,
-                         int64_t ndrift, const MomentTables &mt, double *partial,
-                         const Geometry &g, cudaStream_t st) {
-  dim3 grid((g.nr + 31) / 32, g.nb);
-  constexpr int CELLS = 2;
-  drift_kernel<T, CELLS><<<grid, 32 * DR_W, 0, st>>>(C, f, idx, fx, fy, fp2, ch_start,
-                                                      ch_len, ch_val, ndrift, mt,
-                                                      partial, g);
+                                                       err, spins, g);
   return cudaGetLastError();
 }
 
@@ -1022,7 +838,7 @@ struct FastFoot {
 };
 __device__ __forceinline__ FastFoot<float> fast_foot(const RawCell<float> &c) {
   FastFoot<float> p;
-  p.gather = c.w.x < FP_FAR;
+  p.gather = c.w.x < FP_CHAIN;
   p.rI = (int)(c.w.x >> FP_FBITS);
   p.uI = (int)(c.w.y >> FP_FBITS);
   // both fractions with one packed subtraction of 1 (values 1.frac21)
@@ -1046,7 +862,8 @@ __device__ __forceinline__ FastFoot<double> fast_foot(const RawCell<double> &c) 
 
 // The in-strip gather of one cell, run for every lane with the tap offset
 // zeroed where it does not apply; `slow`: the cell takes strip_slow instead
-// (outside, chain front, far cell, taps outside the strip's columns).
+// (outside, chain front, taps outside the strip's columns, or every cell
+// after a failed wait: wcap = 0).
 template <typename T, int WC>
 __device__ __forceinline__ T strip_fast(const RawCell<T> &c, const T *win, int x0,
                                         uint32_t wcap, bool col_ok, bool &slow) {
@@ -1059,42 +876,37 @@ __device__ __forceinline__ T strip_fast(const RawCell<T> &c, const T *win, int x
 }
 
 // A cell the in-strip gather does not cover: the gather from C in global
-// memory, a chain front, or zero outside; `put` turns false for far cells,
-// whose value and moment come from the far pass.
+// memory, a chain front, or zero outside.
 template <typename T>
 __device__ __forceinline__ T strip_slow(const RawCell<T> &c, const T *__restrict__ Cj,
-                                     const int64_t *__restrict__ ch_start,
-                                     const int32_t *__restrict__ ch_len,
-                                     const T *__restrict__ ch_val, int64_t ndrift,
-                                     const Geometry &g, bool &put) {
+                                        const int64_t *__restrict__ ch_start,
+                                        const int32_t *__restrict__ ch_len,
+                                        const T *__restrict__ ch_val, int64_t ndrift,
+                                        const Geometry &g) {
   const Cell<T> cl = decode(c);
   T v = T(0);
   if (cl.kind == 0)
     v = eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
   else if (cl.kind == 2)
     v = ch_val[__ldg(ch_start + cl.ch) + ndrift % __ldg(ch_len + cl.ch)];
-  put = cl.kind != 3;
   return v;
 }
 
 // One cell of the strip drift once every box has landed (wcap = WC - 3, or 0
 // after a failed wait, which sends every cell to the global-memory gather).
-// The in-strip gather runs for every lane, with the tap offset zeroed where
-// it does not apply; a warp vote sends the rare other cells (outside,
-// chain fronts, far cells, taps outside the strip's columns) through the
-// general decode.  `put`: the cell's value is stored and enters the moment.
+// A warp vote sends the rare cells the in-strip gather does not cover through
+// the general decode.  Every lane of the warp must call it.
 template <typename T, int WC>
 __device__ __forceinline__ T strip_cell(const RawCell<T> &c, const T *win, int x0,
                                         uint32_t wcap, bool col_ok, const T *__restrict__ Cj,
                                         const int64_t *__restrict__ ch_start,
                                         const int32_t *__restrict__ ch_len,
                                         const T *__restrict__ ch_val, int64_t ndrift,
-                                        const Geometry &g, bool &put) {
+                                        const Geometry &g) {
   bool slow;
   T v = strip_fast<T, WC>(c, win, x0, wcap, col_ok, slow);
-  put = col_ok;
   if (__any_sync(0xffffffffu, slow))
-    if (slow) v = strip_slow<T>(c, Cj, ch_start, ch_len, ch_val, ndrift, g, put);
+    if (slow) v = strip_slow<T>(c, Cj, ch_start, ch_len, ch_val, ndrift, g);
   return v;
 }
 
@@ -1146,7 +958,7 @@ __device__ __forceinline__ void strip_rows(
   // the footpoint words further ahead measured 4 % slower)
   for (; u + NW * (PF - 1) < g.nu; u += NW * PF) {
     T v[PF];
-    bool slow[PF], put[PF];
+    bool slow[PF];
     RawCell<T> c[PF];
     bool any = false;
 #pragma unroll
@@ -1154,18 +966,17 @@ __device__ __forceinline__ void strip_rows(
       c[k] = q[k];
       q[k] = load_raw(ids, fxs, fys, fps, off + ahead + k * step);
       v[k] = strip_fast<T, WC>(c[k], win, x0, wcap, col_ok, slow[k]);
-      put[k] = col_ok;
       any |= slow[k];
     }
     if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
       for (int k = 0; k < PF; ++k)
-        if (slow[k]) v[k] = strip_slow<T>(c[k], Cj, ch_start, ch_len, ch_val, ndrift, g, put[k]);
+        if (slow[k]) v[k] = strip_slow<T>(c[k], Cj, ch_start, ch_len, ch_val, ndrift, g);
     }
     T part = T(0);
 #pragma unroll
     for (int k = 0; k < PF; ++k) {
-      if (put[k]) {
+      if (col_ok) {
         fs[off] = v[k];
         part += moment_bu<T>(mt, u + NW * k) * v[k];
       }
@@ -1173,15 +984,15 @@ __device__ __forceinline__ void strip_rows(
     }
     acc += (double)part;
   }
-  // the last, partial group
+  // the last, partial group (u is warp-uniform, so the vote in strip_cell
+  // sees the whole warp)
   T part = T(0);
 #pragma unroll
   for (int k = 0; k < PF; ++k) {
     if (u + NW * k < g.nu) {
-      bool put;
       const T v = strip_cell<T, WC>(q[k], win, x0, wcap, col_ok, Cj, ch_start, ch_len, ch_val,
-                                    ndrift, g, put);
-      if (put) {
+                                    ndrift, g);
+      if (col_ok) {
         fs[off] = v;
         part += moment_bu<T>(mt, u + NW * k) * v;
       }
@@ -1191,7 +1002,12 @@ __device__ __forceinline__ void strip_rows(
   acc += (double)part;
 }
 
-template <typename T, int WC, int NW, int MINB, bool WAITALL>
+// Every box is awaited before the first cell (the other block on the SM, if
+// any, computes meanwhile).  `spins` bounds each of those waits (a wait that
+// runs out sets err bit 0 and sends every cell of the block to the gather
+// from global memory); the last wait, which keeps the block's shared memory
+// until every copy has landed, has the full limit (err bit 1).
+template <typename T, int WC, int NW, int MINB>
 __global__ void __launch_bounds__(32 * NW, MINB)
     drift_strip_kernel(const __grid_constant__ CUtensorMap tmS, const T *__restrict__ C,
                        T *__restrict__ f, const int32_t *__restrict__ idx,
@@ -1199,8 +1015,7 @@ __global__ void __launch_bounds__(32 * NW, MINB)
                        const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
                        const int32_t *__restrict__ ch_len, const T *__restrict__ ch_val,
                        int64_t ndrift, MomentTables mt, double *__restrict__ partial,
-                       const double *__restrict__ farsum, unsigned int *err, int extra,
-                       Geometry g) {
+                       unsigned int *err, uint32_t spins, int extra, Geometry g) {
   constexpr int XL = (WC - 32) / 2;
   // rows of footpoints in flight per thread (2: 6 % faster than 4 and 3 %
   // faster than 1 on the 513 x 513 x 256 case)
@@ -1226,79 +1041,17 @@ __global__ void __launch_bounds__(32 * NW, MINB)
   }
   __syncthreads();
   const T *Cj = C + (size_t)jl * rows * g.pc;
-  const size_t row0 = (size_t)j * g.nu * g.nr + r;
   const bool col_ok = r < g.nr;
-  int ready = 0;  // boxes [0, ready) seen complete by this thread
   bool waits_ok = true;
-  if (WAITALL) {
-    // every box before the first cell (the other block on the SM computes
-    // meanwhile); the per-cell test below then never waits
-    for (; ready < nch; ++ready)
-      if (!mbar_wait_bounded(&bar[ready], 0u)) {
-        waits_ok = false;
-        atomicOr(err, 1u);
-        break;
-      }
-  }
+  for (int c = 0; c < nch; ++c)
+    if (!mbar_wait_bounded(&bar[c], 0u, spins)) {
+      waits_ok = false;
+      atomicOr(err, 1u);
+      break;
+    }
   double acc = 0.0;
-  if constexpr (WAITALL) {
-    strip_rows<T, WC, NW, PF>(win, x0, waits_ok, col_ok, j, r, w, Cj, f, idx, fx, fy, fp2,
-                              ch_start, ch_len, ch_val, ndrift, mt, g, acc);
-  } else {
-    // footpoint words of the next PF rows in flight (the moment weights b_u are
-    // read where used: prefetching them too cost 10 % from register pressure)
-    RawCell<T> q[PF];
-#pragma unroll
-    for (int k = 0; k < PF; ++k) {
-      const int u = w + NW * k;
-      const int uc = u < g.nu ? u : 0;
-      q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? uc : 0) * g.nr);
-    }
-    for (int ub = w; ub < g.nu; ub += NW * PF) {
-      T part = T(0);
-#pragma unroll
-      for (int k = 0; k < PF; ++k) {
-        const int u = ub + NW * k;
-        const Cell<T> cl = decode(q[k]);
-        const int un = u + NW * PF;
-        const int unc = un < g.nu ? un : 0;
-        q[k] = load_raw(idx, fx, fy, fp2, row0 + (size_t)(col_ok ? unc : 0) * g.nr);
-        if (u < g.nu && col_ok) {
-          T v = T(0);
-          if (cl.kind == 0) {
-            const int wc = cl.rI - x0;
-            bool inwin = waits_ok && wc >= 0 && wc <= WC - 4;
-            if (inwin) {
-              // boxes complete in issue order; wait up to the one holding the last tap row
-              const int cb = (cl.uI + 3) / DS_ROWS;
-              while (ready <= cb) {
-                if (!mbar_wait_bounded(&bar[ready], 0u)) {
-                  waits_ok = false;
-                  inwin = false;
-                  atomicOr(err, 1u);
-                  break;
-                }
-                ++ready;
-              }
-            }
-            if (inwin)
-              v = eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y);
-            else
-              v = eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
-          } else if (cl.kind == 2) {
-            const int L = __ldg(ch_len + cl.ch);
-            v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
-          }
-          // far cells: value and moment come from the far pass
-          if (cl.kind != 3) {
-            f[row0 + (size_t)u * g.nr] = v;
-            part += (T)__ldg(mt.bu + u) * v;
-          }
-        }
-      }
-      acc += (double)part;
-    }
-  }
+  strip_rows<T, WC, NW, PF>(win, x0, waits_ok, col_ok, j, r, w, Cj, f, idx, fx, fy, fp2,
+                            ch_start, ch_len, ch_val, ndrift, mt, g, acc);
   // extra: the grid has N_r / 32 blocks and N_r = 32 k + 1; the last block
   // also computes the last column from its strip (columns r0 - 8 .. r0 + 39
   // cover it), one row per thread, instead of a block of one column
@@ -1312,27 +1065,15 @@ __global__ void __launch_bounds__(32 * NW, MINB)
       T v = T(0);
       if (cl.kind == 0) {
         const int wc = cl.rI - x0;
-        bool inwin = waits_ok && wc >= 0 && wc <= WC - 4;
-        if (inwin) {
-          const int cb = (cl.uI + 3) / DS_ROWS;
-          while (ready <= cb) {
-            if (!mbar_wait_bounded(&bar[ready], 0u)) {
-              waits_ok = false;
-              inwin = false;
-              atomicOr(err, 1u);
-              break;
-            }
-            ++ready;
-          }
-        }
-        v = inwin ? eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y)
-                  : eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
+        v = (waits_ok && wc >= 0 && wc <= WC - 4)
+                ? eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y)
+                : eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
       } else if (cl.kind == 2) {
         const int L = __ldg(ch_len + cl.ch);
         v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
       }
       f[cell] = v;
-      acc2 += (double)((T)__ldg(mt.bu + u) * v);
+      acc2 += (double)(moment_bu<T>(mt, u) * v);
     }
   }
   // every box must have landed before the block's shared memory is released
@@ -1346,7 +1087,6 @@ __global__ void __launch_bounds__(32 * NW, MINB)
     double sum = 0.0;
 #pragma unroll
     for (int k = 0; k < NW; ++k) sum += red[k][lane];
-    if (farsum) sum += farsum[(size_t)j * g.nr + r];
     partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * sum;
   }
   if (xblock) {
@@ -1363,149 +1103,73 @@ __global__ void __launch_bounds__(32 * NW, MINB)
   }
 }
 
-// strip layouts: 48 (48 columns, 8 warps, two blocks per SM), 64 (64
-// columns, 16 warps, one block per SM), -48 (48 columns, 16 warps, two blocks
-// per SM), -49 (as -48, every box awaited before the first cell), 50 (48
-// columns, 32 warps, one block per SM), 51 (as 50, every box awaited first);
-// 0: none, the windowed kernel is used.  `want` != 0 asks for one layout,
-// returned only if it fits.  The default for FP32 storage is -49 where two
-// blocks fit (4 % faster than -48 on the 513 x 513 x 256 case: the other
-// block on the SM computes while this one's strip lands), else 51 where one
-// fits, else the windowed kernel; FP64 takes the windowed kernel (its strips
-// fit one block per SM only, which measured slower).
+// Strip layouts (the DRIFT_* kinds): DRIFT_STRIP2, 48 columns, 16 warps, two
+// blocks per SM; DRIFT_STRIP1, 48 columns, 32 warps, one block per SM;
+// DRIFT_WINDOW: none, the windowed kernel.  `want` != DRIFT_AUTO asks for
+// one kind, returned only if it fits (else DRIFT_WINDOW).  The default for
+// FP32 storage is DRIFT_STRIP2 where it fits (4 % faster than per-cell box
+// waits on the 513 x 513 x 256 case: the other block on the SM computes while
+// this one's strip lands), else DRIFT_STRIP1 (strips of up to 1028 rows:
+// 14 % faster than the windowed drift on 1025 x 1025 x 512), else the
+// windowed kernel; FP64 takes the windowed kernel (its strips fit one block
+// per SM only, which measured slower).
 template <typename T>
 int drift_strip_width(int nu, int want) {
   const int nch = (nu + 3 + DS_ROWS - 1) / DS_ROWS;
-  if (nch > 32) return 0;
+  if (nch > 32 || want == DRIFT_WINDOW) return DRIFT_WINDOW;
   auto dyn = [&](int wc) { return (size_t)nch * (DS_ROWS * wc * sizeof(T) + sizeof(uint64_t)); };
   // 228 KB of shared memory per SM, 1 KB of it reserved per block; at most
   // 227 KB per block; static reduction array NW x 32 doubles
-  const bool fit48x8 = 2 * (dyn(48) + 8 * 32 * 8 + 1024) <= 233472;
-  const bool fit48x16 = 2 * (dyn(48) + 16 * 32 * 8 + 1024) <= 233472;
-  const bool fit64 = dyn(64) + 16 * 32 * 8 <= 232448;
-  // one block of 32 warps per SM (strips of up to 1028 rows in FP32)
-  const bool fit48x32 = dyn(48) + 32 * 32 * 8 <= 232448;
-  if (want == 48) return fit48x8 ? 48 : 0;
-  if (want == 64) return fit64 ? 64 : 0;
-  if (want == -48) return fit48x16 ? -48 : 0;
-  if (want == -49) return fit48x16 ? -49 : 0;
-  if (want == 50) return fit48x32 ? 50 : 0;
-  if (want == 51) return fit48x32 ? 51 : 0;
-  if (sizeof(T) != 4) return 0;
-  // strips too tall for two blocks per SM (1025 rows) take one block of 32
-  // warps, every box awaited first: 14 % faster than the windowed drift on
-  // the 1025 x 1025 x 512 case (the per-cell waits of 50 gained nothing)
-  return fit48x16 ? -49 : fit48x32 ? 51 : 0;
+  const bool fit2 = 2 * (dyn(48) + 16 * 32 * 8 + 1024) <= 233472;
+  const bool fit1 = dyn(48) + 32 * 32 * 8 <= 232448;
+  if (want == DRIFT_STRIP2) return fit2 ? DRIFT_STRIP2 : DRIFT_WINDOW;
+  if (want == DRIFT_STRIP1) return fit1 ? DRIFT_STRIP1 : DRIFT_WINDOW;
+  if (sizeof(T) != 4) return DRIFT_WINDOW;
+  return fit2 ? DRIFT_STRIP2 : fit1 ? DRIFT_STRIP1 : DRIFT_WINDOW;
 }
 
-template <typename T, int WC, int NW, int MINB, bool WAITALL = false>
+template <typename T, int WC, int NW, int MINB>
 static cudaError_t drift_strip_go(const CUtensorMap *tmS, const T *C, T *f, const int32_t *idx,
                                   const T *fx, const T *fy, const uint2 *fp2,
                                   const int64_t *ch_start, const int32_t *ch_len,
                                   const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                                  double *partial, const double *farsum, unsigned int *err,
+                                  double *partial, unsigned int *err, uint32_t spins,
                                   const Geometry &g, cudaStream_t st) {
   const int nch = (g.nu + 3 + DS_ROWS - 1) / DS_ROWS;
   const size_t smem = (size_t)nch * DS_ROWS * WC * sizeof(T) + nch * sizeof(uint64_t);
-  cudaError_t e = cudaFuncSetAttribute(drift_strip_kernel<T, WC, NW, MINB, WAITALL>,
+  cudaError_t e = cudaFuncSetAttribute(drift_strip_kernel<T, WC, NW, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   // N_r = 32 k + 1 (every grid of the form 2^n + 1): k blocks, the last one
-  // also takes the last column (not with the far pass, whose far cells are
-  // defined by 32-column blocks); 2.4 % faster than a block of one column on
+  // also takes the last column; 2.4 % faster than a block of one column on
   // the 513 x 513 x 256 case
-  const int extra = (g.nr % 32 == 1 && g.nr > 32 && !farsum) ? 1 : 0;
+  const int extra = (g.nr % 32 == 1 && g.nr > 32) ? 1 : 0;
   const dim3 grid(extra ? g.nr / 32 : (g.nr + 31) / 32, g.nb);
-  drift_strip_kernel<T, WC, NW, MINB, WAITALL><<<grid, 32 * NW, smem, st>>>(
-      *tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val, ndrift, mt, partial, farsum, err,
+  drift_strip_kernel<T, WC, NW, MINB><<<grid, 32 * NW, smem, st>>>(
+      *tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val, ndrift, mt, partial, err, spins,
       extra, g);
   return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_drift_strip(const CUtensorMap *tmS, int width, const T *C, T *f,
+cudaError_t launch_drift_strip(const CUtensorMap *tmS, int kind, const T *C, T *f,
                                const int32_t *idx, const T *fx, const T *fy, const uint2 *fp2,
                                const int64_t *ch_start, const int32_t *ch_len,
                                const T *ch_val, int64_t ndrift, const MomentTables &mt,
-                               double *partial, const double *farsum, unsigned int *err,
+                               double *partial, unsigned int *err, uint32_t spins,
                                const Geometry &g, cudaStream_t st) {
-  switch (width) {
-    case 64:
-      return drift_strip_go<T, 64, 16, 1>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
-                                          ndrift, mt, partial, farsum, err, g, st);
-    case 48:
-      return drift_strip_go<T, 48, 8, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
-                                         ndrift, mt, partial, farsum, err, g, st);
-    case -49:  // -48 with every box awaited before the first cell
-      return drift_strip_go<T, 48, 16, 2, true>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len,
-                                                ch_val, ndrift, mt, partial, farsum, err, g, st);
-    case -48:
-      return drift_strip_go<T, 48, 16, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
-                                          ndrift, mt, partial, farsum, err, g, st);
-    case 50:  // 48 columns, 32 warps, one block per SM, per-cell box waits
-      return drift_strip_go<T, 48, 32, 1>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val,
-                                          ndrift, mt, partial, farsum, err, g, st);
-    case 51:  // 50 with every box awaited before the first cell
-      return drift_strip_go<T, 48, 32, 1, true>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len,
-                                                ch_val, ndrift, mt, partial, farsum, err, g, st);
+  switch (kind) {
+    case DRIFT_STRIP2:
+      return drift_strip_go<T, 48, 16, 2>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len,
+                                          ch_val, ndrift, mt, partial, err, spins, g, st);
+    case DRIFT_STRIP1:
+      return drift_strip_go<T, 48, 32, 1>(tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len,
+                                          ch_val, ndrift, mt, partial, err, spins, g, st);
     default:
       return cudaErrorInvalidValue;
   }
 }
 
-// ---------------------------------------------------------------- far pass
-// Cells of the FP32 strip layout whose taps leave their block's strip
-// columns (0.4 % of the cells of the 513 x 513 x 256 Hernquist case).  One
-// thread per far cell gathers it from C in global memory, writes f and its
-// moment term b_u f; a second pass sums each (slice, r column)'s terms in
-// row order into farsum, which the strip kernel's epilogue adds, so the
-// moment sums keep a fixed order.  Both run before the strip kernel on the
-// same stream; far_prod holds one term per far cell.
-__global__ void far_value_kernel(const float *__restrict__ C, float *__restrict__ f,
-                                 const uint32_t *__restrict__ far_cell,
-                                 const uint2 *__restrict__ far_w, int c_lo, int c_hi,
-                                 MomentTables mt, double *__restrict__ far_prod, Geometry g) {
-  const int c = c_lo + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (c >= c_hi) return;
-  const uint2 w = far_w[c];
-  const uint32_t cell = far_cell[c];
-  const uint32_t slice = (uint32_t)g.nr * (uint32_t)g.nu;
-  const int jl = (int)(cell / slice) - g.j0;
-  const int u = (int)((cell % slice) / (uint32_t)g.nr);
-  const float *Cj = C + (size_t)jl * (g.nu + 3) * g.pc;
-  const float v = eval2d<float>(Cj, g.pc, (int)(w.x >> FP_FBITS), frac21(w.x),
-                                (int)(w.y >> FP_FBITS), frac21(w.y));
-  f[cell] = v;
-  far_prod[c] = (double)((float)__ldg(mt.bu + u) * v);
-}
-
-__global__ void far_sum_kernel(const int32_t *__restrict__ far_col,
-                               const double *__restrict__ far_prod,
-                               double *__restrict__ farsum, Geometry g) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= (int64_t)g.nb * g.nr) return;
-  const size_t col = (size_t)g.j0 * g.nr + (size_t)t;
-  const int c0 = far_col[col], c1 = far_col[col + 1];
-  double acc = 0.0;
-#pragma unroll 4
-  for (int c = c0; c < c1; ++c) acc += far_prod[c];
-  farsum[col] = acc;
-}
-
-cudaError_t launch_far_drift(const float *C, float *f, const uint32_t *far_cell,
-                             const uint2 *far_w, const int32_t *far_col, int c_lo, int c_hi,
-                             const MomentTables &mt, double *far_prod, double *farsum,
-                             const Geometry &g, cudaStream_t st) {
-  if (c_hi > c_lo)
-    far_value_kernel<<<(unsigned)((c_hi - c_lo + 127) / 128), 128, 0, st>>>(
-        C, f, far_cell, far_w, c_lo, c_hi, mt, far_prod, g);
-  const int64_t n = (int64_t)g.nb * g.nr;
-  far_sum_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(far_col, far_prod, farsum, g);
-  return cudaGetLastError();
-}
-
-// tails: chains are independent; the tail slot (ndrift+L-1) mod L differs
-// from the front slot read by the drift since every chain has L >= 2
 template <typename T>
 __global__ void chain_tail_kernel(const T *__restrict__ C, T *__restrict__ ch_val,
                                   const int64_t *__restrict__ ch_start,
@@ -1608,7 +1272,8 @@ __global__ void __launch_bounds__(SC_THREADS)
     scan_kernel(const double *__restrict__ partial, MomentTables mt,
                 double *__restrict__ T2, double *__restrict__ bins,
                 double *__restrict__ Mr, double *__restrict__ shift,
-                double *__restrict__ mtot, unsigned int *count, Geometry g) {
+                double *__restrict__ mtot, unsigned int *count, unsigned int *status,
+                Geometry g) {
   __shared__ dd sh[SC_THREADS];
   __shared__ bool last;
   const int tid = threadIdx.x;
@@ -1669,7 +1334,13 @@ __global__ void __launch_bounds__(SC_THREADS)
       if (lane >= d) xi = dd_add(xi, o);
     }
     wsum[lane] = dd_add(xi, dd{-x.hi, -x.lo});  // exclusive
-    if (lane == 31) *mtot = xi.hi + xi.lo;
+    if (lane == 31) {
+      const double total = xi.hi + xi.lo;
+      *mtot = total;
+      // every cell enters the mass with a positive weight, so a NaN or an
+      // infinity anywhere in f makes the total non-finite
+      if (!isfinite(total)) atomicOr(status, 2u);
+    }
   }
   __syncthreads();
   dd ex = dd_add(wsum[wid], dd_add(inc, dd{-loc.hi, -loc.lo}));
@@ -1687,12 +1358,12 @@ __global__ void __launch_bounds__(SC_THREADS)
 
 cudaError_t launch_scan(const double *partial, const MomentTables &mt,
                         double *T2, double *bins, double *Mr, double *shift,
-                        double *mtot, unsigned int *count, const Geometry &g,
-                        cudaStream_t st) {
+                        double *mtot, unsigned int *count, unsigned int *status,
+                        const Geometry &g, cudaStream_t st) {
   if (g.nr > 2 * SC_THREADS) return cudaErrorInvalidValue;
   const unsigned blocks = (g.nr + SC_RB - 1) / SC_RB;
   scan_kernel<<<blocks, SC_THREADS, 0, st>>>(partial, mt, T2, bins, Mr, shift, mtot,
-                                             count, g);
+                                             count, status, g);
   return cudaGetLastError();
 }
 
@@ -1821,17 +1492,13 @@ cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
   template cudaError_t launch_drift_strip<T>(                                   \
       const CUtensorMap *, int, const T *, T *, const int32_t *, const T *, const T *, \
       const uint2 *, const int64_t *, const int32_t *, const T *, int64_t,       \
-      const MomentTables &, double *, const double *, unsigned int *, const Geometry &, \
+      const MomentTables &, double *, unsigned int *, uint32_t, const Geometry &, \
       cudaStream_t);                                                            \
   template cudaError_t launch_drift_tma<T>(                                     \
       const CUtensorMap *, const T *, T *, const int32_t *, const T *, const T *, \
       const uint2 *, const int64_t *, const int32_t *, const T *, int64_t,        \
-      const MomentTables &, double *, unsigned int *, const Geometry &,          \
+      const MomentTables &, double *, unsigned int *, uint32_t, const Geometry &, \
       cudaStream_t);                                                            \
-  template cudaError_t launch_drift<T>(                                         \
-      const T *, T *, const int32_t *, const T *, const T *, const uint2 *,      \
-      const int64_t *, const int32_t *, const T *, int64_t,                     \
-      const MomentTables &, double *, const Geometry &, cudaStream_t);          \
   template cudaError_t launch_chain_tails<T>(                                   \
       const T *, T *, const int64_t *, const int32_t *, const int32_t *,         \
       const double *, const double *, int64_t, int64_t, int64_t, int64_t,       \

@@ -19,7 +19,17 @@
 // The device address of the array is looked up once per device, with that
 // device current, on the first call on that device (cudaGetSymbolAddress).
 // That first call therefore should come before any stream capture is begun
-// on the device.
+// on the device.  The address belongs to the device's current context: after
+// cudaDeviceReset the next call on that device finds a new context (by its
+// context id) and looks the address up again.
+//
+// Every call copies the coordinate arrays R, U, J and JV from host memory
+// into the scratch array with cudaMemcpyAsync on the caller's stream.
+//
+// Error messages are kept per host thread (vls_noalloc_last_error returns the
+// message of the calling thread's last failed call).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -58,7 +68,8 @@ namespace {
 
 std::mutex g_na_mutex;
 double *g_na_ptr[NA_MAX_DEVICES] = {nullptr};
-std::string g_na_error;
+unsigned long long g_na_ctx[NA_MAX_DEVICES] = {0};  // context id the address belongs to
+thread_local std::string g_na_error;
 
 int na_fail(int code, const std::string &m) {
   g_na_error = m;
@@ -174,19 +185,47 @@ __global__ void __launch_bounds__(1024)
   }
 }
 
-// device address of the scratch array on `device` (looked up once, with the
-// device current)
+// id of the context current on this thread (0 if it cannot be read); the
+// driver calls are reached through the runtime, without a libcuda link
+unsigned long long current_ctx_id() {
+  static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+    fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(fn);
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
+
+// device address of the scratch array on `device`: looked up with the device
+// current on the first call, and again when the device's context has changed
+// (cudaDeviceReset)
 int scratch_on(int device, double **out) {
   if (device < 0 || device >= NA_MAX_DEVICES)
     return na_fail(VLS_EINVAL, "device ordinal out of range");
+  const unsigned long long ctx = current_ctx_id();
   std::lock_guard<std::mutex> lk(g_na_mutex);
-  if (!g_na_ptr[device]) {
+  if (!g_na_ptr[device] || ctx == 0 || ctx != g_na_ctx[device]) {
     double *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return na_fail(VLS_ECUDA, std::string("cudaGetSymbolAddress of the no-alloc scratch: ") +
                                     cudaGetErrorString(e));
     g_na_ptr[device] = p;
+    g_na_ctx[device] = ctx;
   }
   *out = g_na_ptr[device];
   return VLS_OK;

@@ -54,8 +54,6 @@ __host__ __device__ constexpr int rc_maxs() {
   return 2 + (C::NT / 32 - 1) * C::CPW;
 }
 // configuration ids (host and device agree on the order)
-using CfgA = RcCfg<31, 16, 320, 2>;   // 31-row chunks, 16 lines, two blocks per SM
-using CfgA1 = RcCfg<31, 16, 576, 1>;  // the same for up to 35 chunks
 using CfgB = RcCfg<15, 8, 320, 3>;    // 15-row chunks, 8 lines, three blocks per SM
 using CfgB1 = RcCfg<15, 8, 640, 1>;   // the same for up to 77 chunks
 using CfgC = RcCfg<15, 16, 576, 2>;   // 15-row chunks, 16 lines, two blocks per SM
@@ -875,11 +873,7 @@ cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
       al16(2 * (size_t)tr.S * CF::LN * sizeof(R)) +
       (size_t)CF::LN * rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), CF::LN) * sizeof(T);
   if constexpr (rc_bulk_rows<CF>()) {
-    static const bool pipe = [] {
-      const char *e = std::getenv("VLS_PRER_PIPE");
-      return !(e && std::string(e) == "0");
-    }();
-    if (pipe) {
+    {
       // persistent blocks, as many as fit on the device at once
       const size_t psmem = al16(2 * (size_t)tr.S * CF::LN * sizeof(R)) +
                            (size_t)RC_PIPE_TILES * CF::LN *
@@ -1274,33 +1268,28 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
     for (int k = threadIdx.x; k < N; k += blockDim.x) Gs[(size_t)p * g.nr + k] = tile[p * P + 1 + k];
 }
 
-using CfgAdjU = RcCfg<15, 16, 576, 1>;
+// u lines: 15-row chunks in 8-line blocks (up to 72 chunks; 12 % faster than
+// 16-line blocks on 513-row lines); r lines: 15-row chunks in 8-line blocks,
+// and lines too long for those in blocks of up to 80 chunks (1025-row lines)
+using CfgAdjU = RcCfg<15, 8, 576, 1>;
 using CfgAdjR = RcCfg<15, 8, 320, 2>;
-// lines too long for those (up to 70 and 78 chunks: 1025-row lines)
-using CfgAdjU2 = RcCfg<15, 8, 576, 1>;
 using CfgAdjR2 = RcCfg<15, 8, 640, 1>;
 
 }  // namespace
 
 // ------------------------------------------------------------- host side
 // configuration for one direction (u_lines: the ucol kernel's columns, else
-// the prer kernel's rows): `pref` "A", "B", "C", "D", "F" or "I" (31-row
-// chunks of 16 lines; 15-row chunks of 8 lines; 15-row chunks of 16 lines;
-// 23-row chunks of 8 lines; 19-row chunks of 8 lines; 17-row chunks of 16
-// lines) or empty for the default; -1 when no configuration takes the shape
+// the prer kernel's rows), -1 when no configuration takes the shape (the
+// shared-memory segment kernels then solve the lines).  Ids: 2 = B (15-row
+// chunks, 8 lines), 3 = B1 (the same, one block per SM), 4 = C (15-row, 16
+// lines), 5 = D (23-row, 8 lines), 6 = F (19-row, 8 lines), 7 = I (17-row,
+// 16 lines).
 template <typename R>
-int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
+int rc_config(const HostDirTables &t, bool u_lines) {
   const int N = t.M - 2;
   const int kc = sizeof(R) == 8 ? t.kc64 : t.kc32;
-  const std::string p = pref ? pref : "";
   const int b = cfg2_fits<CfgB>(N, kc) ? 2 : cfg2_fits<CfgB1>(N, kc) ? 3 : -1;
-  if (p == "A") return cfg2_fits<CfgA>(N, kc) ? 0 : cfg2_fits<CfgA1>(N, kc) ? 1 : -1;
-  if (p == "B") return b;
-  if (p == "C") return cfg2_fits<CfgC>(N, kc) ? 4 : -1;
-  if (p == "D") return cfg2_fits<CfgD>(N, kc) ? 5 : -1;
-  if (p == "F") return cfg2_fits<CfgF>(N, kc) ? 6 : -1;
-  if (p == "I") return cfg2_fits<CfgI>(N, kc) ? 7 : -1;
-  // default (fastest measured on 513 x 513 x 256): 16-line blocks of 17-row
+  // the fastest measured on 513 x 513 x 256: 16-line blocks of 17-row
   // chunks for the u lines (15, 19 and 23 rows measured 1 %, 3 % and 28 %
   // slower), 8-line blocks of 19-row chunks for the r lines (prer 0.142 ->
   // 0.120 ms against 15-row chunks; 17 and 21 rows 0.130 and 0.128 ms);
@@ -1317,9 +1306,6 @@ int rc_config(const HostDirTables &t, const char *pref, bool u_lines) {
 
 static int cfg_L(int cfg) {
   switch (cfg) {
-    case 0:
-    case 1:
-      return CfgA::L;
     case 5:
       return CfgD::L;
     case 6:
@@ -1389,8 +1375,6 @@ cudaError_t launch_ucol_rc(int cfg, bool kick, const T *f, T *G, const double *s
     return kick ? ucol_rc_go<T, R, true, CF>(f, G, shift, g, tu, st)            \
                 : ucol_rc_go<T, R, false, CF>(f, G, shift, g, tu, st);
   switch (cfg) {
-    VLS_UCOL_CFG(0, CfgA)
-    VLS_UCOL_CFG(1, CfgA1)
     VLS_UCOL_CFG(2, CfgB)
     VLS_UCOL_CFG(3, CfgB1)
     VLS_UCOL_CFG(4, CfgC)
@@ -1407,10 +1391,6 @@ template <typename T, typename R>
 cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
                            unsigned int *err, cudaStream_t st) {
   switch (cfg) {
-    case 0:
-      return prer_rc_go<T, R, CfgA>(G, C, g, tr, err, st);
-    case 1:
-      return prer_rc_go<T, R, CfgA1>(G, C, g, tr, err, st);
     case 2:
       return prer_rc_go<T, R, CfgB>(G, C, g, tr, err, st);
     case 3:
@@ -1428,21 +1408,10 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
   }
 }
 
-// adjoint line kernels (FP64): u lines with 15-row chunks in 8-line blocks
-// (up to 70 chunks; 12 % faster than 16-line blocks on 513-row lines), r
-// lines with 15-row chunks of 8 lines and lines too long for those in
-// 8-line blocks of up to 78 chunks.  VLS_ADJ_RC=long takes the long-line r
-// layout for every length, VLS_ADJ_RC=short the 16-line u layout where it
-// fits (read at each launch, for tests); tables from rc_dir<double>(t, 2)
-static int adj_rc_forced() {
-  const char *e = std::getenv("VLS_ADJ_RC");
-  if (!e) return 0;
-  const std::string v(e);
-  return v == "long" ? 1 : v == "short" ? 2 : 0;
-}
+// adjoint line kernels (FP64), layouts CfgAdjU / CfgAdjR / CfgAdjR2; tables
+// from rc_dir<double>(t, 2)
 bool rc_adj_supported(const HostDirTables &tu, const HostDirTables &tr) {
-  return tu.M - 2 > CfgAdjU::L && tr.M - 2 > CfgAdjR::L &&
-         (cfg_fits<CfgAdjU>(tu.M - 2, tu.kc64) || cfg_fits<CfgAdjU2>(tu.M - 2, tu.kc64)) &&
+  return tu.M - 2 > CfgAdjU::L && tr.M - 2 > CfgAdjR::L && cfg_fits<CfgAdjU>(tu.M - 2, tu.kc64) &&
          (cfg_fits<CfgAdjR>(tr.M - 2, tr.kc64) || cfg_fits<CfgAdjR2>(tr.M - 2, tr.kc64));
 }
 
@@ -1467,9 +1436,7 @@ template <typename T>
 cudaError_t launch_ucol_adj_rc(const T *f, const double *Gb, double *lam, double *sbar,
                                const double *shift, const Geometry &g, const RcDir<double> &tu,
                                cudaStream_t st) {
-  if (tu.S <= rc_maxs<CfgAdjU>() && adj_rc_forced() == 2)
-    return ucol_adj_go<T, CfgAdjU>(f, Gb, lam, sbar, shift, g, tu, st);
-  return ucol_adj_go<T, CfgAdjU2>(f, Gb, lam, sbar, shift, g, tu, st);
+  return ucol_adj_go<T, CfgAdjU>(f, Gb, lam, sbar, shift, g, tu, st);
 }
 
 template <class CF>
@@ -1490,8 +1457,7 @@ static cudaError_t prer_adj_go(const double *Cb, double *Gb, const Geometry &g,
 
 cudaError_t launch_prer_adj_rc(const double *Cb, double *Gb, const Geometry &g,
                                const RcDir<double> &tr, cudaStream_t st) {
-  if (tr.S <= rc_maxs<CfgAdjR>() && adj_rc_forced() != 1)
-    return prer_adj_go<CfgAdjR>(Cb, Gb, g, tr, st);
+  if (tr.S <= rc_maxs<CfgAdjR>()) return prer_adj_go<CfgAdjR>(Cb, Gb, g, tr, st);
   return prer_adj_go<CfgAdjR2>(Cb, Gb, g, tr, st);
 }
 
@@ -1511,8 +1477,9 @@ template cudaError_t launch_ucol_adj_rc<double>(const double *, const double *, 
 VLS_RC_INST(double, double)
 VLS_RC_INST(float, double)
 VLS_RC_INST(float, float)
-template int rc_config<double>(const HostDirTables &, const char *, bool);
-template int rc_config<float>(const HostDirTables &, const char *, bool);
+template int rc_config<double>(const HostDirTables &, bool);
+template int rc_config<float>(const HostDirTables &, bool);
+int rc_chunk_rows(int cfg) { return cfg < 0 ? 0 : cfg_L(cfg); }
 template RcDir<double> rc_dir<double>(const HostDirTables &, int);
 template RcDir<float> rc_dir<float>(const HostDirTables &, int);
 

@@ -222,7 +222,8 @@ double Profile::value(double r, double u, double j) const {
 
 // --------------------------------------------------------------- drifts
 void advance_particle_drift(double R, double U, double J, double dt, double R0,
-                            double *outR, double *outU) {
+                            double *outR, double *outU, bool *halted) {
+  if (halted) *halted = false;
   double H0 = 0.5 * (U * U + (J * J) / (R * R));
   double sgn = (U <= 0) ? -1 : 1;
   double deltaT = dt;
@@ -271,8 +272,11 @@ void advance_particle_drift(double R, double U, double J, double dt, double R0,
     deltaT -= tlim;
     tR0 -= tlim;
     tlim = 10 * dt;
-    // the reference terminates the process when tR0 < deltaT here
-    // (vlasovSolver21.hxx:389-391, reflective kernel only); the step carries on
+    // the reference terminates the process here when tR0 < deltaT
+    // (vlasovSolver21.hxx:389-391): a particle inside the reflection radius R0
+    // (reflective kernel with kernelBufferSize > 0) whose backward orbit
+    // reaches R0 after its pericentre.  The caller turns that into an error.
+    if (tR0 < deltaT && halted) *halted = true;
   }
   newR = std::sqrt(std::pow(std::fabs(newR * newU) - 2 * sgn * H0 * deltaT, 2) +
                    J * J) *
@@ -311,12 +315,15 @@ void slice_footpoints(const Coords &c, int j, double dt_disp, bool reflective,
   fp.driftR.resize(n);
   fp.driftU.resize(n);
   fp.out.resize(n);
+  fp.halted = -1;
   const double J = c.J[j];
   for (int u = 0; u < c.nu; u++)
     for (int r = 0; r < c.nr; r++) {
       const size_t i = (size_t)u * c.nr + r;
       double dR, dU;
-      advance_particle_drift(c.R[r], c.U[u], J, dth, R0, &dR, &dU);
+      bool halted = false;
+      advance_particle_drift(c.R[r], c.U[u], J, dth, R0, &dR, &dU, &halted);
+      if (halted && fp.halted < 0) fp.halted = (int64_t)i;
       fp.driftR[i] = dR;
       fp.driftU[i] = dU;
       fp.out[i] = ((dR >= c.R.back()) || (dR <= c.R.front()) ||

@@ -48,9 +48,11 @@ struct Profile {
   double value(double r, double u, double j) const;
 };
 
-// vlasovSolver21::advanceParticleDrift (vlasovSolver21.hxx:328-408)
+// vlasovSolver21::advanceParticleDrift (vlasovSolver21.hxx:328-408).
+// *halted (may be NULL) is set where the reference terminates the process
+// (:389-391, reachable with a reflection radius R0 > 0 only).
 void advance_particle_drift(double R, double U, double J, double dt, double R0,
-                            double *outR, double *outU);
+                            double *outR, double *outU, bool *halted = nullptr);
 
 // footpoints of one J slice: integer/fraction pairs as decomposeDisplacement
 // produces them, the outside flag, and driftR
@@ -58,6 +60,7 @@ struct SliceFootpoints {
   std::vector<int32_t> rI, uI;
   std::vector<double> rF, uF, driftR, driftU;
   std::vector<uint8_t> out;
+  int64_t halted = -1;  // first cell (in the slice) where the reference halts, or -1
 };
 void slice_footpoints(const Coords &c, int j, double dt_disp, bool reflective,
                       SliceFootpoints &fp);

@@ -181,10 +181,13 @@ class VlasovSolver21Spline:
 
     precision: "fp64" (every value FP64) or "fp32" (FP32 f, coefficients and
     gathers; FP64 recursions, indexing, moments and statistics).
+    layout: kernel layouts (vls_layout_desc), None for the defaults: a dict
+    with any of prefilter ("auto", "segment"), drift ("auto", "window",
+    "strip2", "strip1"), slices_per_batch, streams, drift_wait_spins.
     """
 
     def __init__(self, cfg: Config | ParamsParser | dict, precision: str = "fp64",
-                 device: int = 0, init: bool = True):
+                 device: int = 0, init: bool = True, layout: dict | None = None):
         L = _lib.load()
         if isinstance(cfg, ParamsParser):
             cfg = config_from_params(cfg)
@@ -196,7 +199,20 @@ class VlasovSolver21Spline:
         gd, sd, idesc = _descs(cfg, precision, device)
         self._init_desc = idesc
         h = ctypes.c_void_p()
-        _lib.check(L.vls_create(ctypes.byref(gd), ctypes.byref(sd), ctypes.byref(h)))
+        lay = None
+        if layout:
+            lay = _lib.LayoutDesc()
+            for k, v in layout.items():
+                if k == "prefilter":
+                    v = _lib.PREFILTERS[v]
+                elif k == "drift":
+                    v = _lib.DRIFTS[v]
+                elif k not in ("slices_per_batch", "streams", "drift_wait_spins"):
+                    raise ValueError(f"unknown layout field '{k}'")
+                setattr(lay, k, int(v))
+        _lib.check(L.vls_create_layout(ctypes.byref(gd), ctypes.byref(sd),
+                                       ctypes.byref(lay) if lay is not None else None,
+                                       ctypes.byref(h)))
         self._h = h
         nr, nu, nj = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         L.vls_dims(h, ctypes.byref(nr), ctypes.byref(nu), ctypes.byref(nj))
@@ -206,6 +222,17 @@ class VlasovSolver21Spline:
         self.mass_before = None
         if init:
             self.init_profile()
+
+    def layout(self) -> dict:
+        """The kernel layouts this solver uses (vls_get_layout)."""
+        d = _lib.LayoutDesc()
+        self._ck(self._L.vls_get_layout(self._h, ctypes.byref(d)))
+        pre = {v: k for k, v in _lib.PREFILTERS.items()}
+        drift = {v: k for k, v in _lib.DRIFTS.items()}
+        return dict(prefilter=pre[d.prefilter], drift=drift[d.drift],
+                    slices_per_batch=d.slices_per_batch, streams=d.streams,
+                    drift_wait_spins=d.drift_wait_spins, u_chunk_rows=d.u_chunk_rows,
+                    r_chunk_rows=d.r_chunk_rows)
 
     # -- life cycle -------------------------------------------------------
     def close(self):
