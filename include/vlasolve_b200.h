@@ -316,6 +316,100 @@ int vls_adjoint_set_inner(vls_handle *h, int32_t inner_every);
 int vls_device_bytes(vls_handle *h, size_t *bytes);
 int vls_adjoint_inner_used(vls_handle *h, int32_t *inner_every);
 
+/* ---------------------------------------------------------------------------
+   Spline level.  localSpline<2, double> (localSpline.hxx:60-503) is the
+   reference's 2D cubic B-spline: init(initT), assign(data), build(),
+   evaluateC, evaluateNxPy, evaluate, pos2Coord.  A vls_spline2d is a batch of
+   nslices such splines on one GPU, built by the step's prefilter kernels and
+   evaluated at batches of points; positions are decomposed into (index,
+   fraction) on the host in FP64 (pos2Coord), so indices are the reference's
+   bit for bit.  Only the natural boundary condition (the one the step's
+   splines use) is built; other boundary types return VLS_EINVAL.  Points
+   whose indices lie outside [0, dim) return VLS_EINVAL (the reference reads
+   outside its buffer there). */
+/* localSpline::boundaryTypeV, localSpline.hxx:34 */
+enum { VLS_BC_PERIODIC = 0, VLS_BC_FLAT = 1, VLS_BC_NATURAL = 2, VLS_BC_SUPRA_NATURAL = 3,
+       VLS_BC_NOT_A_KNOT = 4, VLS_BC_LOCAL = 5 };
+/* localSpline::initT (localSpline.hxx:39-46), dimension 0 fastest in the data;
+   vlType: 1 = values at vertices (VERTEX), 0 = at cell centres (CELL);
+   precision VLS_FP64 or VLS_FP32_BULK (FP32 storage, FP64 solves) */
+typedef struct {
+  double start[2], stop[2];
+  int32_t N[2];
+  int32_t scaleType[2];
+  int32_t vlType[2];
+  int32_t bCond[2][2];
+  int32_t precision;
+  int32_t device;
+} vls_spline2d_desc;
+typedef struct vls_spline2d vls_spline2d;
+/* localSpline::init: value counts dim0, dim1 from genScale, start / step_inv
+   in rescaled coordinates (vls_spline2d_scale), device buffers of nslices */
+int vls_spline2d_create(const vls_spline2d_desc *desc, int64_t nslices, vls_spline2d **out);
+int vls_spline2d_destroy(vls_spline2d *s);
+int vls_spline2d_dims(const vls_spline2d *s, int32_t *dim0, int32_t *dim1, int64_t *nslices);
+int vls_spline2d_scale(const vls_spline2d *s, double *start, double *step_inv);
+/* localSpline::assign (localSpline.hxx:205-246): host FP64 values
+   [slice][dim1][dim0] of every slice */
+int vls_spline2d_assign(vls_spline2d *s, const double *data, int64_t nslices);
+/* localSpline::build / create_2D (localSpline.hxx:248-260, :1238-1258) */
+int vls_spline2d_build(vls_spline2d *s);
+/* the padded coefficients of one slice as localSpline's buffer holds them
+   (localSpline.hxx:222): (dim0+2) x (dim1+2) FP64, dim0 fastest */
+int vls_spline2d_coefficients(vls_spline2d *s, int64_t slice, double *coef);
+/* localSpline::pos2Coord (localSpline.hxx:352-358) of n positions along dir */
+int vls_spline2d_pos2coord(const vls_spline2d *s, int32_t dir, int64_t n, const double *p,
+                           int32_t *I, double *F);
+/* localSpline::evaluateC(int, double, int, double) (localSpline.hxx:381-398),
+   evaluateNxPy (:423-441) and evaluate(double, double) (:477-488) at n points;
+   slice (n entries) may be NULL for slice 0 */
+int vls_spline2d_evaluate_c(vls_spline2d *s, int64_t n, const int64_t *slice, const int32_t *Nx,
+                            const double *x, const int32_t *Ny, const double *y, double *v);
+int vls_spline2d_evaluate_nxpy(vls_spline2d *s, int64_t n, const int64_t *slice,
+                               const int32_t *Nx, const double *yy, double *v);
+int vls_spline2d_evaluate(vls_spline2d *s, int64_t n, const int64_t *slice, const double *xx,
+                          const double *yy, double *v);
+/* message of the last failed call on s (or of the last create failure when
+   s is NULL, per host thread) */
+const char *vls_spline2d_last_error(const vls_spline2d *s);
+
+/* interpolSpline<double> (interpol_spline.hxx:9-189), the reference's
+   einspline-backed interface (third-party einspline, not vendored, compiled
+   out by the reference's build).  Boundary codes are einspline's bc_code
+   values the reference passes through (:23-27); natural ends (NATURAL, or
+   DERIV2 with value 0) are built, others return VLS_EINVAL.  Grids in
+   rescaled coordinates, the last node nudged by 1e-10 of a cell as createInit
+   does. */
+enum { VLS_EBC_PERIODIC = 0, VLS_EBC_DERIV1 = 1, VLS_EBC_DERIV2 = 2, VLS_EBC_FLAT = 3,
+       VLS_EBC_NATURAL = 4, VLS_EBC_ANTIPERIODIC = 5 };
+/* interpolSpline::initT (:33-39) */
+typedef struct {
+  double xstart, xend, ystart, yend;
+  int32_t nx, ny;
+  int32_t xbc[2], ybc[2];
+  double xbcv[2], ybcv[2];
+  int32_t xscaleType, yscaleType;
+  int32_t rescaleNeeded, useLog;
+} vls_interp_init;
+typedef struct vls_interp vls_interp;
+/* interpolSpline::createInit (:49-91) */
+int vls_interp_create_init(double xstart, double xstop, int32_t Nx, double ystart,
+                           double ystop, int32_t Ny, int32_t xbctL, int32_t xbctR,
+                           int32_t ybctL, int32_t ybctR, int32_t xscaleType,
+                           int32_t yscaleType, int32_t vltype, int32_t useLog, double xbcvL,
+                           double xbcvR, double ybcvL, double ybcvR, vls_interp_init *out);
+/* interpolSpline::create (:93-110): data ny x nx, x fastest */
+int vls_interp_create(const vls_interp_init *ini, const double *data, int32_t device,
+                      vls_interp **out);
+/* interpolSpline::evaluate (:112-183) at n points: v; g (2 per point: dv/dy,
+   dv/dx) and h (4 per point: yy, yx, xy, xx) when not NULL, in rescaled
+   coordinates; points are clamped to the grid */
+int vls_interp_evaluate(vls_interp *s, int64_t n, const double *x, const double *y, double *v,
+                        double *g, double *h);
+/* interpolSpline::destroy (:185-189) */
+int vls_interp_destroy(vls_interp *s);
+const char *vls_interp_last_error(const vls_interp *s);
+
 /* Radial moment of a grid that already lives in device memory, without any
    allocation (no counterpart in the reference, whose grid is host memory).
    For callers that own all device memory and must not let a library call

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "vlasolve_b200.h"
@@ -257,6 +258,137 @@ class vlasovSolver21_spline {
   vls_solver_desc solver_;
   double mass_before_ = 0;
   size_t nr_ = 0, nu_ = 0, nj_ = 0;
+};
+
+// localSpline<2, double> (localSpline.hxx:60-503) over a vls_spline2d of
+// one or more slices: init(initT), assign(data), build(), evaluateC,
+// evaluateNxPy, evaluate and pos2Coord with the reference's signatures (one
+// point, slice 0), plus batched forms over arrays of points.
+class localSpline2 {
+ public:
+  // localSpline::boundaryTypeV / initT (localSpline.hxx:34-46)
+  struct initT {
+    double start[2], stop[2];
+    int N[2];
+    int scaleType[2];  // VLS_SCALE_*
+    int vlType[2];     // 1 VERTEX, 0 CELL
+    int bCond[2][2];   // VLS_BC_NATURAL
+  };
+  localSpline2() = default;
+  explicit localSpline2(const initT &ini, int64_t nslices = 1, int precision = VLS_FP64,
+                        int device = 0) {
+    init(ini, nslices, precision, device);
+  }
+  localSpline2(const localSpline2 &) = delete;
+  localSpline2 &operator=(const localSpline2 &) = delete;
+  ~localSpline2() { vls_spline2d_destroy(s_); }
+
+  void init(const initT &ini, int64_t nslices = 1, int precision = VLS_FP64, int device = 0) {
+    vls_spline2d_destroy(s_);
+    s_ = nullptr;
+    vls_spline2d_desc d{};
+    for (int k = 0; k < 2; ++k) {
+      d.start[k] = ini.start[k];
+      d.stop[k] = ini.stop[k];
+      d.N[k] = ini.N[k];
+      d.scaleType[k] = ini.scaleType[k];
+      d.vlType[k] = ini.vlType[k];
+      d.bCond[k][0] = ini.bCond[k][0];
+      d.bCond[k][1] = ini.bCond[k][1];
+    }
+    d.precision = precision;
+    d.device = device;
+    const int rc = vls_spline2d_create(&d, nslices, &s_);
+    if (rc != VLS_OK) throw error(rc, vls_spline2d_last_error(nullptr));
+    vls_spline2d_dims(s_, &dim_[0], &dim_[1], &ns_);
+  }
+  // values of every slice, [slice][dim1][dim0]
+  void assign(const double *data) { ck(vls_spline2d_assign(s_, data, ns_)); }
+  void build() { ck(vls_spline2d_build(s_)); }
+  std::pair<int, double> pos2Coord(double p, int dir) const {
+    int32_t I = 0;
+    double F = 0;
+    ck(vls_spline2d_pos2coord(s_, dir, 1, &p, &I, &F));
+    return {I, F};
+  }
+  double evaluateC(int Nx, double x, int Ny, double y) {
+    double v = 0;
+    const int32_t nx = Nx, ny = Ny;
+    ck(vls_spline2d_evaluate_c(s_, 1, nullptr, &nx, &x, &ny, &y, &v));
+    return v;
+  }
+  double evaluateNxPy(int Nx, double yy) {
+    double v = 0;
+    const int32_t nx = Nx;
+    ck(vls_spline2d_evaluate_nxpy(s_, 1, nullptr, &nx, &yy, &v));
+    return v;
+  }
+  double evaluate(double xx, double yy) {
+    double v = 0;
+    ck(vls_spline2d_evaluate(s_, 1, nullptr, &xx, &yy, &v));
+    return v;
+  }
+  // batched: n points on the given slices (slice may be null: slice 0)
+  void evaluate(int64_t n, const int64_t *slice, const double *xx, const double *yy, double *v) {
+    ck(vls_spline2d_evaluate(s_, n, slice, xx, yy, v));
+  }
+  void evaluateC(int64_t n, const int64_t *slice, const int32_t *Nx, const double *x,
+                 const int32_t *Ny, const double *y, double *v) {
+    ck(vls_spline2d_evaluate_c(s_, n, slice, Nx, x, Ny, y, v));
+  }
+  std::vector<double> coefficients(int64_t slice = 0) {
+    std::vector<double> c((size_t)(dim_[0] + 2) * (dim_[1] + 2));
+    ck(vls_spline2d_coefficients(s_, slice, c.data()));
+    return c;
+  }
+  int dim(int k) const { return dim_[k]; }
+
+ private:
+  void ck(int rc) const {
+    if (rc != VLS_OK) throw error(rc, vls_spline2d_last_error(s_));
+  }
+  vls_spline2d *s_ = nullptr;
+  int32_t dim_[2] = {0, 0};
+  int64_t ns_ = 0;
+};
+
+// interpolSpline<double> (interpol_spline.hxx:9-189): static createInit,
+// create, evaluate (value; value and gradient; value, gradient and
+// Hessian) and destroy, as the reference's einspline wrapper declares them.
+struct interpolSpline {
+  typedef vls_interp_init initT;
+  typedef vls_interp interpT;
+  static initT createInit(double xstart, double xstop, int Nx, double ystart, double ystop,
+                          int Ny, int xbctL, int xbctR, int ybctL, int ybctR, int xscaleType,
+                          int yscaleType, int vltype, bool useLog = false, double xbcvL = 0,
+                          double xbcvR = 0, double ybcvL = 0, double ybcvR = 0) {
+    initT g{};
+    const int rc = vls_interp_create_init(xstart, xstop, Nx, ystart, ystop, Ny, xbctL, xbctR,
+                                          ybctL, ybctR, xscaleType, yscaleType, vltype,
+                                          useLog ? 1 : 0, xbcvL, xbcvR, ybcvL, ybcvR, &g);
+    if (rc != VLS_OK) throw error(rc, vls_interp_last_error(nullptr));
+    return g;
+  }
+  static interpT *create(initT &ini, const double *data, int device = 0) {
+    interpT *s = nullptr;
+    const int rc = vls_interp_create(&ini, data, device, &s);
+    if (rc != VLS_OK) throw error(rc, vls_interp_last_error(nullptr));
+    return s;
+  }
+  static void evaluate(interpT *s, double x, double y, double *v) { ck(s, x, y, v, 0, 0); }
+  static void evaluate(interpT *s, double x, double y, double *v, double *g) {
+    ck(s, x, y, v, g, 0);
+  }
+  static void evaluate(interpT *s, double x, double y, double *v, double *g, double *h) {
+    ck(s, x, y, v, g, h);
+  }
+  static void destroy(interpT *s) { vls_interp_destroy(s); }
+
+ private:
+  static void ck(interpT *s, double x, double y, double *v, double *g, double *h) {
+    const int rc = vls_interp_evaluate(s, 1, &x, &y, v, g, h);
+    if (rc != VLS_OK) throw error(rc, vls_interp_last_error(s));
+  }
 };
 
 }  // namespace vls

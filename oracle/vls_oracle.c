@@ -496,6 +496,30 @@ static double evaluate_nxpy(const vlo_ctx *c, const double *d, long s1,
   return result;
 }
 
+/* the two gathers on a padded coefficient slice of row pitch s1 (exposed
+   for the spline-level tests): evaluateC at (Nx, x, Ny, y), and evaluateNxPy's
+   sum at node Nx and (Ny, y) already decomposed by pos2Coord (Ny = the integer
+   part, before localSpline's "1 +") */
+double vlo_evaluate_c(const double *coef, long s1, int Nx, double x, int Ny, double y) {
+  return evaluate_c(coef, s1, Nx, x, Ny, y);
+}
+double vlo_evaluate_nxpy(const double *d, long s1, int Nx, int Ny0, double y) {
+  long ref0, ref1, ref2, ref3;
+  int Ny = 1 + Ny0;
+  double result;
+  Nx++;
+  ref0 = Nx + (Ny - 1) * s1;
+  ref1 = Nx + Ny * s1;
+  ref2 = Nx + (Ny + 1) * s1;
+  ref3 = Nx + (Ny + 2) * s1;
+  result = 1.0 / 36.0;
+  result *= BV2(1. - y) * (d[ref0 - 1] + d[ref0] * 4 + d[ref0 + 1]) +
+            BV1(1. - y) * (d[ref1 - 1] + d[ref1] * 4 + d[ref1 + 1]) +
+            BV1(y) * (d[ref2 - 1] + d[ref2] * 4 + d[ref2 + 1]) +
+            BV2(y) * (d[ref3 - 1] + d[ref3] * 4 + d[ref3 + 1]);
+  return result;
+}
+
 /* localSpline::evaluate(double,double), localSpline.hxx:477-488 */
 static double evaluate_xy(const vlo_ctx *c, const double *d, long s1,
                           double xx, double yy) {

@@ -93,6 +93,11 @@ void vlo_stats(const vlo_ctx *c, double *out7);
    -> padded coefficients ((nu+2) x (nr+2)) */
 void vlo_prefilter2d(long nr, long nu, double hi_r, double hi_u,
                      const double *f, double *coef);
+/* evaluateC (localSpline.hxx:381-398) and evaluateNxPy's sum (:423-441) on
+   padded coefficients of row pitch s1 = nr + 2; Ny for the latter is the
+   integer part pos2Coord returns */
+double vlo_evaluate_c(const double *coef, long s1, int Nx, double x, int Ny, double y);
+double vlo_evaluate_nxpy(const double *coef, long s1, int Nx, int Ny, double y);
 /* kick of the whole grid with per-r shift (already multiplied by G/R^2 dt) */
 void vlo_kick(vlo_ctx *c, const double *shift);
 /* drift of the whole grid (tails refreshed, chains rolled) */

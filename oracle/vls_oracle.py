@@ -86,6 +86,10 @@ def lib():
         L.vlo_moments.argtypes = [ctypes.c_void_p, P(d), P(d)]
         L.vlo_stats.argtypes = [ctypes.c_void_p, P(d)]
         L.vlo_prefilter2d.argtypes = [ctypes.c_long, ctypes.c_long, d, d, P(d), P(d)]
+        L.vlo_evaluate_c.argtypes = [P(d), ctypes.c_long, ctypes.c_int, d, ctypes.c_int, d]
+        L.vlo_evaluate_c.restype = d
+        L.vlo_evaluate_nxpy.argtypes = [P(d), ctypes.c_long, ctypes.c_int, ctypes.c_int, d]
+        L.vlo_evaluate_nxpy.restype = d
         L.vlo_kick.argtypes = [ctypes.c_void_p, P(d)]
         L.vlo_drift.argtypes = [ctypes.c_void_p]
         _lib = L
@@ -226,3 +230,19 @@ def prefilter2d(f_slice, hi_r, hi_u):
     out = np.empty((nu + 2, nr + 2))
     lib().vlo_prefilter2d(nr, nu, hi_r, hi_u, _ptr(f), _ptr(out))
     return out
+
+
+def evaluate_c(coef, Nx, x, Ny, y):
+    """localSpline::evaluateC on padded coefficients (nu + 2, nr + 2), per point."""
+    c = np.ascontiguousarray(coef, dtype=np.float64)
+    s1 = c.shape[1]
+    return np.array([lib().vlo_evaluate_c(_ptr(c), s1, int(a), float(b), int(e), float(f))
+                     for a, b, e, f in zip(Nx, x, Ny, y)])
+
+
+def evaluate_nxpy(coef, Nx, Ny, y):
+    """evaluateNxPy's sum at node Nx and the decomposed (Ny, y), per point."""
+    c = np.ascontiguousarray(coef, dtype=np.float64)
+    s1 = c.shape[1]
+    return np.array([lib().vlo_evaluate_nxpy(_ptr(c), s1, int(a), int(e), float(f))
+                     for a, e, f in zip(Nx, Ny, y)])

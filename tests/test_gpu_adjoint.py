@@ -223,10 +223,15 @@ def test_adjoint_random_directions_match_central_differences():
         print(f"direction {trial}: adjoint {pred:.12e} fd {fd:.12e}")
         assert abs(pred - fd) <= 1e-6 * abs(fd), (trial, pred, fd)
     # the chain part alone, so that a wrong ring transpose cannot hide behind
-    # the much larger grid part
+    # the much larger grid part.  Its derivative is ~1e-9 of L, below the
+    # rounding noise of a difference at h = 1e-5; L depends on the chain
+    # values almost linearly (only through their tiny share of the mass), so
+    # the central difference takes hc = 0.5
+    hc = 0.5
     w = c0 * rng.standard_normal(c0.shape)
     pred = float(np.dot(dch, w))
-    fd = (_loss(s, f0, c0 + h * w, nsteps, dbins) - _loss(s, f0, c0 - h * w, nsteps, dbins)) / (2 * h)
+    fd = (_loss(s, f0, c0 + hc * w, nsteps, dbins) -
+          _loss(s, f0, c0 - hc * w, nsteps, dbins)) / (2 * hc)
     print(f"chains only: adjoint {pred:.12e} fd {fd:.12e}")
     assert abs(pred - fd) <= 1e-6 * abs(fd), (pred, fd)
 

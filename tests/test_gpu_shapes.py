@@ -18,9 +18,11 @@ pytestmark = pytest.mark.gpu
 # 701 u vertices: lines too long for 16-line blocks of 15-row chunks, which
 # take 23-row chunks by default; 1001 r vertices: FP64 rows whose four
 # persistent r-solve tiles exceed a block's shared memory (the plain kernel
-# takes them)
+# takes them); 2048 r or u vertices, the largest grids a handle takes: lines
+# beyond the register layouts, whose shared-memory segment tiles hold half
+# the usual lines in FP64
 SHAPES = [(3, 31), (31, 32), (32, 61), (61, 62), (62, 93), (93, 3), (150, 40),
-          (46, 68), (20, 700), (1000, 8)]
+          (46, 68), (20, 700), (1000, 8), (2047, 8), (8, 2047)]
 
 FP64_TOL = 1e-12
 FP32_L2 = 2e-6

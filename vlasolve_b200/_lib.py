@@ -33,6 +33,11 @@ EXPORTED = [
     "vls_adjoint_forward", "vls_adjoint_backward", "vls_adjoint_set_inner",
     "vls_adjoint_inner_used", "vls_device_bytes", "vls_write_restart",
     "vls_restart_info", "vls_read_restart",
+    "vls_spline2d_create", "vls_spline2d_destroy", "vls_spline2d_dims", "vls_spline2d_scale",
+    "vls_spline2d_assign", "vls_spline2d_build", "vls_spline2d_coefficients",
+    "vls_spline2d_pos2coord", "vls_spline2d_evaluate_c", "vls_spline2d_evaluate_nxpy",
+    "vls_spline2d_evaluate", "vls_spline2d_last_error", "vls_interp_create_init",
+    "vls_interp_create", "vls_interp_evaluate", "vls_interp_destroy", "vls_interp_last_error",
 ]
 KERNEL_KINDS = ["ucol_kick", "ucol", "prer", "tails", "drift", "scan", "moment",
                 "stats", "convert", "adj_drift", "adj_tails", "adj_prer", "adj_ucol",
@@ -70,6 +75,28 @@ class LayoutDesc(ctypes.Structure):
                 ("slices_per_batch", ctypes.c_int32), ("streams", ctypes.c_int32),
                 ("drift_wait_spins", ctypes.c_int32), ("u_chunk_rows", ctypes.c_int32),
                 ("r_chunk_rows", ctypes.c_int32)]
+
+
+class Spline2dDesc(ctypes.Structure):
+    _fields_ = [("start", ctypes.c_double * 2), ("stop", ctypes.c_double * 2),
+                ("N", ctypes.c_int32 * 2), ("scaleType", ctypes.c_int32 * 2),
+                ("vlType", ctypes.c_int32 * 2), ("bCond", (ctypes.c_int32 * 2) * 2),
+                ("precision", ctypes.c_int32), ("device", ctypes.c_int32)]
+
+
+class InterpInit(ctypes.Structure):
+    _fields_ = [("xstart", ctypes.c_double), ("xend", ctypes.c_double),
+                ("ystart", ctypes.c_double), ("yend", ctypes.c_double),
+                ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+                ("xbc", ctypes.c_int32 * 2), ("ybc", ctypes.c_int32 * 2),
+                ("xbcv", ctypes.c_double * 2), ("ybcv", ctypes.c_double * 2),
+                ("xscaleType", ctypes.c_int32), ("yscaleType", ctypes.c_int32),
+                ("rescaleNeeded", ctypes.c_int32), ("useLog", ctypes.c_int32)]
+
+
+# localSpline::boundaryTypeV and einspline's bc_code (interpolSpline)
+BC = {"periodic": 0, "flat": 1, "natural": 2, "supra_natural": 3, "not_a_knot": 4, "local": 5}
+EBC = {"periodic": 0, "deriv1": 1, "deriv2": 2, "flat": 3, "natural": 4, "antiperiodic": 5}
 
 
 class InitDesc(ctypes.Structure):
@@ -142,6 +169,22 @@ def load(path: str = LIB_PATH):
         "vls_adjoint_set_inner": [H, i32],
         "vls_adjoint_inner_used": [H, P(i32)],
         "vls_device_bytes": [H, P(ctypes.c_size_t)],
+        "vls_spline2d_create": [P(Spline2dDesc), i64, P(H)],
+        "vls_spline2d_destroy": [H],
+        "vls_spline2d_dims": [H, P(i32), P(i32), P(i64)],
+        "vls_spline2d_scale": [H, P(d), P(d)],
+        "vls_spline2d_assign": [H, P(d), i64],
+        "vls_spline2d_build": [H],
+        "vls_spline2d_coefficients": [H, i64, P(d)],
+        "vls_spline2d_pos2coord": [H, i32, i64, P(d), P(i32), P(d)],
+        "vls_spline2d_evaluate_c": [H, i64, P(i64), P(i32), P(d), P(i32), P(d), P(d)],
+        "vls_spline2d_evaluate_nxpy": [H, i64, P(i64), P(i32), P(d), P(d)],
+        "vls_spline2d_evaluate": [H, i64, P(i64), P(d), P(d), P(d)],
+        "vls_interp_create_init": [d, d, i32, d, d, i32, i32, i32, i32, i32, i32, i32, i32, i32,
+                                   d, d, d, d, P(InterpInit)],
+        "vls_interp_create": [P(InterpInit), P(d), i32, P(H)],
+        "vls_interp_evaluate": [H, i64, P(d), P(d), P(d), P(d), P(d)],
+        "vls_interp_destroy": [H],
         "vls_radial_mass_noalloc": [ctypes.c_void_p, i32, i64, i64, i64, P(d), P(d), P(d),
                                     P(d), ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, i32],
@@ -152,6 +195,9 @@ def load(path: str = LIB_PATH):
         fn.restype = ctypes.c_int
     L.vls_last_error.argtypes = [H]
     L.vls_last_error.restype = ctypes.c_char_p
+    for name in ("vls_spline2d_last_error", "vls_interp_last_error"):
+        getattr(L, name).argtypes = [H]
+        getattr(L, name).restype = ctypes.c_char_p
     L.vls_noalloc_last_error.argtypes = []
     L.vls_noalloc_last_error.restype = ctypes.c_char_p
     _lib = L

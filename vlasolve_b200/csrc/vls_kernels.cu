@@ -279,11 +279,13 @@ __device__ __forceinline__ R kick_exact(const R *cb, const Geometry &g, int u,
          R(6);
 }
 
-template <typename T, typename R, bool KICK>
+// TW columns per block (UcolCfg<R>::TW, or half of it where two buffers of
+// that many long columns exceed a block's shared memory)
+template <typename T, typename R, bool KICK, int TW>
 __global__ void __launch_bounds__(UC_THREADS)
     ucol_kernel(const T *__restrict__ f, T *__restrict__ G,
                 const double *__restrict__ shift, Geometry g, DirTables tu) {
-  constexpr int TW = UcolCfg<R>::TW, NSEG = UcolCfg<R>::NSEG;
+  constexpr int NSEG = UC_THREADS / TW;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int M = g.nu + 2;
   const int rows = M + 1;
@@ -365,22 +367,23 @@ template <typename T, typename R>
 cudaError_t launch_ucol(bool kick, const T *f, T *G, const double *shift,
                         const Geometry &g, const DirTables &tu, cudaStream_t st) {
   constexpr int TW = UcolCfg<R>::TW;
-  const size_t smem =
-      align16(2 * (size_t)(g.nu + 2) * sizeof(R)) + 2 * (size_t)(g.nu + 3) * TW * sizeof(R);
-  dim3 grid((g.nr + TW - 1) / TW, g.nb);
-  cudaError_t e;
-  if (kick) {
-    e = cudaFuncSetAttribute(ucol_kernel<T, R, true>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto smem_for = [&](int tw) {
+    return align16(2 * (size_t)(g.nu + 2) * sizeof(R)) + 2 * (size_t)(g.nu + 3) * tw * sizeof(R);
+  };
+  auto go = [&](auto kern, int tw) {
+    const size_t smem = smem_for(tw);
+    dim3 grid((g.nr + tw - 1) / tw, g.nb);
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    ucol_kernel<T, R, true><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
-  } else {
-    e = cudaFuncSetAttribute(ucol_kernel<T, R, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    ucol_kernel<T, R, false><<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
-  }
-  return cudaGetLastError();
+    kern<<<grid, UC_THREADS, smem, st>>>(f, G, shift, g, tu);
+    return cudaGetLastError();
+  };
+  // 227 KB per block: FP64 columns of more than ~1600 rows take half the columns
+  if (smem_for(TW) > 232448)
+    return kick ? go(ucol_kernel<T, R, true, TW / 2>, TW / 2)
+                : go(ucol_kernel<T, R, false, TW / 2>, TW / 2);
+  return kick ? go(ucol_kernel<T, R, true, TW>, TW) : go(ucol_kernel<T, R, false, TW>, TW);
 }
 
 // ------------------------------------------------------------------ prer
@@ -404,12 +407,13 @@ __host__ __device__ inline int prer_pitch(int M, int elem) {
   return P;
 }
 
-template <typename T, typename R>
-__global__ void __launch_bounds__(PrerCfg<R>::THREADS)
+// ROWS rows of G per block (PrerCfg<R>::ROWS, or half of it where a tile of
+// that many long rows exceeds a block's shared memory)
+template <typename T, typename R, int ROWS>
+__global__ void __launch_bounds__(ROWS * PrerCfg<R>::NSEG)
     prer_kernel(const T *__restrict__ G, T *__restrict__ C, Geometry g,
                 DirTables tr) {
-  constexpr int ROWS = PrerCfg<R>::ROWS, NSEG = PrerCfg<R>::NSEG,
-                NT = PrerCfg<R>::THREADS;
+  constexpr int NSEG = PrerCfg<R>::NSEG, NT = ROWS * NSEG;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int M = g.nr + 2;
   const int LS = prer_pitch(M, sizeof(R));
@@ -457,15 +461,29 @@ __global__ void __launch_bounds__(PrerCfg<R>::THREADS)
 template <typename T, typename R>
 cudaError_t launch_prer(const T *G, T *C, const Geometry &g, const DirTables &tr,
                         cudaStream_t st) {
-  constexpr int ROWS = PrerCfg<R>::ROWS;
+  constexpr int ROWS = PrerCfg<R>::ROWS, NSEG = PrerCfg<R>::NSEG;
   const int M = g.nr + 2;
-  const size_t smem = align16(2 * (size_t)M * sizeof(R)) +
-                      (size_t)ROWS * prer_pitch(M, sizeof(R)) * sizeof(R);
+  auto smem_for = [&](int rows) {
+    return align16(2 * (size_t)M * sizeof(R)) +
+           (size_t)rows * prer_pitch(M, sizeof(R)) * sizeof(R);
+  };
+  // 227 KB per block: FP64 rows of more than ~1600 columns take half the rows
+  if (smem_for(ROWS) > 232448) {
+    constexpr int H = ROWS / 2;
+    const size_t smem = smem_for(H);
+    dim3 grid((g.nu + 2 + H - 1) / H, g.nb);
+    cudaError_t e = cudaFuncSetAttribute(
+        prer_kernel<T, R, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    prer_kernel<T, R, H><<<grid, H * NSEG, smem, st>>>(G, C, g, tr);
+    return cudaGetLastError();
+  }
+  const size_t smem = smem_for(ROWS);
   dim3 grid((g.nu + 2 + ROWS - 1) / ROWS, g.nb);
   cudaError_t e = cudaFuncSetAttribute(
-      prer_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      prer_kernel<T, R, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  prer_kernel<T, R><<<grid, PrerCfg<R>::THREADS, smem, st>>>(G, C, g, tr);
+  prer_kernel<T, R, ROWS><<<grid, ROWS * NSEG, smem, st>>>(G, C, g, tr);
   return cudaGetLastError();
 }
 
@@ -1168,6 +1186,250 @@ cudaError_t launch_drift_strip(const CUtensorMap *tmS, int kind, const T *C, T *
     default:
       return cudaErrorInvalidValue;
   }
+}
+
+// ------------------------------------------------- lean FP32 strip drift
+// Strip-local footpoint words (FP32 handles whose drift stages strips): the
+// packed word of each cell re-encoded for the strip that gathers it, so that
+// the in-strip cell needs no index arithmetic:
+//   x bits 0-1   0 = the taps lie in the block's strip, else the cell takes
+//                the general path (outside, chain front, taps outside the
+//                strip's columns, the extra last column), which reads the
+//                packed word;
+//   x, y bits 2-22  the 21-bit fractions where a float's mantissa holds them
+//                   (float 1.frac = bits | 0x3F800000);
+//   x bits 23-31 / y bits 23-31  bits 2-10 / 11-19 of the byte offset of the
+//                   taps' first element in the strip (row uI, column
+//                   rI - (r0 - 8), WC = 48 columns).
+constexpr int LS_WC = 48, LS_XL = 8;
+static unsigned grid_for(size_t n);
+__global__ void strip_words_kernel(const uint2 *__restrict__ fp2, uint2 *__restrict__ fps,
+                                   int nr, int nu, size_t cells, int extra) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i % (size_t)nr);
+    const uint2 w = fp2[i];
+    uint32_t kind = 1u, off = 0u;
+    if (w.x < FP_CHAIN && !(extra && r == nr - 1)) {
+      const int rI = (int)(w.x >> FP_FBITS), uI = (int)(w.y >> FP_FBITS);
+      const int wc = rI - ((r >> 5) << 5) + LS_XL;
+      if (wc >= 0 && wc <= LS_WC - 4) {
+        kind = 0u;
+        off = (uint32_t)(uI * LS_WC + wc) * 4u;
+      }
+    }
+    fps[i] = make_uint2(kind | ((w.x & FP_FMASK) << 2) | (((off >> 2) & 511u) << 23),
+                        ((w.y & FP_FMASK) << 2) | (((off >> 11) & 511u) << 23));
+  }
+}
+
+cudaError_t launch_strip_words(const uint2 *fp2, uint2 *fps, const Geometry &g,
+                               cudaStream_t st) {
+  const size_t cells = (size_t)g.nr * g.nu * g.nj;
+  const int extra = (g.nr % 32 == 1 && g.nr > 32) ? 1 : 0;
+  strip_words_kernel<<<grid_for(cells), 256, 0, st>>>(fp2, fps, g.nr, g.nu, cells, extra);
+  return cudaGetLastError();
+}
+
+// in-strip gather of one cell from its strip-local word; fail = 1 after a
+// failed wait (every cell then takes the general path)
+__device__ __forceinline__ float lean_fast(uint2 w, const float *win, uint32_t fail,
+                                           bool &slow) {
+  const float2 t = __fadd2_rn(
+      make_float2(__uint_as_float((w.x & 0x007FFFFCu) | 0x3F800000u),
+                  __uint_as_float((w.y & 0x007FFFFCu) | 0x3F800000u)),
+      make_float2(-1.f, -1.f));
+  uint32_t off = ((w.x >> 21) & 0x7FCu) | ((w.y >> 12) & 0xFF800u);
+  slow = ((w.x & 3u) | fail) != 0u;
+  off = slow ? 0u : off;
+  const float *p = reinterpret_cast<const float *>(reinterpret_cast<const char *>(win) + off);
+  return gather_f32x2([&](int a, int b) { return p[a * LS_WC + b]; }, t.x, t.y);
+}
+
+template <int NW, int MINB>
+__global__ void __launch_bounds__(32 * NW, MINB)
+    drift_lean_kernel(const __grid_constant__ CUtensorMap tmS, const float *__restrict__ C,
+                      float *__restrict__ f, const uint2 *__restrict__ fps,
+                      const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
+                      const int32_t *__restrict__ ch_len, const float *__restrict__ ch_val,
+                      int64_t ndrift, MomentTables mt, double *__restrict__ partial,
+                      unsigned int *err, uint32_t spins, int extra, Geometry g) {
+  constexpr int WC = LS_WC, XL = LS_XL, PF = 2;
+  constexpr uint32_t BYTES = DS_ROWS * WC * sizeof(float);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ double red[NW][32];
+  const int rows = g.nu + 3;
+  const int nch = (rows + DS_ROWS - 1) / DS_ROWS;
+  float *win = reinterpret_cast<float *>(smem_raw);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + (size_t)nch * BYTES);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int r0 = blockIdx.x * 32, r = r0 + lane;
+  const int jl = blockIdx.y, j = g.j0 + jl;
+  const int x0 = r0 - XL;
+  if (tid == 0) {
+    for (int c = 0; c < nch; ++c) mbar_init(&bar[c], 1);
+    mbar_fence_init();
+    for (int c = 0; c < nch; ++c) {
+      mbar_expect_tx(&bar[c], BYTES);
+      tma_load_3d(win + (size_t)c * DS_ROWS * WC, &tmS, x0, c * DS_ROWS, jl, &bar[c]);
+    }
+  }
+  __syncthreads();
+  const float *Cj = C + (size_t)jl * rows * g.pc;
+  const bool col_ok = r < g.nr;
+  uint32_t fail = 0u;
+  for (int c = 0; c < nch; ++c)
+    if (!mbar_wait_bounded(&bar[c], 0u, spins)) {
+      fail = 1u;
+      atomicOr(err, 1u);
+      break;
+    }
+  double acc = 0.0;
+  {
+    const size_t sb = (size_t)j * g.nu * g.nr + (size_t)r;
+    const uint2 *ws = fps + sb;
+    float *fs = f + sb;
+    const uint32_t step = (uint32_t)NW * (uint32_t)g.nr;
+    const uint32_t ahead = (uint32_t)PF * step;
+    uint32_t off = (uint32_t)w * (uint32_t)g.nr;
+    uint2 q[PF];
+#pragma unroll
+    for (int k = 0; k < PF; ++k) q[k] = __ldg(ws + off + k * step);
+    int u = w;
+    for (; u + NW * (PF - 1) < g.nu; u += NW * PF) {
+      float v[PF];
+      bool slow[PF];
+      uint2 c[PF];
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < PF; ++k) {
+        c[k] = q[k];
+        q[k] = __ldg(ws + off + ahead + k * step);
+        v[k] = lean_fast(c[k], win, fail, slow[k]);
+        slow[k] = slow[k] && col_ok;
+        any |= slow[k];
+      }
+      if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+        for (int k = 0; k < PF; ++k)
+          if (slow[k]) {
+            RawCell<float> rc;
+            rc.w = __ldg(fp2 + sb + off + k * step);
+            v[k] = strip_slow<float>(rc, Cj, ch_start, ch_len, ch_val, ndrift, g);
+          }
+      }
+      float part = 0.f;
+#pragma unroll
+      for (int k = 0; k < PF; ++k) {
+        if (col_ok) {
+          fs[off + k * step] = v[k];
+          part += __ldg(mt.bu32 + u + NW * k) * v[k];
+        }
+      }
+      off += PF * step;
+      acc += (double)part;
+    }
+    float part = 0.f;
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      if (u + NW * k < g.nu) {
+        bool slow;
+        float v = lean_fast(q[k], win, fail, slow);
+        slow = slow && col_ok;
+        if (__any_sync(0xffffffffu, slow) && slow) {
+          RawCell<float> rc;
+          rc.w = __ldg(fp2 + sb + off + k * step);
+          v = strip_slow<float>(rc, Cj, ch_start, ch_len, ch_val, ndrift, g);
+        }
+        if (col_ok) {
+          fs[off + k * step] = v;
+          part += __ldg(mt.bu32 + u + NW * k) * v;
+        }
+      }
+    }
+    acc += (double)part;
+  }
+  // the extra last column (N_r = 32 k + 1), one row per thread, from the
+  // packed words
+  double acc2 = 0.0;
+  const bool xblock = extra && blockIdx.x == gridDim.x - 1;
+  if (xblock) {
+    const int rx = r0 + 32;
+    for (int u = tid; u < g.nu; u += 32 * NW) {
+      const size_t cell = ((size_t)j * g.nu + u) * g.nr + rx;
+      RawCell<float> rc;
+      rc.w = __ldg(fp2 + cell);
+      const Cell<float> cl = decode(rc);
+      float v = 0.f;
+      if (cl.kind == 0) {
+        const int wc = cl.rI - x0;
+        v = (!fail && wc >= 0 && wc <= WC - 4)
+                ? eval_strip<float, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y)
+                : eval2d<float>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
+      } else if (cl.kind == 2) {
+        const int L = __ldg(ch_len + cl.ch);
+        v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
+      }
+      f[cell] = v;
+      acc2 += (double)(__ldg(mt.bu32 + u) * v);
+    }
+  }
+  if (tid == 0) {
+    for (int c = 0; c < nch; ++c)
+      if (!mbar_wait_bounded(&bar[c], 0u)) atomicOr(err, 2u);
+  }
+  red[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && col_ok) {
+    double sum = 0.0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) sum += red[k][lane];
+    partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * sum;
+  }
+  if (xblock) {
+    __syncthreads();
+    red[w][lane] = acc2;
+    __syncthreads();
+    if (tid == 0) {
+      double sum = 0.0;
+      for (int k = 0; k < NW; ++k)
+        for (int l = 0; l < 32; ++l) sum += red[k][l];
+      partial[(size_t)j * g.nr + r0 + 32] = __ldg(mt.wj + j) * sum;
+    }
+  }
+}
+
+template <int NW, int MINB>
+static cudaError_t drift_lean_go(const CUtensorMap *tmS, const float *C, float *f,
+                                 const uint2 *fps, const uint2 *fp2, const int64_t *ch_start,
+                                 const int32_t *ch_len, const float *ch_val, int64_t ndrift,
+                                 const MomentTables &mt, double *partial, unsigned int *err,
+                                 uint32_t spins, const Geometry &g, cudaStream_t st) {
+  const int nch = (g.nu + 3 + DS_ROWS - 1) / DS_ROWS;
+  const size_t smem = (size_t)nch * DS_ROWS * LS_WC * sizeof(float) + nch * sizeof(uint64_t);
+  cudaError_t e = cudaFuncSetAttribute(drift_lean_kernel<NW, MINB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int extra = (g.nr % 32 == 1 && g.nr > 32) ? 1 : 0;
+  const dim3 grid(extra ? g.nr / 32 : (g.nr + 31) / 32, g.nb);
+  drift_lean_kernel<NW, MINB><<<grid, 32 * NW, smem, st>>>(*tmS, C, f, fps, fp2, ch_start,
+                                                           ch_len, ch_val, ndrift, mt, partial,
+                                                           err, spins, extra, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_drift_lean(const CUtensorMap *tmS, int kind, const float *C, float *f,
+                              const uint2 *fps, const uint2 *fp2, const int64_t *ch_start,
+                              const int32_t *ch_len, const float *ch_val, int64_t ndrift,
+                              const MomentTables &mt, double *partial, unsigned int *err,
+                              uint32_t spins, const Geometry &g, cudaStream_t st) {
+  if (kind == DRIFT_STRIP2)
+    return drift_lean_go<16, 2>(tmS, C, f, fps, fp2, ch_start, ch_len, ch_val, ndrift, mt,
+                                partial, err, spins, g, st);
+  if (kind == DRIFT_STRIP1)
+    return drift_lean_go<32, 1>(tmS, C, f, fps, fp2, ch_start, ch_len, ch_val, ndrift, mt,
+                                partial, err, spins, g, st);
+  return cudaErrorInvalidValue;
 }
 
 template <typename T>
