@@ -39,8 +39,6 @@ struct vls_handle {
   int32_t *idx = nullptr;        // FP64 footpoints
   void *fx = nullptr, *fy = nullptr;
   uint2 *fp2 = nullptr;          // FP32 packed footpoints
-  uint2 *fps = nullptr;          // FP32 strip-local words (strip drifts)
-  bool lean = false;             // the strip drift reads fps
   int64_t nch = 0, nel = 0;
   int64_t *ch_start = nullptr;
   int32_t *ch_len = nullptr;
@@ -379,10 +377,6 @@ static int encode_and_upload_footpoints(vls_handle *h, bool build_chains) {
       TRY(upload(h, h->fp2 + off, packed.data(), n * sizeof(uint2)));
     }
   }
-  if (h->lean) {
-    CK(h, launch_strip_words(h->fp2, h->fps, geometry(h), h->st));
-    CK(h, cudaStreamSynchronize(h->st));
-  }
   h->fp_gen++;
   return VLS_OK;
 }
@@ -566,7 +560,7 @@ extern "C" int vls_create_layout(const vls_grid_desc *grid, const vls_solver_des
   *out = nullptr;
   const vls_layout_desc lay = layout ? *layout : vls_layout_desc{};
   if (lay.prefilter < VLS_PREFILTER_AUTO || lay.prefilter > VLS_PREFILTER_SEGMENT ||
-      lay.drift < VLS_DRIFT_AUTO || lay.drift > 5 || lay.slices_per_batch < 0 ||
+      lay.drift < VLS_DRIFT_AUTO || lay.drift > VLS_DRIFT_STRIP1 || lay.slices_per_batch < 0 ||
       lay.streams < 0 || lay.streams > 8)
     return fail(nullptr, VLS_EINVAL, "vls_create: invalid layout descriptor");
   if (solver->precision != VLS_FP64 && solver->precision != VLS_FP32_BULK &&
@@ -708,19 +702,8 @@ extern "C" int vls_create_layout(const vls_grid_desc *grid, const vls_solver_des
       cudaMemsetAsync(h->flag, 0, sizeof(unsigned int) * 4, h->st) != cudaSuccess)
     return fin(fail(hp, VLS_ECUDA, "cudaMemsetAsync failed"));
   // drift kernel: whole-strip staging where it fits (see vls_layout_desc)
-  {
-    // 4 / 5: the lean strip drift with two / one block per SM
-    const int want = lay.drift == 4 ? DRIFT_STRIP2 : lay.drift == 5 ? DRIFT_STRIP1 : lay.drift;
-    h->drift_kind = h->esize == 4 ? drift_strip_width<float>(c.nu, want)
-                                  : drift_strip_width<double>(c.nu, want);
-    h->lean = h->esize == 4 && lay.drift >= 4 && h->drift_kind != DRIFT_WINDOW;
-    if (h->lean) {
-      const size_t fcells = cells + (size_t)FOOT_PAD_ROWS * c.nr + 32;
-      if (dalloc(hp, &h->fps, sizeof(uint2) * fcells) != VLS_OK ||
-          cudaMemset(h->fps, 0, sizeof(uint2) * fcells) != cudaSuccess)
-        return fin(fail(hp, VLS_ECUDA, "strip-local footpoint words"));
-    }
-  }
+  h->drift_kind = h->esize == 4 ? drift_strip_width<float>(c.nu, lay.drift)
+                                : drift_strip_width<double>(c.nu, lay.drift);
   h->drift_spins = lay.drift_wait_spins == 0  ? MBAR_SPIN_LIMIT
                    : lay.drift_wait_spins < 0 ? 0u
                                               : (uint32_t)lay.drift_wait_spins;
@@ -1072,10 +1055,6 @@ extern "C" int vls_set_footpoints(vls_handle *h, const int32_t *rI,
     for (size_t i = 0; i < h->cells; i++) p[i] = encode_packed(c, idx[i], rF[i], uF[i]);
     TRY(upload(h, h->fp2, p.data(), sizeof(uint2) * h->cells));
   }
-  if (h->lean) {
-    CK(h, launch_strip_words(h->fp2, h->fps, geometry(h), h->st));
-    CK(h, cudaStreamSynchronize(h->st));
-  }
   h->fp_gen++;
   return VLS_OK;
 }
@@ -1140,12 +1119,6 @@ static int drift_once(vls_handle *h, bool kick) {
     CK(h, timed(
               h, VLS_K_DRIFT,
               [&] {
-                if (h->lean)
-                  return launch_drift_lean(&h->tmS[sl], h->drift_kind, (const float *)C,
-                                           (float *)h->f, h->fps, h->fp2, h->ch_start,
-                                           h->ch_len, (const float *)h->ch_val, h->ndrift,
-                                           moment_tables(h), h->partial, h->flag + 1,
-                                           h->drift_spins, g, bs);
                 if (h->drift_kind != DRIFT_WINDOW)
                   return launch_drift_strip<T>(&h->tmS[sl], h->drift_kind, C, (T *)h->f,
                                                h->idx, (const T *)h->fx, (const T *)h->fy,

@@ -121,15 +121,6 @@ cudaError_t launch_drift_strip(const CUtensorMap *tmS, int kind, const T *C, T *
                                const T *ch_val, int64_t ndrift, const MomentTables &mt,
                                double *partial, unsigned int *err, uint32_t spins,
                                const Geometry &g, cudaStream_t st);
-// strip-local footpoint words of FP32 strip drifts (fps, same length and
-// padding as fp2) from the packed words, and the drift that reads them
-cudaError_t launch_strip_words(const uint2 *fp2, uint2 *fps, const Geometry &g,
-                               cudaStream_t st);
-cudaError_t launch_drift_lean(const CUtensorMap *tmS, int kind, const float *C, float *f,
-                              const uint2 *fps, const uint2 *fp2, const int64_t *ch_start,
-                              const int32_t *ch_len, const float *ch_val, int64_t ndrift,
-                              const MomentTables &mt, double *partial, unsigned int *err,
-                              uint32_t spins, const Geometry &g, cudaStream_t st);
 // chains [c_lo, c_hi) (all of the launch's slices) of nchains in total
 template <typename T>
 cudaError_t launch_chain_tails(const T *C, T *ch_val, const int64_t *ch_start,

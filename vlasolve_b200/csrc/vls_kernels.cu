@@ -1020,11 +1020,6 @@ __device__ __forceinline__ void strip_rows(
   acc += (double)part;
 }
 
-// Every box is awaited before the first cell (the other block on the SM, if
-// any, computes meanwhile).  `spins` bounds each of those waits (a wait that
-// runs out sets err bit 0 and sends every cell of the block to the gather
-// from global memory); the last wait, which keeps the block's shared memory
-// until every copy has landed, has the full limit (err bit 1).
 template <typename T, int WC, int NW, int MINB>
 __global__ void __launch_bounds__(32 * NW, MINB)
     drift_strip_kernel(const __grid_constant__ CUtensorMap tmS, const T *__restrict__ C,
@@ -1060,9 +1055,12 @@ __global__ void __launch_bounds__(32 * NW, MINB)
   __syncthreads();
   const T *Cj = C + (size_t)jl * rows * g.pc;
   const bool col_ok = r < g.nr;
+  int ready = 0;  // boxes [0, ready) seen complete by this thread
   bool waits_ok = true;
-  for (int c = 0; c < nch; ++c)
-    if (!mbar_wait_bounded(&bar[c], 0u, spins)) {
+  // every box before the first cell (the other block on the SM computes
+  // meanwhile); `spins` bounds each wait
+  for (; ready < nch; ++ready)
+    if (!mbar_wait_bounded(&bar[ready], 0u, spins)) {
       waits_ok = false;
       atomicOr(err, 1u);
       break;
@@ -1083,15 +1081,31 @@ __global__ void __launch_bounds__(32 * NW, MINB)
       T v = T(0);
       if (cl.kind == 0) {
         const int wc = cl.rI - x0;
-        v = (waits_ok && wc >= 0 && wc <= WC - 4)
-                ? eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y)
-                : eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
+        bool inwin = waits_ok && wc >= 0 && wc <= WC - 4;
+        if (inwin) {
+          // every box was awaited above (ready == nch), so these bounded
+          // waits never run; without the loop the compiler's register
+          // allocation of this kernel spills (40 B a thread, the drift 8 %
+          // slower on the 513 x 513 x 256 case)
+          const int cb = (cl.uI + 3) / DS_ROWS;
+          while (ready <= cb) {
+            if (!mbar_wait_bounded(&bar[ready], 0u)) {
+              waits_ok = false;
+              inwin = false;
+              atomicOr(err, 1u);
+              break;
+            }
+            ++ready;
+          }
+        }
+        v = inwin ? eval_strip<T, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y)
+                  : eval2d<T>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
       } else if (cl.kind == 2) {
         const int L = __ldg(ch_len + cl.ch);
         v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
       }
       f[cell] = v;
-      acc2 += (double)(moment_bu<T>(mt, u) * v);
+      acc2 += (double)((T)__ldg(mt.bu + u) * v);
     }
   }
   // every box must have landed before the block's shared memory is released
@@ -1186,250 +1200,6 @@ cudaError_t launch_drift_strip(const CUtensorMap *tmS, int kind, const T *C, T *
     default:
       return cudaErrorInvalidValue;
   }
-}
-
-// ------------------------------------------------- lean FP32 strip drift
-// Strip-local footpoint words (FP32 handles whose drift stages strips): the
-// packed word of each cell re-encoded for the strip that gathers it, so that
-// the in-strip cell needs no index arithmetic:
-//   x bits 0-1   0 = the taps lie in the block's strip, else the cell takes
-//                the general path (outside, chain front, taps outside the
-//                strip's columns, the extra last column), which reads the
-//                packed word;
-//   x, y bits 2-22  the 21-bit fractions where a float's mantissa holds them
-//                   (float 1.frac = bits | 0x3F800000);
-//   x bits 23-31 / y bits 23-31  bits 2-10 / 11-19 of the byte offset of the
-//                   taps' first element in the strip (row uI, column
-//                   rI - (r0 - 8), WC = 48 columns).
-constexpr int LS_WC = 48, LS_XL = 8;
-static unsigned grid_for(size_t n);
-__global__ void strip_words_kernel(const uint2 *__restrict__ fp2, uint2 *__restrict__ fps,
-                                   int nr, int nu, size_t cells, int extra) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(i % (size_t)nr);
-    const uint2 w = fp2[i];
-    uint32_t kind = 1u, off = 0u;
-    if (w.x < FP_CHAIN && !(extra && r == nr - 1)) {
-      const int rI = (int)(w.x >> FP_FBITS), uI = (int)(w.y >> FP_FBITS);
-      const int wc = rI - ((r >> 5) << 5) + LS_XL;
-      if (wc >= 0 && wc <= LS_WC - 4) {
-        kind = 0u;
-        off = (uint32_t)(uI * LS_WC + wc) * 4u;
-      }
-    }
-    fps[i] = make_uint2(kind | ((w.x & FP_FMASK) << 2) | (((off >> 2) & 511u) << 23),
-                        ((w.y & FP_FMASK) << 2) | (((off >> 11) & 511u) << 23));
-  }
-}
-
-cudaError_t launch_strip_words(const uint2 *fp2, uint2 *fps, const Geometry &g,
-                               cudaStream_t st) {
-  const size_t cells = (size_t)g.nr * g.nu * g.nj;
-  const int extra = (g.nr % 32 == 1 && g.nr > 32) ? 1 : 0;
-  strip_words_kernel<<<grid_for(cells), 256, 0, st>>>(fp2, fps, g.nr, g.nu, cells, extra);
-  return cudaGetLastError();
-}
-
-// in-strip gather of one cell from its strip-local word; fail = 1 after a
-// failed wait (every cell then takes the general path)
-__device__ __forceinline__ float lean_fast(uint2 w, const float *win, uint32_t fail,
-                                           bool &slow) {
-  const float2 t = __fadd2_rn(
-      make_float2(__uint_as_float((w.x & 0x007FFFFCu) | 0x3F800000u),
-                  __uint_as_float((w.y & 0x007FFFFCu) | 0x3F800000u)),
-      make_float2(-1.f, -1.f));
-  uint32_t off = ((w.x >> 21) & 0x7FCu) | ((w.y >> 12) & 0xFF800u);
-  slow = ((w.x & 3u) | fail) != 0u;
-  off = slow ? 0u : off;
-  const float *p = reinterpret_cast<const float *>(reinterpret_cast<const char *>(win) + off);
-  return gather_f32x2([&](int a, int b) { return p[a * LS_WC + b]; }, t.x, t.y);
-}
-
-template <int NW, int MINB>
-__global__ void __launch_bounds__(32 * NW, MINB)
-    drift_lean_kernel(const __grid_constant__ CUtensorMap tmS, const float *__restrict__ C,
-                      float *__restrict__ f, const uint2 *__restrict__ fps,
-                      const uint2 *__restrict__ fp2, const int64_t *__restrict__ ch_start,
-                      const int32_t *__restrict__ ch_len, const float *__restrict__ ch_val,
-                      int64_t ndrift, MomentTables mt, double *__restrict__ partial,
-                      unsigned int *err, uint32_t spins, int extra, Geometry g) {
-  constexpr int WC = LS_WC, XL = LS_XL, PF = 2;
-  constexpr uint32_t BYTES = DS_ROWS * WC * sizeof(float);
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ double red[NW][32];
-  const int rows = g.nu + 3;
-  const int nch = (rows + DS_ROWS - 1) / DS_ROWS;
-  float *win = reinterpret_cast<float *>(smem_raw);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + (size_t)nch * BYTES);
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int r0 = blockIdx.x * 32, r = r0 + lane;
-  const int jl = blockIdx.y, j = g.j0 + jl;
-  const int x0 = r0 - XL;
-  if (tid == 0) {
-    for (int c = 0; c < nch; ++c) mbar_init(&bar[c], 1);
-    mbar_fence_init();
-    for (int c = 0; c < nch; ++c) {
-      mbar_expect_tx(&bar[c], BYTES);
-      tma_load_3d(win + (size_t)c * DS_ROWS * WC, &tmS, x0, c * DS_ROWS, jl, &bar[c]);
-    }
-  }
-  __syncthreads();
-  const float *Cj = C + (size_t)jl * rows * g.pc;
-  const bool col_ok = r < g.nr;
-  uint32_t fail = 0u;
-  for (int c = 0; c < nch; ++c)
-    if (!mbar_wait_bounded(&bar[c], 0u, spins)) {
-      fail = 1u;
-      atomicOr(err, 1u);
-      break;
-    }
-  double acc = 0.0;
-  {
-    const size_t sb = (size_t)j * g.nu * g.nr + (size_t)r;
-    const uint2 *ws = fps + sb;
-    float *fs = f + sb;
-    const uint32_t step = (uint32_t)NW * (uint32_t)g.nr;
-    const uint32_t ahead = (uint32_t)PF * step;
-    uint32_t off = (uint32_t)w * (uint32_t)g.nr;
-    uint2 q[PF];
-#pragma unroll
-    for (int k = 0; k < PF; ++k) q[k] = __ldg(ws + off + k * step);
-    int u = w;
-    for (; u + NW * (PF - 1) < g.nu; u += NW * PF) {
-      float v[PF];
-      bool slow[PF];
-      uint2 c[PF];
-      bool any = false;
-#pragma unroll
-      for (int k = 0; k < PF; ++k) {
-        c[k] = q[k];
-        q[k] = __ldg(ws + off + ahead + k * step);
-        v[k] = lean_fast(c[k], win, fail, slow[k]);
-        slow[k] = slow[k] && col_ok;
-        any |= slow[k];
-      }
-      if (__any_sync(0xffffffffu, any)) {
-#pragma unroll
-        for (int k = 0; k < PF; ++k)
-          if (slow[k]) {
-            RawCell<float> rc;
-            rc.w = __ldg(fp2 + sb + off + k * step);
-            v[k] = strip_slow<float>(rc, Cj, ch_start, ch_len, ch_val, ndrift, g);
-          }
-      }
-      float part = 0.f;
-#pragma unroll
-      for (int k = 0; k < PF; ++k) {
-        if (col_ok) {
-          fs[off + k * step] = v[k];
-          part += __ldg(mt.bu32 + u + NW * k) * v[k];
-        }
-      }
-      off += PF * step;
-      acc += (double)part;
-    }
-    float part = 0.f;
-#pragma unroll
-    for (int k = 0; k < PF; ++k) {
-      if (u + NW * k < g.nu) {
-        bool slow;
-        float v = lean_fast(q[k], win, fail, slow);
-        slow = slow && col_ok;
-        if (__any_sync(0xffffffffu, slow) && slow) {
-          RawCell<float> rc;
-          rc.w = __ldg(fp2 + sb + off + k * step);
-          v = strip_slow<float>(rc, Cj, ch_start, ch_len, ch_val, ndrift, g);
-        }
-        if (col_ok) {
-          fs[off + k * step] = v;
-          part += __ldg(mt.bu32 + u + NW * k) * v;
-        }
-      }
-    }
-    acc += (double)part;
-  }
-  // the extra last column (N_r = 32 k + 1), one row per thread, from the
-  // packed words
-  double acc2 = 0.0;
-  const bool xblock = extra && blockIdx.x == gridDim.x - 1;
-  if (xblock) {
-    const int rx = r0 + 32;
-    for (int u = tid; u < g.nu; u += 32 * NW) {
-      const size_t cell = ((size_t)j * g.nu + u) * g.nr + rx;
-      RawCell<float> rc;
-      rc.w = __ldg(fp2 + cell);
-      const Cell<float> cl = decode(rc);
-      float v = 0.f;
-      if (cl.kind == 0) {
-        const int wc = cl.rI - x0;
-        v = (!fail && wc >= 0 && wc <= WC - 4)
-                ? eval_strip<float, WC>(win + (size_t)cl.uI * WC + wc, cl.x, cl.y)
-                : eval2d<float>(Cj, g.pc, cl.rI, cl.x, cl.uI, cl.y);
-      } else if (cl.kind == 2) {
-        const int L = __ldg(ch_len + cl.ch);
-        v = ch_val[__ldg(ch_start + cl.ch) + ndrift % L];
-      }
-      f[cell] = v;
-      acc2 += (double)(__ldg(mt.bu32 + u) * v);
-    }
-  }
-  if (tid == 0) {
-    for (int c = 0; c < nch; ++c)
-      if (!mbar_wait_bounded(&bar[c], 0u)) atomicOr(err, 2u);
-  }
-  red[w][lane] = acc;
-  __syncthreads();
-  if (w == 0 && col_ok) {
-    double sum = 0.0;
-#pragma unroll
-    for (int k = 0; k < NW; ++k) sum += red[k][lane];
-    partial[(size_t)j * g.nr + r] = __ldg(mt.wj + j) * sum;
-  }
-  if (xblock) {
-    __syncthreads();
-    red[w][lane] = acc2;
-    __syncthreads();
-    if (tid == 0) {
-      double sum = 0.0;
-      for (int k = 0; k < NW; ++k)
-        for (int l = 0; l < 32; ++l) sum += red[k][l];
-      partial[(size_t)j * g.nr + r0 + 32] = __ldg(mt.wj + j) * sum;
-    }
-  }
-}
-
-template <int NW, int MINB>
-static cudaError_t drift_lean_go(const CUtensorMap *tmS, const float *C, float *f,
-                                 const uint2 *fps, const uint2 *fp2, const int64_t *ch_start,
-                                 const int32_t *ch_len, const float *ch_val, int64_t ndrift,
-                                 const MomentTables &mt, double *partial, unsigned int *err,
-                                 uint32_t spins, const Geometry &g, cudaStream_t st) {
-  const int nch = (g.nu + 3 + DS_ROWS - 1) / DS_ROWS;
-  const size_t smem = (size_t)nch * DS_ROWS * LS_WC * sizeof(float) + nch * sizeof(uint64_t);
-  cudaError_t e = cudaFuncSetAttribute(drift_lean_kernel<NW, MINB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const int extra = (g.nr % 32 == 1 && g.nr > 32) ? 1 : 0;
-  const dim3 grid(extra ? g.nr / 32 : (g.nr + 31) / 32, g.nb);
-  drift_lean_kernel<NW, MINB><<<grid, 32 * NW, smem, st>>>(*tmS, C, f, fps, fp2, ch_start,
-                                                           ch_len, ch_val, ndrift, mt, partial,
-                                                           err, spins, extra, g);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_drift_lean(const CUtensorMap *tmS, int kind, const float *C, float *f,
-                              const uint2 *fps, const uint2 *fp2, const int64_t *ch_start,
-                              const int32_t *ch_len, const float *ch_val, int64_t ndrift,
-                              const MomentTables &mt, double *partial, unsigned int *err,
-                              uint32_t spins, const Geometry &g, cudaStream_t st) {
-  if (kind == DRIFT_STRIP2)
-    return drift_lean_go<16, 2>(tmS, C, f, fps, fp2, ch_start, ch_len, ch_val, ndrift, mt,
-                                partial, err, spins, g, st);
-  if (kind == DRIFT_STRIP1)
-    return drift_lean_go<32, 1>(tmS, C, f, fps, fp2, ch_start, ch_len, ch_val, ndrift, mt,
-                                partial, err, spins, g, st);
-  return cudaErrorInvalidValue;
 }
 
 template <typename T>

@@ -204,9 +204,9 @@ class VlasovSolver21Spline:
             lay = _lib.LayoutDesc()
             for k, v in layout.items():
                 if k == "prefilter":
-                    v = _lib.PREFILTERS[v]
+                    v = _lib.PREFILTERS[v] if isinstance(v, str) else v
                 elif k == "drift":
-                    v = _lib.DRIFTS[v]
+                    v = _lib.DRIFTS[v] if isinstance(v, str) else v
                 elif k not in ("slices_per_batch", "streams", "drift_wait_spins"):
                     raise ValueError(f"unknown layout field '{k}'")
                 setattr(lay, k, int(v))
@@ -229,7 +229,8 @@ class VlasovSolver21Spline:
         self._ck(self._L.vls_get_layout(self._h, ctypes.byref(d)))
         pre = {v: k for k, v in _lib.PREFILTERS.items()}
         drift = {v: k for k, v in _lib.DRIFTS.items()}
-        return dict(prefilter=pre[d.prefilter], drift=drift[d.drift],
+        return dict(prefilter=pre.get(d.prefilter, d.prefilter),
+                    drift=drift.get(d.drift, d.drift),
                     slices_per_batch=d.slices_per_batch, streams=d.streams,
                     drift_wait_spins=d.drift_wait_spins, u_chunk_rows=d.u_chunk_rows,
                     r_chunk_rows=d.r_chunk_rows)
