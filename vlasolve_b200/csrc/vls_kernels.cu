@@ -1020,7 +1020,7 @@ __device__ __forceinline__ void strip_rows(
   acc += (double)part;
 }
 
-template <typename T, int WC, int NW, int MINB>
+template <typename T, int WC, int NW, int MINB, int PF = 2>
 __global__ void __launch_bounds__(32 * NW, MINB)
     drift_strip_kernel(const __grid_constant__ CUtensorMap tmS, const T *__restrict__ C,
                        T *__restrict__ f, const int32_t *__restrict__ idx,
@@ -1030,9 +1030,10 @@ __global__ void __launch_bounds__(32 * NW, MINB)
                        int64_t ndrift, MomentTables mt, double *__restrict__ partial,
                        unsigned int *err, uint32_t spins, int extra, Geometry g) {
   constexpr int XL = (WC - 32) / 2;
-  // rows of footpoints in flight per thread (2: 6 % faster than 4 and 3 %
-  // faster than 1 on the 513 x 513 x 256 case)
-  constexpr int PF = 2;
+  // PF: rows of footpoints in flight per thread.  16 warps with PF = 2 (two
+  // blocks per SM) measured fastest on the 513 x 513 x 256 case: drift 0.309
+  // ms against 0.318 / 0.361 (PF 3 / 1), 0.319 / 0.327 (12 warps, PF 2 / 3),
+  // 0.398 / 0.316 (8 warps, PF 2 / 4)
   constexpr uint32_t BYTES = DS_ROWS * WC * sizeof(T);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ double red[NW][32];
@@ -1160,7 +1161,7 @@ int drift_strip_width(int nu, int want) {
   return fit2 ? DRIFT_STRIP2 : fit1 ? DRIFT_STRIP1 : DRIFT_WINDOW;
 }
 
-template <typename T, int WC, int NW, int MINB>
+template <typename T, int WC, int NW, int MINB, int PF = 2>
 static cudaError_t drift_strip_go(const CUtensorMap *tmS, const T *C, T *f, const int32_t *idx,
                                   const T *fx, const T *fy, const uint2 *fp2,
                                   const int64_t *ch_start, const int32_t *ch_len,
@@ -1169,7 +1170,7 @@ static cudaError_t drift_strip_go(const CUtensorMap *tmS, const T *C, T *f, cons
                                   const Geometry &g, cudaStream_t st) {
   const int nch = (g.nu + 3 + DS_ROWS - 1) / DS_ROWS;
   const size_t smem = (size_t)nch * DS_ROWS * WC * sizeof(T) + nch * sizeof(uint64_t);
-  cudaError_t e = cudaFuncSetAttribute(drift_strip_kernel<T, WC, NW, MINB>,
+  cudaError_t e = cudaFuncSetAttribute(drift_strip_kernel<T, WC, NW, MINB, PF>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   // N_r = 32 k + 1 (every grid of the form 2^n + 1): k blocks, the last one
@@ -1177,7 +1178,7 @@ static cudaError_t drift_strip_go(const CUtensorMap *tmS, const T *C, T *f, cons
   // the 513 x 513 x 256 case
   const int extra = (g.nr % 32 == 1 && g.nr > 32) ? 1 : 0;
   const dim3 grid(extra ? g.nr / 32 : (g.nr + 31) / 32, g.nb);
-  drift_strip_kernel<T, WC, NW, MINB><<<grid, 32 * NW, smem, st>>>(
+  drift_strip_kernel<T, WC, NW, MINB, PF><<<grid, 32 * NW, smem, st>>>(
       *tmS, C, f, idx, fx, fy, fp2, ch_start, ch_len, ch_val, ndrift, mt, partial, err, spins,
       extra, g);
   return cudaGetLastError();

@@ -33,7 +33,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 
 #include "vls_async.cuh"
 #include "vls_internal.h"
@@ -858,6 +861,34 @@ cudaError_t ucol_rc_go(const T *f, T *G, const double *shift, const Geometry &g,
   return cudaGetLastError();
 }
 
+// occupancy of the persistent r-solve per (device, kernel, shared memory,
+// threads), computed on first use
+struct PipeOcc {
+  int nsm = 0, per = 0;
+};
+struct PipeOccKey {
+  int dev;
+  const void *k;
+  size_t smem;
+  int nt;
+  bool operator<(const PipeOccKey &o) const {
+    return std::tie(dev, k, smem, nt) < std::tie(o.dev, o.k, o.smem, o.nt);
+  }
+};
+std::mutex g_occ_mutex;
+std::map<PipeOccKey, PipeOcc> g_occ;
+bool pipe_occ_lookup(int dev, const void *k, size_t smem, int nt, PipeOcc &o) {
+  std::lock_guard<std::mutex> lk(g_occ_mutex);
+  auto it = g_occ.find(PipeOccKey{dev, k, smem, nt});
+  if (it == g_occ.end()) return false;
+  o = it->second;
+  return true;
+}
+void pipe_occ_store(int dev, const void *k, size_t smem, int nt, const PipeOcc &o) {
+  std::lock_guard<std::mutex> lk(g_occ_mutex);
+  g_occ[PipeOccKey{dev, k, smem, nt}] = o;
+}
+
 template <typename T, typename R, class CF>
 cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
                        unsigned int *err, cudaStream_t st) {
@@ -879,23 +910,33 @@ cudaError_t prer_rc_go(const T *G, T *C, const Geometry &g, const RcDir<R> &tr,
                            (size_t)RC_PIPE_TILES * CF::LN *
                                rc_tile_pitch_rows(M, g.gp, g.pc, sizeof(T), CF::LN) * sizeof(T);
       auto kp = prer_pipe_kernel<T, R, CF>;
-      int dev = 0, nsm = 0, per = 0, smax = 0;
+      int dev = 0;
       cudaError_t e;
       if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-      if ((e = cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
-          cudaSuccess)
+      // blocks per SM of the persistent kernel for this tile size, found once
+      // per device (occupancy queries cost host time at every step otherwise)
+      PipeOcc o;
+      if (!pipe_occ_lookup(dev, (const void *)kp, psmem, nt, o)) {
+        int smax = 0;
+        if ((e = cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
+            cudaSuccess)
+          return e;
+        // four tiles of long FP64 rows (1025 columns: 272 KB) do not fit a
+        // block: the plain kernel below then takes the rows
+        if (psmem <= (size_t)smax) {
+          if ((e = rc_attr(kp, psmem)) != cudaSuccess) return e;
+          if ((e = cudaDeviceGetAttribute(&o.nsm, cudaDevAttrMultiProcessorCount, dev)) !=
+              cudaSuccess)
+            return e;
+          if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per, kp, nt, psmem)) !=
+              cudaSuccess)
+            return e;
+        }
+        pipe_occ_store(dev, (const void *)kp, psmem, nt, o);
+      } else if (o.per >= CF::MINB && (e = rc_attr(kp, psmem)) != cudaSuccess) {
         return e;
-      // four tiles of long FP64 rows (1025 columns: 272 KB) do not fit a
-      // block: the plain kernel below then takes the rows
-      if (psmem <= (size_t)smax) {
-        if ((e = rc_attr(kp, psmem)) != cudaSuccess) return e;
-        if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) !=
-            cudaSuccess)
-          return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kp, nt, psmem)) !=
-            cudaSuccess)
-          return e;
       }
+      const int nsm = o.nsm, per = o.per;
       // only where it keeps the plain kernel's blocks per SM (four FP64
       // tiles of a 513-column row group hold one block per SM)
       if (per >= CF::MINB) {
