@@ -20,6 +20,7 @@
 
 #include <algorithm>
 
+#include "vls_dd.cuh"
 #include "vls_internal.h"
 
 namespace vls {
@@ -192,43 +193,85 @@ __global__ void ucol_adj_kernel(const T *__restrict__ f, double *__restrict__ Gb
 }
 
 // shift, transposed: sbar (per slice) -> beta_r' = sum_{r > r'} Rcoef_r sum_j sbar[j][r]
-// (beta[0..N_r)), and the moment's transpose per radius to beta[N_r..2 N_r)
-// (one block of 1024 threads: 32 slice groups x 32 radii sum in parallel,
-// in a fixed order; the N_r-long reverse scan in one thread)
+// (beta[0..N_r)), and the moment's transpose per radius to beta[N_r..2 N_r).
+// Each block sums 32 radii over the slices (32 slice groups j = w, w + 32,
+// ... in parallel, then the groups in order) into beta[N_r + r] as scratch;
+// the last block to finish (count, left at zero again) runs the reverse
+// exclusive scan over the radii, compensated as the forward's enclosed-mass
+// scan, and writes the moment term over the scratch.  The summation order is
+// fixed.
 __global__ void __launch_bounds__(1024) shift_adj_kernel(const double *__restrict__ sbar,
-                                                         double *__restrict__ beta,
+                                                         double *beta, unsigned int *count,
                                                          MomentTables mt, Geometry g) {
-  extern __shared__ double ssum[];
   __shared__ double part[32][33];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int r0 = 0; r0 < g.nr; r0 += 32) {
-    const int r = r0 + lane;
+  __shared__ dd wsum[32];
+  __shared__ bool last;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  {
+    const int r = blockIdx.x * 32 + lane;
     double s = 0.0;
-    if (r < g.nr)
-      for (int j = w; j < g.nj; j += 32) s += sbar[(size_t)j * g.nr + r];
+    if (r < g.nr) {
+#pragma unroll 8
+      for (int j = w; j < g.nj; j += 32) s += __ldg(sbar + (size_t)j * g.nr + r);
+    }
     part[w][lane] = s;
     __syncthreads();
     if (w == 0 && r < g.nr) {
       double t = 0.0;
       for (int k = 0; k < 32; ++k) t += part[k][lane];
-      ssum[r] = t * mt.Rcoef[r];
+      beta[g.nr + r] = t * mt.Rcoef[r];
     }
-    __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    double acc = 0.0;
-    for (int r = g.nr - 1; r >= 0; --r) {
-      beta[r] = acc;  // exclusive: bins_r' enters s_r for r > r'
-      acc += ssum[r];
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // q = N_r - 1 - r ascending: thread t holds q = t per .. t per + per - 1
+  const int per = (g.nr + 1023) / 1024;  // 1 or 2
+  double x[2] = {0.0, 0.0};
+  dd loc{0.0, 0.0};
+  for (int k = 0; k < per; ++k) {
+    const int q = tid * per + k;
+    if (q < g.nr) {
+      x[k] = *((volatile double *)beta + g.nr + (g.nr - 1 - q));
+      loc = dd_add(loc, dd{x[k], 0.0});
+    }
+  }
+  dd inc = loc;
+  for (int d = 1; d < 32; d <<= 1) {
+    const dd o = dd_shfl_up(inc, d);
+    if (lane >= d) inc = dd_add(inc, o);
+  }
+  if (lane == 31) wsum[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const dd xw = wsum[lane];
+    dd xi = xw;
+    for (int d = 1; d < 32; d <<= 1) {
+      const dd o = dd_shfl_up(xi, d);
+      if (lane >= d) xi = dd_add(xi, o);
+    }
+    wsum[lane] = dd_add(xi, dd{-xw.hi, -xw.lo});  // exclusive over warps
+  }
+  __syncthreads();
+  dd ex = dd_add(wsum[w], dd_add(inc, dd{-loc.hi, -loc.lo}));
+  for (int k = 0; k < per; ++k) {
+    const int q = tid * per + k;
+    if (q < g.nr) {
+      beta[g.nr - 1 - q] = ex.hi + ex.lo;  // exclusive: bins_r' enters s_r for r > r'
+      ex = dd_add(ex, dd{x[k], 0.0});
     }
   }
   // the moment's transpose per radius: mB_r = beta_r dR4_r + beta_{r-1} dR4_{r-1}
   __syncthreads();
-  for (int r = threadIdx.x; r < g.nr; r += blockDim.x) {
+  for (int r = tid; r < g.nr; r += blockDim.x) {
     double b = beta[r] * mt.dR4[r];
     if (r > 0) b += beta[r - 1] * mt.dR4[r - 1];
     beta[g.nr + r] = b;
   }
+  if (tid == 0) *count = 0u;
 }
 
 // moment, transposed: lam += w_j b_u (beta_r dR_r/4 + beta_{r-1} dR_{r-1}/4)
@@ -673,17 +716,14 @@ cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const M
                                     const T *fy, const int32_t *idx, const uint2 *fp2,
                                     const int32_t *t_idx, const double *t_x,
                                     const double *t_y, const Geometry &g, cudaStream_t st) {
-  constexpr int Q = 2;
-  auto go = [&](auto kern, int R) {
-    const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
-                    (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
-    kern<<<grid, dim3(32, 4), 0, st>>>(lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2,
-                                       t_idx, t_x, t_y, g);
-    return cudaGetLastError();
-  };
-  // 8 node rows per thread: 0.196 ms per transposed step on 257 x 257 x 128
-  // against 0.198 / 0.264 for 16 / 32 rows and 0.215 for the fixed blocks
-  return go(drift_adj_sweep_kernel<T, 8, Q>, 8);
+  // 8 node rows x 3 columns per thread: 0.189 ms per transposed step on
+  // 257 x 257 x 128 against 0.195 / 0.226 for 2 / 4 columns, 0.198 / 0.264
+  // for 16 / 32 rows and 0.215 for fixed blocks of rows
+  constexpr int Q = 3, R = 8;
+  const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
+                  (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
+  drift_adj_sweep_kernel<T, R, Q><<<grid, dim3(32, 4), 0, st>>>(
+      lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2, t_idx, t_x, t_y, g);
   return cudaGetLastError();
 }
 
@@ -709,17 +749,15 @@ cudaError_t launch_drift_adj_gather_perm(const double *vperm, const uint2 *geo, 
                                          const uint32_t *ends, const int64_t *ebase,
                                          const int32_t *t_idx, const double *t_x,
                                          const double *t_y, const Geometry &g, cudaStream_t st) {
-  constexpr int Q = 2;
-  auto go = [&](auto kern, int R) {
-    const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
-                    (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
-    kern<<<grid, dim3(32, 4), 0, st>>>(vperm, geo, Cb, ends, ebase, t_idx, t_x, t_y, g);
-    return cudaGetLastError();
-  };
-  // 16 node rows per thread: 0.182 ms per transposed step (permutation
-  // included) on 257 x 257 x 128 against 0.187 / 0.196 for 8 / 32 rows and
-  // 0.207 for the fixed blocks
-  return go(drift_adj_sweep_perm_kernel<16, Q>, 16);
+  // 16 node rows x 2 columns per thread: 0.182 ms per transposed step
+  // (permutation included) on 257 x 257 x 128 against 0.187 / 0.196 for 8 /
+  // 32 rows, 0.188 / 0.213 for 3 / 4 columns and 0.207 for fixed blocks of
+  // rows
+  constexpr int Q = 2, R = 16;
+  const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
+                  (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
+  drift_adj_sweep_perm_kernel<R, Q><<<grid, dim3(32, 4), 0, st>>>(vperm, geo, Cb, ends, ebase,
+                                                                   t_idx, t_x, t_y, g);
   return cudaGetLastError();
 }
 
@@ -754,15 +792,10 @@ cudaError_t launch_ucol_adj(const T *f, double *Gb, double *A, double *B, double
   return cudaGetLastError();
 }
 
-cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTables &mt,
-                             const Geometry &g, cudaStream_t st) {
-  const size_t smem = (size_t)g.nr * sizeof(double);
-  if (smem > (32u << 10)) {
-    const cudaError_t e = cudaFuncSetAttribute(
-        shift_adj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  shift_adj_kernel<<<1, 1024, smem, st>>>(sbar, beta, mt, g);
+cudaError_t launch_shift_adj(const double *sbar, double *beta, unsigned int *count,
+                             const MomentTables &mt, const Geometry &g, cudaStream_t st) {
+  if (g.nr > 2048) return cudaErrorInvalidValue;
+  shift_adj_kernel<<<(g.nr + 31) / 32, 1024, 0, st>>>(sbar, beta, count, mt, g);
   return cudaGetLastError();
 }
 

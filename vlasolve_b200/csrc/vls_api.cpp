@@ -1071,8 +1071,14 @@ const RcDir<float> &rcdir<float>(const vls_handle *h, bool u) {
   return u ? h->rcu_f : h->rcr_f;
 }
 
+// One split step: f_out = D P_r P_u Kick(P_u f_in).  f_in and f_out are the
+// handle's grid unless given (the adjoint's recomputation steps from one
+// stored state into the next); they may be the same buffer.
 template <typename T, typename R>
-static int drift_once(vls_handle *h, bool kick) {
+static int drift_once(vls_handle *h, bool kick, const void *f_in = nullptr,
+                      void *f_out = nullptr) {
+  const T *fin = (const T *)(f_in ? f_in : h->f);
+  T *fout = (T *)(f_out ? f_out : h->f);
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
   const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
   const size_t gslot = (size_t)h->B * (h->co.nu + 2) * h->gp;
@@ -1091,9 +1097,9 @@ static int drift_once(vls_handle *h, bool kick) {
               h, kick ? VLS_K_UCOL_KICK : VLS_K_UCOL,
               [&] {
                 if (h->rcu_cfg >= 0)
-                  return launch_ucol_rc<T, R>(h->rcu_cfg, kick, (const T *)h->f, G, h->shift,
-                                              g, rcdir<R>(h, true), bs);
-                return launch_ucol<T, R>(kick, (const T *)h->f, G, h->shift, g, tu, bs);
+                  return launch_ucol_rc<T, R>(h->rcu_cfg, kick, fin, G, h->shift, g,
+                                              rcdir<R>(h, true), bs);
+                return launch_ucol<T, R>(kick, fin, G, h->shift, g, tu, bs);
               },
               bs));
     CK(h, timed(
@@ -1120,13 +1126,13 @@ static int drift_once(vls_handle *h, bool kick) {
               h, VLS_K_DRIFT,
               [&] {
                 if (h->drift_kind != DRIFT_WINDOW)
-                  return launch_drift_strip<T>(&h->tmS[sl], h->drift_kind, C, (T *)h->f,
+                  return launch_drift_strip<T>(&h->tmS[sl], h->drift_kind, C, fout,
                                                h->idx, (const T *)h->fx, (const T *)h->fy,
                                                h->fp2, h->ch_start, h->ch_len,
                                                (const T *)h->ch_val, h->ndrift,
                                                moment_tables(h), h->partial, h->flag + 1,
                                                h->drift_spins, g, bs);
-                return launch_drift_tma<T>(&h->tmC[sl], C, (T *)h->f, h->idx,
+                return launch_drift_tma<T>(&h->tmC[sl], C, fout, h->idx,
                                            (const T *)h->fx, (const T *)h->fy, h->fp2,
                                            h->ch_start, h->ch_len, (const T *)h->ch_val,
                                            h->ndrift, moment_tables(h), h->partial,
@@ -1189,6 +1195,26 @@ extern "C" int vls_step(vls_handle *h, int32_t nsteps) {
     default:
       return step_impl<float, float>(h, nsteps);
   }
+}
+
+// One linked step from the state f_in, whose shift scan_once has just
+// computed, into f_out (the adjoint's recomputation).
+static int step_between(vls_handle *h, const void *f_in, void *f_out) {
+  int rc;
+  switch (h->prec) {
+    case VLS_FP64:
+      rc = drift_once<double, double>(h, true, f_in, f_out);
+      break;
+    case VLS_FP32_BULK:
+      rc = drift_once<float, double>(h, true, f_in, f_out);
+      break;
+    default:
+      rc = drift_once<float, float>(h, true, f_in, f_out);
+  }
+  if (rc != VLS_OK) return rc;
+  h->time += h->solver.dt;
+  h->step++;
+  return VLS_OK;
 }
 
 // device-side status words, cleared once reported:
@@ -1663,7 +1689,10 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift,
                 : launch_ucol_adj<T>((const T *)fn, b.Gb, b.A, b.B, b.lam, b.sbar, shift, g, tu,
                                      h->st);
   }));
-  CK(h, timed(h, VLS_K_ADJ_MOMENT, [&] { return launch_shift_adj(b.sbar, b.beta, mt, g, h->st); }));
+  // count[1]: the shift transpose's blocks (count[0] is the scan's)
+  CK(h, timed(h, VLS_K_ADJ_MOMENT, [&] {
+    return launch_shift_adj(b.sbar, b.beta, h->count + 1, mt, g, h->st);
+  }));
   b.pending = true;  // added by the next step's readers of lam, or at the end
   return VLS_OK;
 }
@@ -1751,19 +1780,21 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
   CK(h, cudaMemsetAsync(b.lam, 0, cells * sizeof(double), h->st));
   CK(h, cudaMemsetAsync(b.ringb, 0, (size_t)std::max<int64_t>(h->nel, 1) * sizeof(double), h->st));
   CK(h, launch_moment_adj(b.lam, b.beta, mt, g, h->st));
-  // from the state at step a: stash the states of steps a .. b-1, then apply
-  // the transposed steps b-1 .. a
+  // from the state at step a (in h->f): stash the states of steps a .. e-1,
+  // each step reading its state from the stash and writing the next one
+  // there, then apply the transposed steps e-1 .. a.  h->f keeps the state
+  // of step a, and the moments (valid after each step) are those of the
+  // last state stashed.
   auto pass = [&](int64_t a, int64_t e) -> int {
+    CK(h, cudaMemcpyAsync(b.stash[0], h->f, h->esize * cells, cudaMemcpyDeviceToDevice, h->st));
     for (int64_t n = a; n < e; ++n) {
-      CK(h, cudaMemcpyAsync(b.stash[n - a], h->f, h->esize * cells, cudaMemcpyDeviceToDevice,
-                            h->st));
       b.ndrift[n - a] = h->ndrift;
       // the shift of step n, as the step computes it from f_n
       TRY(ensure_moments<T>(h));
       TRY(scan_once(h));
       CK(h, cudaMemcpyAsync(b.shifts + (size_t)(n - a) * g.nr, h->shift, g.nr * sizeof(double),
                             cudaMemcpyDeviceToDevice, h->st));
-      if (n + 1 < e) TRY(vls_step(h, 1));
+      if (n + 1 < e) TRY(step_between(h, b.stash[n - a], b.stash[n + 1 - a]));
     }
     for (int64_t n = e - 1; n >= a; --n)
       TRY(adj_step<T>(h, b, b.stash[n - a], b.ndrift[n - a], b.shifts + (size_t)(n - a) * g.nr));

@@ -190,8 +190,8 @@ cudaError_t launch_ucol_adj(const T *f, double *Gb, double *A, double *B, double
                             double *sbar, const double *shift, const Geometry &g,
                             const DirTables &tu, cudaStream_t st);
 // beta: 2 N_r values (beta, then the moment's transpose per radius)
-cudaError_t launch_shift_adj(const double *sbar, double *beta, const MomentTables &mt,
-                             const Geometry &g, cudaStream_t st);
+cudaError_t launch_shift_adj(const double *sbar, double *beta, unsigned int *count,
+                             const MomentTables &mt, const Geometry &g, cudaStream_t st);
 cudaError_t launch_moment_adj(double *lam, const double *beta, const MomentTables &mt,
                               const Geometry &g, cudaStream_t st);
 // chunked adjoint line kernels (vls_rc.cu), used when rc_adj_supported

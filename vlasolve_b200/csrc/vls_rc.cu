@@ -1159,46 +1159,43 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
   const int ulo = fast ? max((int)floor(-qf) + 1, 0) : 0;
   const int uhi = fast ? min((int)ceil((double)(N - 1) - qf) - 1, N - 1) : -1;
   double sb = 0.0;
-  // shift derivative: sum over this thread's kicked rows
-  if (ro.active) {
-#pragma unroll 1
-    for (int i = 0; i < L; ++i) {
-      const int u = kfirst + i - 1;
-      if (u >= N) break;
-      const double fb = FB[u * LN + ro.ln];
-      if (fast) {
-        if (u < ulo || u > uhi) continue;
-        const double *gp = GS + (ptrdiff_t)(u + o) * LN + ro.ln;
-        sb += fb * (dw[0] * gp[0] + dw[1] * gp[LN] + dw[2] * gp[2 * LN] + dw[3] * gp[3 * LN]);
-      } else {
-        const double newU = __ldg(g.U + u) + sft;
-        if (!(newU > g.u0 && newU < g.umax)) continue;
-        const double y = (newU - g.su) * g.hu;
-        const double yf = floor(y);
-        double ww[4], dd[4];
-        adj_kick_weights(y - yf, ww, dd);
-        const int Ny = 1 + (int)yf;
-        for (int m = 0; m < 4; ++m)
-          if (Ny - 1 + m < M) sb += fb * dd[m] * GS[(Ny - 1 + m) * LN + ro.ln];
-      }
-    }
-  }
-  sb *= g.hu;
-  // ḡ: gather when every column of the block is in fraction form
-  const bool scatter = __syncthreads_or(ro.active && colok && !fast);
-  double gk[L];
   double g0 = 0.0, gM = 0.0;
+  // gather when every column of the block is in fraction form
+  const bool scatter = __syncthreads_or(ro.active && colok && !fast);
   if (!scatter) {
+    // Fraction form, from registers: row u of f̄' (u in [ulo, uhi], else 0)
+    // kicks to rows u + o .. u + o + 3 of g.  The thread's own rows
+    // u = kfirst - 1 + i are in v; the taps of the derivative, g rows
+    // kfirst - 1 + o + t (t = 0 .. L + 2), and the rows of f̄' the gather
+    // reads, kfirst - o - 3 + t, are read once each, in order (outside
+    // [0, M] the g index is clamped: its f̄' factor is zero there).
+    const int gb = kfirst - 1 + o;
+    auto gtap = [&](int t) { return GS[min(max(gb + t, 0), M) * LN + ro.ln]; };
+    double t0 = gtap(0), t1 = gtap(1), t2 = gtap(2);
 #pragma unroll
     for (int i = 0; i < L; ++i) {
-      const int k = kfirst + i;
-      double acc = 0.0;
+      const double t3 = gtap(i + 3);
+      const int u = kfirst - 1 + i;
+      const double fb = (u >= ulo && u <= uhi) ? FB[u * LN + ro.ln] : 0.0;
+      sb = rfma(fb, dw[0] * t0 + dw[1] * t1 + dw[2] * t2 + dw[3] * t3, sb);
+      t0 = t1;
+      t1 = t2;
+      t2 = t3;
+    }
+    const int fbase = kfirst - o - 3;
+    auto ftap = [&](int t) {
+      const int u = fbase + t;
+      return (u >= ulo && u <= uhi) ? FB[u * LN + ro.ln] : 0.0;
+    };
+    double a0 = ftap(0), a1 = ftap(1), a2 = ftap(2);
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int u = k - o - m;
-        if (u >= ulo && u <= uhi) acc += w[m] * FB[u * LN + ro.ln];
-      }
-      gk[i] = acc;
+    for (int i = 0; i < L; ++i) {
+      // row k = kfirst + i takes f̄' rows k - o - m, m = 0 .. 3
+      const double a3 = ftap(i + 3);
+      v[i] = w[0] * a3 + w[1] * a2 + w[2] * a1 + w[3] * a0;
+      a0 = a1;
+      a1 = a2;
+      a2 = a3;
     }
     if (ro.s == 0)
       for (int m = 0; m < 4; ++m) {
@@ -1211,7 +1208,32 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
         if (u >= ulo && u <= uhi) gM += w[m] * FB[u * LN + ro.ln];
       }
   } else {
+    // shift derivative: sum over this thread's kicked rows
+    if (ro.active) {
+#pragma unroll 1
+      for (int i = 0; i < L; ++i) {
+        const int u = kfirst + i - 1;
+        if (u >= N) break;
+        const double fb = FB[u * LN + ro.ln];
+        if (fast) {
+          if (u < ulo || u > uhi) continue;
+          const double *gp = GS + (ptrdiff_t)(u + o) * LN + ro.ln;
+          sb += fb * (dw[0] * gp[0] + dw[1] * gp[LN] + dw[2] * gp[2 * LN] + dw[3] * gp[3 * LN]);
+        } else {
+          const double newU = __ldg(g.U + u) + sft;
+          if (!(newU > g.u0 && newU < g.umax)) continue;
+          const double y = (newU - g.su) * g.hu;
+          const double yf = floor(y);
+          double ww[4], dd[4];
+          adj_kick_weights(y - yf, ww, dd);
+          const int Ny = 1 + (int)yf;
+          for (int m = 0; m < 4; ++m)
+            if (Ny - 1 + m < M) sb += fb * dd[m] * GS[(Ny - 1 + m) * LN + ro.ln];
+        }
+      }
+    }
     // shared-memory scatter into GS (g is no longer needed)
+    __syncthreads();
     for (int e = threadIdx.x; e < (M + 1) * LN; e += blockDim.x) GS[e] = 0.0;
     __syncthreads();
     if (ro.active) {
@@ -1238,10 +1260,11 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
     }
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < L; ++i) gk[i] = GS[min(kfirst + i, M) * LN + ro.ln];
+    for (int i = 0; i < L; ++i) v[i] = GS[min(kfirst + i, M) * LN + ro.ln];
     g0 = GS[ro.ln];
     gM = GS[(M - 1) * LN + ro.ln];
   }
+  sb *= g.hu;
   // s̄ of the column, summed over its chunks in chunk order
   __syncthreads();
   if (ro.active) F[ro.s * LN + ro.ln] = sb;
@@ -1252,9 +1275,7 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
     sbar[(size_t)j * g.nr + r] = tot;
   }
   __syncthreads();
-  // 4. λ = P_u^T ḡ
-#pragma unroll
-  for (int i = 0; i < L; ++i) v[i] = gk[i];
+  // 4. λ = P_u^T ḡ (ḡ in v)
   rc_solve_adj<CF>(v, ro, E, F, t, ro.s == 0 ? g0 : 0.0, ro.s == S - 1 ? gM : 0.0);
   if (ro.active && colok) {
     double *lc = lam + (size_t)j * N * g.nr + r;
