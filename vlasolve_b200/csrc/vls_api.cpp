@@ -1071,14 +1071,16 @@ const RcDir<float> &rcdir<float>(const vls_handle *h, bool u) {
   return u ? h->rcu_f : h->rcr_f;
 }
 
-// One split step: f_out = D P_r P_u Kick(P_u f_in).  f_in and f_out are the
-// handle's grid unless given (the adjoint's recomputation steps from one
-// stored state into the next); they may be the same buffer.
+// One split step: f_out = D P_r P_u Kick(P_u f_in).  f_in, f_out and the
+// kick's shift are the handle's unless given (the adjoint's recomputation
+// steps from one stored state into the next with the shift it stored); f_in
+// and f_out may be the same buffer.
 template <typename T, typename R>
 static int drift_once(vls_handle *h, bool kick, const void *f_in = nullptr,
-                      void *f_out = nullptr) {
+                      void *f_out = nullptr, const double *shift = nullptr) {
   const T *fin = (const T *)(f_in ? f_in : h->f);
   T *fout = (T *)(f_out ? f_out : h->f);
+  const double *sft = shift ? shift : h->shift;
   const DirTables tu = dir_tables(h->tu, h->rp_u, h->q_u);
   const DirTables tr = dir_tables(h->tr, h->rp_r, h->q_r);
   const size_t gslot = (size_t)h->B * (h->co.nu + 2) * h->gp;
@@ -1097,9 +1099,9 @@ static int drift_once(vls_handle *h, bool kick, const void *f_in = nullptr,
               h, kick ? VLS_K_UCOL_KICK : VLS_K_UCOL,
               [&] {
                 if (h->rcu_cfg >= 0)
-                  return launch_ucol_rc<T, R>(h->rcu_cfg, kick, fin, G, h->shift, g,
+                  return launch_ucol_rc<T, R>(h->rcu_cfg, kick, fin, G, sft, g,
                                               rcdir<R>(h, true), bs);
-                return launch_ucol<T, R>(kick, fin, G, h->shift, g, tu, bs);
+                return launch_ucol<T, R>(kick, fin, G, sft, g, tu, bs);
               },
               bs));
     CK(h, timed(
@@ -1160,11 +1162,13 @@ static int ensure_moments(vls_handle *h) {
   return VLS_OK;
 }
 
-static int scan_once(vls_handle *h) {
+// shift_out: where the shift goes (the handle's unless given)
+static int scan_once(vls_handle *h, double *shift_out = nullptr) {
   const Geometry g = geometry(h);
   CK(h, timed(h, VLS_K_SCAN, [&] {
        return launch_scan(h->partial, moment_tables(h), h->T2, h->bins, h->Mr,
-                          h->shift, h->mtot, h->count, h->flag + 2, g, h->st);
+                          shift_out ? shift_out : h->shift, h->mtot, h->count, h->flag + 2,
+                          g, h->st);
      }));
   return VLS_OK;
 }
@@ -1198,18 +1202,18 @@ extern "C" int vls_step(vls_handle *h, int32_t nsteps) {
 }
 
 // One linked step from the state f_in, whose shift scan_once has just
-// computed, into f_out (the adjoint's recomputation).
-static int step_between(vls_handle *h, const void *f_in, void *f_out) {
+// computed into `shift`, to f_out (the adjoint's recomputation).
+static int step_between(vls_handle *h, const void *f_in, void *f_out, const double *shift) {
   int rc;
   switch (h->prec) {
     case VLS_FP64:
-      rc = drift_once<double, double>(h, true, f_in, f_out);
+      rc = drift_once<double, double>(h, true, f_in, f_out, shift);
       break;
     case VLS_FP32_BULK:
-      rc = drift_once<float, double>(h, true, f_in, f_out);
+      rc = drift_once<float, double>(h, true, f_in, f_out, shift);
       break;
     default:
-      rc = drift_once<float, float>(h, true, f_in, f_out);
+      rc = drift_once<float, float>(h, true, f_in, f_out, shift);
   }
   if (rc != VLS_OK) return rc;
   h->time += h->solver.dt;
@@ -1789,12 +1793,12 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
     CK(h, cudaMemcpyAsync(b.stash[0], h->f, h->esize * cells, cudaMemcpyDeviceToDevice, h->st));
     for (int64_t n = a; n < e; ++n) {
       b.ndrift[n - a] = h->ndrift;
-      // the shift of step n, as the step computes it from f_n
+      // the shift of step n, as the step computes it from f_n, kept for the
+      // transposed step
+      double *sn = b.shifts + (size_t)(n - a) * g.nr;
       TRY(ensure_moments<T>(h));
-      TRY(scan_once(h));
-      CK(h, cudaMemcpyAsync(b.shifts + (size_t)(n - a) * g.nr, h->shift, g.nr * sizeof(double),
-                            cudaMemcpyDeviceToDevice, h->st));
-      if (n + 1 < e) TRY(step_between(h, b.stash[n - a], b.stash[n + 1 - a]));
+      TRY(scan_once(h, sn));
+      if (n + 1 < e) TRY(step_between(h, b.stash[n - a], b.stash[n + 1 - a], sn));
     }
     for (int64_t n = e - 1; n >= a; --n)
       TRY(adj_step<T>(h, b, b.stash[n - a], b.ndrift[n - a], b.shifts + (size_t)(n - a) * g.nr));
