@@ -236,6 +236,40 @@ def test_adjoint_random_directions_match_central_differences():
     assert abs(pred - fd) <= 1e-6 * abs(fd), (pred, fd)
 
 
+def test_adjoint_with_the_gathers_long_row_blocks():
+    """A grid of 513 x 509 x 136 vertices has enough threads for the gathers'
+    long row blocks (16 node rows per thread in the cell-ordered FP64 gather,
+    32 in the entry-ordered FP32 one; the small grids above take 8 and 16):
+    a seeded random direction over every cell against central differences of
+    FP64 runs (1e-6 relative), and the FP32-storage transpose against the
+    FP64 one on every cell (1e-4 of the largest)."""
+    from vlasolve_b200 import VlasovSolver21Spline
+    c = cfg(pres=512, ures=(508, 136), dt=0.01)
+    nsteps = 2
+    s = VlasovSolver21Spline(c, precision="fp64")
+    f0, c0 = s.f, s.chains()["val"].copy()
+    assert f0.shape == (136, 509, 513)
+    rng = np.random.default_rng(20261204)
+    dbins = rng.standard_normal(s.nr)
+    s.adjoint_forward(nsteps, nsteps)
+    df0, _ = s.adjoint_backward(dbins)
+    df0 = np.asarray(df0).reshape(f0.shape)
+    v = f0 * rng.standard_normal(f0.shape)
+    pred = float(np.sum(df0 * v))
+    h = 1e-5
+    fd = (_loss(s, f0 + h * v, c0, nsteps, dbins) -
+          _loss(s, f0 - h * v, c0, nsteps, dbins)) / (2 * h)
+    print(f"adjoint {pred:.12e} fd {fd:.12e}")
+    assert abs(pred - fd) <= 1e-6 * abs(fd), (pred, fd)
+    s.close()
+    s32 = VlasovSolver21Spline(c, precision="fp32")
+    s32.adjoint_forward(nsteps, nsteps)
+    d32, _ = s32.adjoint_backward(dbins)
+    d32 = np.asarray(d32).reshape(f0.shape)
+    s32.close()
+    assert np.max(np.abs(d32 - df0)) <= 1e-4 * np.max(np.abs(df0))
+
+
 def test_fp32_adjoint_matches_fp64_adjoint_cell_by_cell():
     """The FP32-storage handle's transposed step (the entry-ordered gather)
     against the FP64 handle's (the cell-ordered gather) on every cell of

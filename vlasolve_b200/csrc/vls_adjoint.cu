@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "vls_dd.cuh"
 #include "vls_internal.h"
@@ -709,6 +710,28 @@ cudaError_t launch_chain_adj(const double *lam, const double *mB, const MomentTa
   return cudaGetLastError();
 }
 
+// SMs of the current device, looked up once per device
+static int device_sms() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    cache[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+
+// threads of a gather with R node rows and Q columns per thread, in waves of
+// 1024 resident threads per SM
+static double gather_waves(const Geometry &g, int Q, int R) {
+  const double cols = 32.0 * ((g.pc + 32 * Q - 1) / (32 * Q));
+  const double rows = 4.0 * ((g.nu + 3 + 4 * R - 1) / (4 * R));
+  return cols * rows * g.nj / (1024.0 * device_sms());
+}
+
 template <typename T>
 cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const MomentTables &mt,
                                     const double *tv, double *Cb, const uint32_t *ends,
@@ -716,15 +739,21 @@ cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const M
                                     const T *fy, const int32_t *idx, const uint2 *fp2,
                                     const int32_t *t_idx, const double *t_x,
                                     const double *t_y, const Geometry &g, cudaStream_t st) {
-  // 8 node rows x 3 columns per thread: 0.189 ms per transposed step on
-  // 257 x 257 x 128 against 0.195 / 0.226 for 2 / 4 columns, 0.198 / 0.264
-  // for 16 / 32 rows and 0.215 for fixed blocks of rows
-  constexpr int Q = 3, R = 8;
-  const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
-                  (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
-  drift_adj_sweep_kernel<T, R, Q><<<grid, dim3(32, 4), 0, st>>>(
-      lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2, t_idx, t_x, t_y, g);
-  return cudaGetLastError();
+  // 3 columns per thread; 16 node rows where that still gives 4 waves of
+  // threads, else 8.  Per transposed step: 257 x 257 x 128 8 rows 0.190 ms
+  // (16 rows 0.199, 2 / 4 columns 0.195 / 0.226); 513 x 513 x 256 16 rows
+  // 1.101 ms (8 / 32 rows 1.192 / 1.133); 1025 x 1025 x 64 16 rows 1.045 ms
+  // (8 / 32 rows 1.101 / 1.102)
+  constexpr int Q = 3;
+  auto go = [&](auto kern, int R) {
+    const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
+                    (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
+    kern<<<grid, dim3(32, 4), 0, st>>>(lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2,
+                                       t_idx, t_x, t_y, g);
+    return cudaGetLastError();
+  };
+  if (gather_waves(g, Q, 16) >= 4.0) return go(drift_adj_sweep_kernel<T, 16, Q>, 16);
+  return go(drift_adj_sweep_kernel<T, 8, Q>, 8);
 }
 
 static dim3 slice_grid(const Geometry &g) {
@@ -749,16 +778,20 @@ cudaError_t launch_drift_adj_gather_perm(const double *vperm, const uint2 *geo, 
                                          const uint32_t *ends, const int64_t *ebase,
                                          const int32_t *t_idx, const double *t_x,
                                          const double *t_y, const Geometry &g, cudaStream_t st) {
-  // 16 node rows x 2 columns per thread: 0.182 ms per transposed step
-  // (permutation included) on 257 x 257 x 128 against 0.187 / 0.196 for 8 /
-  // 32 rows, 0.188 / 0.213 for 3 / 4 columns and 0.207 for fixed blocks of
-  // rows
-  constexpr int Q = 2, R = 16;
-  const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
-                  (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
-  drift_adj_sweep_perm_kernel<R, Q><<<grid, dim3(32, 4), 0, st>>>(vperm, geo, Cb, ends, ebase,
-                                                                   t_idx, t_x, t_y, g);
-  return cudaGetLastError();
+  // 2 columns per thread; 32 node rows where that still gives 4 waves of
+  // threads, else 16.  Per transposed step, the permutation included:
+  // 257 x 257 x 128 16 rows 0.185 ms (8 / 32 rows 0.188 / 0.196, 3 / 4
+  // columns 0.188 / 0.213); 513 x 513 x 256 32 rows 0.981 ms (16 rows
+  // 1.006); 1025 x 1025 x 64 32 rows 0.934 ms (16 rows 0.959)
+  constexpr int Q = 2;
+  auto go = [&](auto kern, int R) {
+    const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
+                    (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
+    kern<<<grid, dim3(32, 4), 0, st>>>(vperm, geo, Cb, ends, ebase, t_idx, t_x, t_y, g);
+    return cudaGetLastError();
+  };
+  if (gather_waves(g, Q, 32) >= 4.0) return go(drift_adj_sweep_perm_kernel<32, Q>, 32);
+  return go(drift_adj_sweep_perm_kernel<16, Q>, 16);
 }
 
 #define VLS_INV_INST(T)                                                                       \
