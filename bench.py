@@ -420,8 +420,8 @@ def adjoint_block(nsteps, K):
     whole backward pass of the autograd function (step adjoint plus the
     initial-state map), the step adjoint alone (vls_adjoint_backward, with
     its recomputation), and the plain forward of the same steps, the last two
-    as device time on the solver's stream (and wall time);
-    adjoint_over_forward is the step adjoint over that forward."""
+    as device time on the solver's stream (and wall time), medians of three
+    runs each; adjoint_over_forward is the step adjoint over that forward."""
     import numpy as np
     import torch
     from vlasolve_b200 import VlasovSolver21Spline
@@ -448,37 +448,44 @@ def adjoint_block(nsteps, K):
         t2 = time.perf_counter()
         grads[prec] = th.grad.numpy().copy()
         # the step adjoint alone (recomputation included, initial-state map
-        # excluded): one more backward pass with the same seed
+        # excluded): three more backward passes with the same seed, and three
+        # plain forward runs of the same steps; the medians are reported
         s = p.solver
         dbins = np.zeros(s.nr)
         dbins[:-1] = (torch.as_tensor(rho.detach()) - torch.as_tensor(target)).numpy()
         stream = torch.cuda.ExternalStream(s.stream_ptr())
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        s.sync()
-        ta = time.perf_counter()
-        ev[0].record(stream)
-        s.adjoint_backward(dbins)
-        ev[1].record(stream)
-        s.sync()
-        tb = time.perf_counter()
-        # plain forward of the same steps
-        s.set_init_params(**dict(zip(p.params, map(float, theta))))
-        s.sync()
-        t3 = time.perf_counter()
-        ev[2].record(stream)
-        s.step(nsteps)
-        ev[3].record(stream)
-        s.sync()
-        t4 = time.perf_counter()
-        torch.cuda.synchronize()
-        adj_dev = ev[0].elapsed_time(ev[1]) * 1e-3
-        fwd_dev = ev[2].elapsed_time(ev[3]) * 1e-3
+
+        def timed_run(fn):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            s.sync()
+            w0 = time.perf_counter()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            s.sync()
+            w1 = time.perf_counter()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) * 1e-3, w1 - w0
+
+        def forward():
+            s.set_init_params(**dict(zip(p.params, map(float, theta))))
+            s.sync()
+            return timed_run(lambda: s.step(nsteps))
+
+        adj = [timed_run(lambda: s.adjoint_backward(dbins)) for _ in range(3)]
+        fwd = [forward() for _ in range(3)]
+        adj_dev = float(np.median([a[0] for a in adj]))
+        fwd_dev = float(np.median([f[0] for f in fwd]))
         # device times (CUDA events on the solver's stream) and the wall times
         # around the same calls (host launch overhead included)
         out[prec] = {"grad": grads[prec].tolist(), "loss": float(L.detach()),
                      "forward_checkpointed_s": t1 - t0, "backward_s": t2 - t1,
                      "step_adjoint_s": adj_dev, "forward_s": fwd_dev,
-                     "step_adjoint_wall_s": tb - ta, "forward_wall_s": t4 - t3,
+                     "step_adjoint_runs_s": [a[0] for a in adj],
+                     "forward_runs_s": [f[0] for f in fwd],
+                     "step_adjoint_wall_s": float(np.median([a[1] for a in adj])),
+                     "forward_wall_s": float(np.median([f[1] for f in fwd])),
                      "adjoint_over_forward": adj_dev / fwd_dev}
         if prec == "fp64":
             fd = np.zeros(3)

@@ -236,20 +236,22 @@ def test_adjoint_random_directions_match_central_differences():
     assert abs(pred - fd) <= 1e-6 * abs(fd), (pred, fd)
 
 
-def test_adjoint_with_the_gathers_long_row_blocks():
-    """A grid of 513 x 509 x 136 vertices has enough threads for the gathers'
-    long row blocks (16 node rows per thread in the cell-ordered FP64 gather,
-    32 in the entry-ordered FP32 one; the small grids above take 8 and 16):
-    a seeded random direction over every cell against central differences of
-    FP64 runs (1e-6 relative), and the FP32-storage transpose against the
-    FP64 one on every cell (1e-4 of the largest)."""
+@pytest.mark.parametrize("nj", [72, 136])
+def test_adjoint_on_grids_past_the_l2(nj):
+    """Grids of 513 x 509 x nj vertices (150 and 284 MB of FP64 adjoint
+    field), whose FP32 handles take the entry-ordered gather (16 node rows
+    per thread at nj = 72, 32 at nj = 136; the FP64 cell-ordered gather
+    takes 32 rows per warp at both): a seeded random direction over every cell
+    against central differences of FP64 runs (1e-6 relative), and the
+    FP32-storage transpose against the FP64 one on every cell (1e-4 of the
+    largest)."""
     from vlasolve_b200 import VlasovSolver21Spline
-    c = cfg(pres=512, ures=(508, 136), dt=0.01)
+    c = cfg(pres=512, ures=(508, nj), dt=0.01)
     nsteps = 2
     s = VlasovSolver21Spline(c, precision="fp64")
     f0, c0 = s.f, s.chains()["val"].copy()
-    assert f0.shape == (136, 509, 513)
-    rng = np.random.default_rng(20261204)
+    assert f0.shape == (nj, 509, 513)
+    rng = np.random.default_rng(20261204 + nj)
     dbins = rng.standard_normal(s.nr)
     s.adjoint_forward(nsteps, nsteps)
     df0, _ = s.adjoint_backward(dbins)
@@ -271,8 +273,8 @@ def test_adjoint_with_the_gathers_long_row_blocks():
 
 
 def test_fp32_adjoint_matches_fp64_adjoint_cell_by_cell():
-    """The FP32-storage handle's transposed step (the entry-ordered gather)
-    against the FP64 handle's (the cell-ordered gather) on every cell of
+    """The FP32-storage handle's transposed step (packed footpoint words)
+    against the FP64 handle's (FP64 fractions) on every cell of
     dL/df0 and every chain element: the two differ only by the FP32 rounding
     of the forward states they linearise around."""
     out = []

@@ -464,55 +464,17 @@ __device__ __forceinline__ double bweight(int m, double t) {
   return (m == 0 || m == 3) ? bv2d(s) : bv1d(s);
 }
 
-// one entry of the inverse map: its value (cells: lam plus the pending
-// moment term), base column and fractions
-template <typename T>
-__device__ __forceinline__ void inv_entry(uint32_t id, const double *__restrict__ lam,
-                                          const double *__restrict__ mB, const MomentTables &mt,
-                                          double wjj, const double *__restrict__ tv,
-                                          size_t cbase, const T *__restrict__ fx,
-                                          const T *__restrict__ fy,
-                                          const int32_t *__restrict__ idx,
-                                          const uint2 *__restrict__ fp2,
-                                          const int32_t *__restrict__ t_idx,
-                                          const double *__restrict__ t_x,
-                                          const double *__restrict__ t_y, int nr, double &v,
-                                          double &x, double &y, int &rI) {
-  if (id & INV_TAIL) {
-    const uint32_t c = id & ~INV_TAIL;
-    v = tv[c];
-    rI = t_idx[c] & 0xffff;
-    x = t_x[c];
-    y = t_y[c];
-    return;
-  }
-  const int u = (int)(id >> 16), r = (int)(id & 0xffffu);
-  const size_t i = cbase + (size_t)u * nr + r;
-  v = lam[i];
-  if (mB) v += wjj * mt.bu[u] * mB[r];
-  if (sizeof(T) == 8) {
-    rI = idx[i] & 0xffff;
-    x = (double)fx[i];
-    y = (double)fy[i];
-  } else {
-    const uint2 w = fp2[i];
-    rI = (int)(w.x >> AFP_FBITS);
-    const uint32_t m = (1u << AFP_FBITS) - 1u;
-    x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
-    y = (double)(__uint_as_float(0x3F800000u | ((w.y & m) << 2)) - 1.0f);
-  }
-}
-
 // Cb[j][p][q] = sum over the buckets (p - a, q - b), a, b = 0..3, of
-// lam * w_a(y) w_b(x) / 36 (the gathers below, sweep_nodes).
+// lam * w_a(y) w_b(x) / 36, by one of two gathers: lane_nodes (one lane per
+// bucket column, entries read through their cell index) or sweep_nodes (a
+// thread per block of node rows and columns, entries read in entry order).
 
-// Entry-ordered form of the gather (FP32 handles).  The packed footpoint
-// word of each entry (a chain tail is GEO_TAIL, chain id) is stored once in entry order when the map is built, and each
-// transposed step first permutes its values into entry order (vperm: lam
-// plus the pending moment term, or the tail's ring adjoint), so that a
-// visit of the gather reads two arrays at the same index.  For FP64
-// handles the entry-ordered fractions (16 B) cost more than they save, and
-// the cell-ordered gather above is used.
+// Entry order (FP32 handles whose lam does not fit in L2).  The packed
+// footpoint word of each entry (a chain tail is GEO_TAIL, chain id) is
+// stored once in entry order when the map is built, and each transposed
+// step first permutes its values into entry order (vperm: lam plus the
+// pending moment term, or the tail's ring adjoint), so that a visit of the
+// gather reads two arrays at the same index.
 constexpr uint32_t GEO_TAIL = 0xFFFFFFFFu;
 
 __global__ void inv_geo_kernel(const uint32_t *__restrict__ ent,
@@ -557,17 +519,17 @@ __global__ void inv_perm_kernel(const uint32_t *__restrict__ ent,
   }
 }
 
-// The gathers.  A thread sums the nodes of RB rows p0.. and Q columns q0..,
-// walking the base rows p0-3 .. p0+RB-1 in order with the sums of the four
-// node rows pb .. pb+3 in registers: node row pb is complete once base row pb
-// is done (base rows pb-3 .. pb are the only ones reaching it) and is
-// written then.  The buckets of one base row reaching the Q columns are
-// adjacent, one contiguous run of entries.  Every node receives its
-// contributions in a fixed order (base rows ascending, entries in bucket
-// order), so the result does not depend on scheduling.  The sliding window
-// keeps four rows of sums per column in registers (a block of RB rows held
-// whole measured 8-12 % slower: more registers, fewer warps, more visits of
-// each entry).  entry(e, v, x, y, rI) reads entry e of the slice.
+// The entry-ordered gather.  A thread sums the nodes of RB rows p0.. and Q
+// columns q0.., walking the base rows p0-3 .. p0+RB-1 in order with the sums
+// of the four node rows pb .. pb+3 in registers: node row pb is complete
+// once base row pb is done (base rows pb-3 .. pb are the only ones reaching
+// it) and is written then.  The buckets of one base row reaching the Q
+// columns are adjacent, one contiguous run of entries.  Every node receives
+// its contributions in a fixed order (base rows ascending, entries in
+// bucket order), so the result does not depend on scheduling.  The sliding
+// window keeps four rows of sums per column in registers (a block of RB
+// rows held whole measured 8-12 % slower: more registers, fewer warps, more
+// visits of each entry).  entry(e, v, x, y, rI) reads entry e of the slice.
 template <int RB, int Q, class Entry>
 __device__ __forceinline__ void sweep_nodes(const Entry &entry, double *__restrict__ Cbj,
                                             const uint32_t *__restrict__ endj, int p0, int q0,
@@ -614,32 +576,6 @@ __device__ __forceinline__ void sweep_nodes(const Entry &entry, double *__restri
   }
 }
 
-template <typename T, int RB, int Q>
-__global__ void __launch_bounds__(128)
-    drift_adj_sweep_kernel(const double *__restrict__ lam, const double *__restrict__ mB,
-                           MomentTables mt, const double *__restrict__ tv,
-                           double *__restrict__ Cb, const uint32_t *__restrict__ ends,
-                           const uint32_t *__restrict__ ent, const int64_t *__restrict__ ebase,
-                           const T *__restrict__ fx, const T *__restrict__ fy,
-                           const int32_t *__restrict__ idx, const uint2 *__restrict__ fp2,
-                           const int32_t *__restrict__ t_idx, const double *__restrict__ t_x,
-                           const double *__restrict__ t_y, Geometry g) {
-  const int q0 = (blockIdx.x * 32 + threadIdx.x) * Q;
-  const int p0 = (blockIdx.y * blockDim.y + threadIdx.y) * RB;
-  const int j = blockIdx.z;
-  if (q0 >= g.pc || p0 >= g.nu + 3) return;
-  const size_t S = (size_t)g.nr * g.nu;
-  const uint32_t *entj = ent + ebase[j];
-  const size_t cbase = (size_t)j * S;
-  const double wjj = mB ? mt.wj[j] : 0.0;
-  sweep_nodes<RB, Q>(
-      [&](uint32_t e, double &v, double &x, double &y, int &rI) {
-        inv_entry<T>(entj[e], lam, mB, mt, wjj, tv, cbase, fx, fy, idx, fp2, t_idx, t_x, t_y,
-                     g.nr, v, x, y, rI);
-      },
-      Cb + (size_t)j * (g.nu + 3) * g.pc, ends + (size_t)j * S, p0, q0, g);
-}
-
 template <int RB, int Q>
 __global__ void __launch_bounds__(128)
     drift_adj_sweep_perm_kernel(const double *__restrict__ vperm, const uint2 *__restrict__ geo,
@@ -672,6 +608,135 @@ __global__ void __launch_bounds__(128)
         }
       },
       Cb + (size_t)j * (g.nu + 3) * g.pc, ends + (size_t)j * S, p0, q0, g);
+}
+
+// The cell-ordered gather.  A warp covers 32 consecutive bucket
+// columns cb = c0 - 3 + lane of one block of node rows; each lane visits
+// only its own bucket of each base row (every entry of the block once per
+// pass, no per-column tests) and adds the entry's 4 x 4 products into the
+// sums of the node rows pb .. pb + 3 and columns cb .. cb + 3 it holds.  A
+// node row is complete once its own base row is done; node column q then
+// sums the lanes q - b's column-offset-b sums, b = 0 .. 3, by shuffles in
+// that order, and lanes 3 .. 31 write the 29 columns c0 .. c0 + 28.  The
+// summation order is fixed.  entry(e, v, x, y) reads entry e of the slice
+// (its bucket gives the base node).
+template <int RB, class Entry>
+__device__ __forceinline__ void lane_nodes(const Entry &entry, double *__restrict__ Cbj,
+                                           const uint32_t *__restrict__ endj, int p0, int c0,
+                                           const Geometry &g) {
+  const int lane = threadIdx.x & 31;
+  const int cb = c0 - 3 + lane;
+  const bool col_ok = cb >= 0 && cb < g.nr;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  const int pend = min(p0 + RB, g.nu + 3);
+  for (int pb = p0 - 3; pb < pend; ++pb) {
+    if (col_ok && pb >= 0 && pb < g.nu) {
+      const size_t k = (size_t)pb * g.nr + cb;
+      const uint32_t e1 = endj[k];
+      for (uint32_t e = k ? endj[k - 1] : 0u; e < e1; ++e) {
+        double v, x, y;
+        entry(e, v, x, y);
+        const double sy = 1.0 - y, sx = 1.0 - x;
+        const double wy[4] = {bv2d(sy), bv1d(sy), bv1d(y), bv2d(y)};
+        const double vx[4] = {v * bv2d(sx), v * bv1d(sx), v * bv1d(x), v * bv2d(x)};
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(vx[b], wy[a], acc[a][b]);
+      }
+    }
+    // node row pb is complete
+    double t = acc[0][0];
+    t += __shfl_up_sync(0xffffffffu, acc[0][1], 1);
+    t += __shfl_up_sync(0xffffffffu, acc[0][2], 2);
+    t += __shfl_up_sync(0xffffffffu, acc[0][3], 3);
+    if (pb >= p0 && lane >= 3 && cb < g.pc) Cbj[(size_t)pb * g.pc + cb] = t * (1.0 / 36.0);
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      acc[0][b] = acc[1][b];
+      acc[1][b] = acc[2][b];
+      acc[2][b] = acc[3][b];
+      acc[3][b] = 0.0;
+    }
+  }
+}
+
+template <typename T, int RB>
+__global__ void __launch_bounds__(128)
+    drift_adj_lane_kernel(const double *__restrict__ lam, const double *__restrict__ mB,
+                          MomentTables mt, const double *__restrict__ tv,
+                          double *__restrict__ Cb, const uint32_t *__restrict__ ends,
+                          const uint32_t *__restrict__ ent, const int64_t *__restrict__ ebase,
+                          const T *__restrict__ fx, const T *__restrict__ fy,
+                          const uint2 *__restrict__ fp2, const double *__restrict__ t_x,
+                          const double *__restrict__ t_y, Geometry g) {
+  const int c0 = blockIdx.x * 29;
+  const int p0 = (blockIdx.y * blockDim.y + threadIdx.y) * RB;
+  const int j = blockIdx.z;
+  if (p0 >= g.nu + 3) return;  // the whole warp
+  const size_t S = (size_t)g.nr * g.nu;
+  const uint32_t *entj = ent + ebase[j];
+  const size_t cbase = (size_t)j * S;
+  const double wjj = mB ? mt.wj[j] : 0.0;
+  lane_nodes<RB>(
+      [&](uint32_t e, double &v, double &x, double &y) {
+        const uint32_t id = entj[e];
+        if (id & INV_TAIL) {
+          const uint32_t c = id & ~INV_TAIL;
+          v = tv[c];
+          x = t_x[c];
+          y = t_y[c];
+          return;
+        }
+        const int u = (int)(id >> 16), r = (int)(id & 0xffffu);
+        const size_t i = cbase + (size_t)u * g.nr + r;
+        v = lam[i];
+        if (mB) v += wjj * mt.bu[u] * mB[r];
+        if (sizeof(T) == 8) {
+          x = (double)fx[i];
+          y = (double)fy[i];
+        } else {
+          const uint2 w = fp2[i];
+          const uint32_t m = (1u << AFP_FBITS) - 1u;
+          x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
+          y = (double)(__uint_as_float(0x3F800000u | ((w.y & m) << 2)) - 1.0f);
+        }
+      },
+      Cb + (size_t)j * (g.nu + 3) * g.pc, ends + (size_t)j * S, p0, c0, g);
+}
+
+template <int RB>
+__global__ void __launch_bounds__(128)
+    drift_adj_lane_perm_kernel(const double *__restrict__ vperm, const uint2 *__restrict__ geo,
+                               double *__restrict__ Cb, const uint32_t *__restrict__ ends,
+                               const int64_t *__restrict__ ebase, const double *__restrict__ t_x,
+                               const double *__restrict__ t_y, Geometry g) {
+  const int c0 = blockIdx.x * 29;
+  const int p0 = (blockIdx.y * blockDim.y + threadIdx.y) * RB;
+  const int j = blockIdx.z;
+  if (p0 >= g.nu + 3) return;  // the whole warp
+  const size_t S = (size_t)g.nr * g.nu;
+  const int64_t eb = ebase[j];
+  const double *vj = vperm + eb;
+  const uint2 *gj = geo + eb;
+  lane_nodes<RB>(
+      [&](uint32_t e, double &v, double &x, double &y) {
+        v = vj[e];
+        const uint2 w = gj[e];
+        if (w.x == GEO_TAIL) {
+          x = t_x[w.y];
+          y = t_y[w.y];
+        } else {
+          const uint32_t m = (1u << AFP_FBITS) - 1u;
+          x = (double)(__uint_as_float(0x3F800000u | ((w.x & m) << 2)) - 1.0f);
+          y = (double)(__uint_as_float(0x3F800000u | ((w.y & m) << 2)) - 1.0f);
+        }
+      },
+      Cb + (size_t)j * (g.nu + 3) * g.pc, ends + (size_t)j * S, p0, c0, g);
 }
 
 }  // namespace
@@ -732,28 +797,34 @@ static double gather_waves(const Geometry &g, int Q, int R) {
   return cols * rows * g.nj / (1024.0 * device_sms());
 }
 
+// the same for the lane-per-bucket gather (29 node columns per warp)
+static double lane_waves(const Geometry &g, int R) {
+  const double cols = 32.0 * ((g.pc + 28) / 29);
+  const double rows = 4.0 * ((g.nu + 3 + 4 * R - 1) / (4 * R));
+  return cols * rows * g.nj / (1024.0 * device_sms());
+}
+
 template <typename T>
 cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const MomentTables &mt,
                                     const double *tv, double *Cb, const uint32_t *ends,
                                     const uint32_t *ent, const int64_t *ebase, const T *fx,
-                                    const T *fy, const int32_t *idx, const uint2 *fp2,
-                                    const int32_t *t_idx, const double *t_x,
+                                    const T *fy, const uint2 *fp2, const double *t_x,
                                     const double *t_y, const Geometry &g, cudaStream_t st) {
-  // 3 columns per thread; 16 node rows where that still gives 4 waves of
-  // threads, else 8.  Per transposed step: 257 x 257 x 128 8 rows 0.190 ms
-  // (16 rows 0.199, 2 / 4 columns 0.195 / 0.226); 513 x 513 x 256 16 rows
-  // 1.101 ms (8 / 32 rows 1.192 / 1.133); 1025 x 1025 x 64 16 rows 1.045 ms
-  // (8 / 32 rows 1.101 / 1.102)
-  constexpr int Q = 3;
+  // 32 node rows per warp where that still gives 4 waves of threads, else
+  // 16.  Per transposed step, FP64: 257 x 257 x 128 0.163 ms (8 / 32 rows
+  // 0.168 / 0.167; the entry-ordered gather 0.190), 513 x 513 x 256 1.081 ms
+  // (16 rows 1.114; entry-ordered 1.101), 1025 x 1025 x 64 1.056 ms (16 rows
+  // 1.093; entry-ordered 1.044); FP32 257 x 257 x 128 0.155 ms (entry-ordered
+  // with its permutation 0.184)
   auto go = [&](auto kern, int R) {
-    const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
-                    (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)), (unsigned)g.nj);
-    kern<<<grid, dim3(32, 4), 0, st>>>(lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, idx, fp2,
-                                       t_idx, t_x, t_y, g);
+    const dim3 grid((unsigned)((g.pc + 28) / 29), (unsigned)((g.nu + 3 + 4 * R - 1) / (4 * R)),
+                    (unsigned)g.nj);
+    kern<<<grid, dim3(32, 4), 0, st>>>(lam, mB, mt, tv, Cb, ends, ent, ebase, fx, fy, fp2, t_x,
+                                       t_y, g);
     return cudaGetLastError();
   };
-  if (gather_waves(g, Q, 16) >= 4.0) return go(drift_adj_sweep_kernel<T, 16, Q>, 16);
-  return go(drift_adj_sweep_kernel<T, 8, Q>, 8);
+  if (lane_waves(g, 32) >= 4.0) return go(drift_adj_lane_kernel<T, 32>, 32);
+  return go(drift_adj_lane_kernel<T, 16>, 16);
 }
 
 static dim3 slice_grid(const Geometry &g) {
@@ -778,11 +849,6 @@ cudaError_t launch_drift_adj_gather_perm(const double *vperm, const uint2 *geo, 
                                          const uint32_t *ends, const int64_t *ebase,
                                          const int32_t *t_idx, const double *t_x,
                                          const double *t_y, const Geometry &g, cudaStream_t st) {
-  // 2 columns per thread; 32 node rows where that still gives 4 waves of
-  // threads, else 16.  Per transposed step, the permutation included:
-  // 257 x 257 x 128 16 rows 0.185 ms (8 / 32 rows 0.188 / 0.196, 3 / 4
-  // columns 0.188 / 0.213); 513 x 513 x 256 32 rows 0.981 ms (16 rows
-  // 1.006); 1025 x 1025 x 64 32 rows 0.934 ms (16 rows 0.959)
   constexpr int Q = 2;
   auto go = [&](auto kern, int R) {
     const dim3 grid((unsigned)((g.pc + 32 * Q - 1) / (32 * Q)),
@@ -801,8 +867,7 @@ cudaError_t launch_drift_adj_gather_perm(const double *vperm, const uint2 *geo, 
   template cudaError_t launch_drift_adj_gather<T>(                                            \
       const double *, const double *, const MomentTables &, const double *, double *,         \
       const uint32_t *, const uint32_t *, const int64_t *, const T *, const T *,              \
-      const int32_t *, const uint2 *, const int32_t *, const double *,                        \
-      const double *, const Geometry &, cudaStream_t);
+      const uint2 *, const double *, const double *, const Geometry &, cudaStream_t);
 VLS_INV_INST(float)
 
 VLS_INV_INST(double)

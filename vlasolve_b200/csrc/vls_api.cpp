@@ -1605,6 +1605,22 @@ struct AdjBufs {
 // The inverse footpoint map of the current footpoints for the drift's
 // transpose (launch_inv_fill), built once per footpoint set: count, scan,
 // place, order.
+// FP32 handles whose adjoint field (8 B per cell) does not fit in L2 read
+// the drift transpose's entries in entry order, after a permutation pass
+// each step; below that the cell-ordered reads hit L2 and the pass costs
+// more than it saves (FP32 per transposed step: 257 x 257 x 128 0.155 ms
+// cell-ordered against 0.184; 513 x 513 x 256 1.035 against 0.978; 1025 x
+// 1025 x 64 1.015 against 0.933).  FP64 handles read their 16 B of
+// fractions through the cell index at every size.
+template <typename T>
+static bool adj_entry_ordered(vls_handle *h) {
+  if (sizeof(T) != 4) return false;
+  int l2 = 0;
+  if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->solver.device) != cudaSuccess)
+    l2 = 0;
+  return h->cells * sizeof(double) > (size_t)l2;
+}
+
 template <typename T>
 static int ensure_inv(vls_handle *h) {
   if (h->inv_gen == h->fp_gen) return VLS_OK;
@@ -1617,7 +1633,7 @@ static int ensure_inv(vls_handle *h) {
     TRY(adj_alloc(h, &h->inv_ebase, (size_t)(g.nj + 1) * sizeof(int64_t)));
     TRY(adj_alloc(h, &h->inv_chc, (size_t)std::max<int64_t>(nch, 1) * sizeof(int64_t)));
     TRY(adj_alloc(h, &h->inv_tv, (size_t)std::max<int64_t>(nch, 1) * sizeof(double)));
-    if (sizeof(T) == 4) {
+    if (adj_entry_ordered<T>(h)) {
       const size_t ne = h->cells + (size_t)nch;
       TRY(adj_alloc(h, &h->inv_geo, ne * sizeof(uint2)));
       TRY(adj_alloc(h, &h->inv_vperm, ne * sizeof(double)));
@@ -1679,8 +1695,8 @@ static int adj_step(vls_handle *h, AdjBufs &b, const void *fn, int64_t ndrift,
     CK(h, timed(h, VLS_K_ADJ_DRIFT, [&] {
       return launch_drift_adj_gather<T>(b.lam, mB, mt, h->inv_tv, b.Cb, h->inv_ends,
                                         h->inv_ent, h->inv_ebase, (const T *)h->fx,
-                                        (const T *)h->fy, h->idx, h->fp2, h->t_idx,
-                                        h->t_x, h->t_y, g, h->st);
+                                        (const T *)h->fy, h->fp2, h->t_x, h->t_y, g,
+                                        h->st);
     }));
   }
   CK(h, timed(h, VLS_K_ADJ_PRER, [&] {
@@ -1712,11 +1728,12 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
   {
     // chunked transposed line solves where the forward prefilter uses
     // register chunks and the lines fit them; the entry-ordered gather for
-    // FP32 handles, the cell-ordered one for FP64
+    // FP32 handles whose adjoint field does not fit in L2, the cell-ordered
+    // one otherwise
     b.rc = rc_adj_supported(h->tu, h->tr) && h->layout.prefilter != VLS_PREFILTER_SEGMENT;
     b.rcu = rc_dir<double>(h->tu, 2);
     b.rcr = rc_dir<double>(h->tr, 2);
-    b.perm = sizeof(T) == 4;
+    b.perm = adj_entry_ordered<T>(h);
   }
   TRY(ensure_inv<T>(h));
   if (!h->ab_lam || (h->ab_rc != b.rc && !b.rc)) {

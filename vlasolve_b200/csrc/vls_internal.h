@@ -164,16 +164,17 @@ cudaError_t launch_chain_adj(const double *lam, const double *mB, const MomentTa
                              double *ringb, double *tv, const int64_t *ch_cell,
                              const int64_t *ch_start, const int32_t *ch_len, int64_t nch,
                              int64_t ndrift, const Geometry &g, cudaStream_t st);
-// cell-ordered gather (FP64 handles; 8 x 2 C nodes per thread)
+// cell-ordered gather (one lane per bucket column; entries read through
+// their cell index)
 template <typename T>
 cudaError_t launch_drift_adj_gather(const double *lam, const double *mB, const MomentTables &mt,
                                     const double *tv, double *Cb, const uint32_t *ends,
                                     const uint32_t *ent, const int64_t *ebase, const T *fx,
-                                    const T *fy, const int32_t *idx, const uint2 *fp2,
-                                    const int32_t *t_idx, const double *t_x,
+                                    const T *fy, const uint2 *fp2, const double *t_x,
                                     const double *t_y, const Geometry &g, cudaStream_t st);
-// entry-ordered form (FP32 handles): packed words of the entries once per
-// map, values permuted into entry order each step, gather
+// entry-ordered form (FP32 handles whose lam does not fit in L2): packed
+// words of the entries once per map, values permuted into entry order each
+// step, gather
 cudaError_t launch_inv_geo(const uint32_t *ent, const int64_t *ebase, const uint2 *fp2,
                            uint2 *geo, const Geometry &g, cudaStream_t st);
 cudaError_t launch_inv_perm(const uint32_t *ent, const int64_t *ebase, const double *lam,
