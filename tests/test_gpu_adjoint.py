@@ -178,6 +178,24 @@ def test_chunked_adjoint_lines_match_one_thread_per_line():
     np.testing.assert_allclose(g, g_ref, rtol=1e-10)
 
 
+def test_chunked_adjoint_lines_of_1025_vertices():
+    """The same on lines of 1025 vertices in both directions (70-chunk u
+    lines, and r lines in the 4-line blocks of the longest layout), cell by
+    cell on dL/df0."""
+    from vlasolve_b200 import VlasovSolver21Spline
+    c = cfg(pres=1024, ures=(1024, 4), dt=0.01)
+    out = []
+    for layout in (None, {"prefilter": "segment"}):
+        s = VlasovSolver21Spline(c, precision="fp64", layout=layout)
+        assert s.f.shape == (4, 1025, 1025)
+        s.adjoint_forward(3, 3)
+        df0, _ = s.adjoint_backward(np.cos(0.01 * np.arange(s.nr)))
+        out.append(np.asarray(df0).copy())
+        s.close()
+    assert np.max(np.abs(out[1])) > 0
+    np.testing.assert_allclose(out[0], out[1], rtol=0, atol=1e-10 * np.max(np.abs(out[1])))
+
+
 def _kbuf_solver(precision):
     """A small grid with delayed-kernel chains (kernel radius at the third r
     vertex) and footpoints far enough to leave the drift strips."""

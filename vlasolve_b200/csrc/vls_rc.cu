@@ -1330,12 +1330,16 @@ __global__ void __launch_bounds__(CF::NT, CF::MINB)
     for (int k = threadIdx.x; k < N; k += blockDim.x) Gs[(size_t)p * g.nr + k] = tile[p * P + 1 + k];
 }
 
-// u lines: 15-row chunks in 8-line blocks (up to 72 chunks; 12 % faster than
-// 16-line blocks on 513-row lines); r lines: 15-row chunks in 8-line blocks,
-// and lines too long for those in blocks of up to 80 chunks (1025-row lines)
+// u lines: 15-row chunks in 8-line blocks (up to 70 chunks; 12 % faster than
+// 16-line blocks on 513-row lines, and 0.835 against 1.193 ms per
+// transposed step for 4-line blocks on 1025 x 1025 x 64); r lines: 15-row
+// chunks in 8-line blocks up to 38 chunks, longer lines in 4-line blocks of
+// up to 82 chunks (two blocks of 320 threads per SM on 1025-row lines: 0.284
+// against 0.332 ms per transposed step on 1025 x 1025 x 64 for one block of
+// 8 lines)
 using CfgAdjU = RcCfg<15, 8, 576, 1>;
 using CfgAdjR = RcCfg<15, 8, 320, 2>;
-using CfgAdjR2 = RcCfg<15, 8, 640, 1>;
+using CfgAdjR2 = RcCfg<15, 4, 352, 1>;
 
 }  // namespace
 
@@ -1473,7 +1477,8 @@ cudaError_t launch_prer_rc(int cfg, const T *G, T *C, const Geometry &g, const R
 // adjoint line kernels (FP64), layouts CfgAdjU / CfgAdjR / CfgAdjR2; tables
 // from rc_dir<double>(t, 2)
 bool rc_adj_supported(const HostDirTables &tu, const HostDirTables &tr) {
-  return tu.M - 2 > CfgAdjU::L && tr.M - 2 > CfgAdjR::L && cfg_fits<CfgAdjU>(tu.M - 2, tu.kc64) &&
+  return tu.M - 2 > CfgAdjU::L && tr.M - 2 > CfgAdjR::L &&
+         cfg_fits<CfgAdjU>(tu.M - 2, tu.kc64) &&
          (cfg_fits<CfgAdjR>(tr.M - 2, tr.kc64) || cfg_fits<CfgAdjR2>(tr.M - 2, tr.kc64));
 }
 
