@@ -236,6 +236,12 @@ int vls_moments(vls_handle *h, double *bins, double *Mr, double *mtot);
 /* mass of the most recent step's moment (the value the reference prints as
    " (M=...)" each step, vlasovSolver21_spline.hxx:744) */
 int vls_last_mass(vls_handle *h, double *mtot);
+/* the same read without waiting: the copy of the most recent step's mass
+   into *mtot is queued on the handle's stream, and *mtot holds it once a
+   synchronising call (vls_sync, vls_get_f, ...) has returned.  With mtot in
+   page-locked host memory the call returns at once, so a loop that reads
+   every step's mass does not stall the device between steps. */
+int vls_last_mass_async(vls_handle *h, double *mtot);
 
 /* vlasovSolver21::statistics (vlasovSolver21.hxx:627-690) on the current f:
    FP64 device reductions with compensated summation. */

@@ -307,6 +307,28 @@ def test_bad_inputs_report_errors():
         s.load_snapshot("/nonexistent/file.ND")
 
 
+def test_queued_mass_reads_match_the_waiting_ones():
+    """vls_last_mass_async: the mass of every step queued into a page-locked
+    host array equals vls_last_mass after the same step of an identical
+    handle."""
+    import torch
+    g, cfg = load_golden("udf_tiny")
+    a, b = solver(cfg), solver(cfg)
+    want = []
+    for _ in range(5):
+        a.step(1)
+        want.append(a.last_mass())
+    got = torch.zeros(5, dtype=torch.float64).pin_memory().numpy()
+    for i in range(5):
+        b.step(1)
+        b.last_mass_into(got, i)
+    b.sync()
+    np.testing.assert_array_equal(got, np.array(want))
+    assert np.all(got > 0)
+    with pytest.raises(IndexError):
+        b.last_mass_into(got, 5)
+
+
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 @pytest.mark.parametrize("name", ["udf_tiny", "udf_rect_kbuf", "udf_nolink"])
 def test_slice_batches_on_streams_are_bit_identical(name, prec):

@@ -27,7 +27,7 @@ EXPORTED = [
     "vls_dims", "vls_coords", "vls_init_profile", "vls_set_f", "vls_get_f",
     "vls_get_footpoints", "vls_set_footpoints", "vls_get_chains",
     "vls_set_chain_values", "vls_step", "vls_sync", "vls_kernel_launches",
-    "vls_moments", "vls_last_mass", "vls_stats", "vls_get_time", "vls_set_time",
+    "vls_moments", "vls_last_mass", "vls_last_mass_async", "vls_stats", "vls_get_time", "vls_set_time",
     "vls_write_ndfield", "vls_read_ndfield", "vls_stream", "vls_set_profiling",
     "vls_profile_read", "vls_radial_mass_noalloc", "vls_noalloc_last_error",
     "vls_adjoint_forward", "vls_adjoint_backward", "vls_adjoint_set_inner",
@@ -152,6 +152,7 @@ def load(path: str = LIB_PATH):
         "vls_kernel_launches": [H, P(i64)],
         "vls_moments": [H, P(d), P(d), P(d)],
         "vls_last_mass": [H, P(d)],
+        "vls_last_mass_async": [H, P(d)],
         "vls_stats": [H, P(StatsOut)],
         "vls_get_time": [H, P(d), P(i64)],
         "vls_set_time": [H, d, i64],

@@ -1330,6 +1330,13 @@ extern "C" int vls_last_mass(vls_handle *h, double *mtot) {
   return VLS_OK;
 }
 
+extern "C" int vls_last_mass_async(vls_handle *h, double *mtot) {
+  if (!h || !mtot) return VLS_EINVAL;
+  CK(h, cudaSetDevice(h->solver.device));
+  CK(h, cudaMemcpyAsync(mtot, h->mtot, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  return VLS_OK;
+}
+
 // ------------------------------------------------------------------ stats
 static void two_sum_acc(double &s, double &c, double x) {
   const double t = s + x;

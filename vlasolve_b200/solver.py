@@ -349,6 +349,17 @@ class VlasovSolver21Spline:
         self._ck(self._L.vls_last_mass(self._h, ctypes.byref(m)))
         return m.value
 
+    def last_mass_into(self, out: np.ndarray, index: int):
+        """Queue the copy of the most recent step's mass into out[index]
+        (vls_last_mass_async): out is a float64 array, ideally in page-locked
+        memory; the value is there after the next synchronising call."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array")
+        if not 0 <= index < out.size:
+            raise IndexError(index)
+        ptr = ctypes.cast(out.ctypes.data + 8 * index, _P(ctypes.c_double))
+        self._ck(self._L.vls_last_mass_async(self._h, ptr))
+
     def moments(self):
         b, M, t = np.empty(self.nr), np.empty(self.nr), ctypes.c_double()
         self._ck(self._L.vls_moments(self._h, _dptr(b), _dptr(M), ctypes.byref(t)))
