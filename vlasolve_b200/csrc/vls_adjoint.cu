@@ -458,7 +458,7 @@ __global__ void chain_adj_kernel(const double *__restrict__ lam, const double *_
 }
 
 // weight m of the cubic B-spline at fraction t (times 6): m = 0..3 are
-// BV2(1-t), BV1(1-t), BV1(t), BV2(t), as scatter16 computes them
+// BV2(1-t), BV1(1-t), BV1(t), BV2(t), the drift's tap weights
 __device__ __forceinline__ double bweight(int m, double t) {
   const double s = m < 2 ? 1.0 - t : t;
   return (m == 0 || m == 3) ? bv2d(s) : bv1d(s);

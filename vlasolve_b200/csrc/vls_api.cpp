@@ -74,8 +74,8 @@ struct vls_handle {
   cudaEvent_t ev_fork = nullptr, ev_join[8] = {};
   std::vector<int64_t> chain_lo;  // first chain of slice j (size nj + 1)
   // register-resident prefilter tables (per direction and recursion type)
-  // and whether its kernels take this grid; VLS_PREFILTER=segment selects
-  // the shared-memory segment kernels instead
+  // and whether its kernels take this grid (-1: the shared-memory segment
+  // kernels, for longer lines or the segment prefilter layout)
   RcDir<double> rcu_d{}, rcr_d{};
   RcDir<float> rcu_f{}, rcr_f{};
   int rcu_cfg = -1, rcr_cfg = -1;
