@@ -321,6 +321,16 @@ int vls_adjoint_set_inner(vls_handle *h, int32_t inner_every);
    memory only in vls_destroy, so this is also its peak. */
 int vls_device_bytes(vls_handle *h, size_t *bytes);
 int vls_adjoint_inner_used(vls_handle *h, int32_t *inner_every);
+/* For derivatives with respect to init.* parameters by central differences
+   (no counterpart in the reference): with the dL/df0 and dL/dc0 of the last
+   vls_adjoint_backward, *dgrid = <dL/df0, f(plus) - f(minus)> and *dchain =
+   <dL/dc0, c(plus) - c(minus)>, f and c the initial grid and chain values
+   vls_init_profile makes for the two parameter sets (renormalised to their
+   M).  The grids are evaluated on the device with its FP64 math functions,
+   so they differ from vls_init_profile's host grid in the last bits; the
+   handle's state is not touched.  VLS_ESTATE before a backward pass. */
+int vls_adjoint_init_dot(vls_handle *h, const vls_init_desc *plus,
+                         const vls_init_desc *minus, double *dgrid, double *dchain);
 
 /* ---------------------------------------------------------------------------
    Spline level.  localSpline<2, double> (localSpline.hxx:60-503) is the

@@ -66,6 +66,36 @@ def test_fp32_adjoint_matches_fp64_adjoint(precision):
     assert np.all(err <= FP32_RTOL), (g32, g64, err)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_initial_state_contraction_on_the_device_matches_the_host_grids(precision):
+    """vls_adjoint_init_dot (the grids of theta +- h made and contracted with
+    dL/df0 on the device, the chain values on the host) against the same
+    contractions of the host-made initial states (vls_init_profile) on the
+    host, for each parameter; and VLS_ESTATE before a backward pass."""
+    from vlasolve_b200 import _lib
+    p = problem(precision)
+    target = p.run(THETA + DTHETA)
+    rho = p.run(THETA)
+    with pytest.raises(_lib.VlsError) as e:
+        p.solver.adjoint_init_dot(dict(zip(p.params, THETA)), dict(zip(p.params, THETA)))
+    assert e.value.code == _lib.VLS_ESTATE
+    dbins = np.zeros(p.solver.nr)
+    dbins[:-1] = (rho - target) / p.vol
+    df0, dch0 = p.solver.adjoint_backward(dbins)
+    for k in range(len(p.params)):
+        h = p.ic_step * max(1.0, abs(THETA[k]))
+        tp, tm = THETA.copy(), THETA.copy()
+        tp[k] += h
+        tm[k] -= h
+        dg, dc = p.solver.adjoint_init_dot(dict(zip(p.params, tp)), dict(zip(p.params, tm)))
+        fp, cp = p.initial_state(tp)
+        fm, cm = p.initial_state(tm)
+        want_g = float(np.vdot(df0, fp - fm))
+        want_c = float(np.vdot(dch0, cp - cm))
+        assert abs(dg - want_g) <= 1e-7 * abs(want_g), (k, dg, want_g)
+        assert abs(dc - want_c) <= 1e-7 * abs(want_c) + 1e-300, (k, dc, want_c)
+
+
 @pytest.mark.parametrize("K", [1, 4, 12])
 def test_checkpoint_interval_does_not_change_gradient(K):
     p_ref = problem(K=5)

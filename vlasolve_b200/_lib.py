@@ -31,7 +31,7 @@ EXPORTED = [
     "vls_write_ndfield", "vls_read_ndfield", "vls_stream", "vls_set_profiling",
     "vls_profile_read", "vls_radial_mass_noalloc", "vls_noalloc_last_error",
     "vls_adjoint_forward", "vls_adjoint_backward", "vls_adjoint_set_inner",
-    "vls_adjoint_inner_used", "vls_device_bytes", "vls_write_restart",
+    "vls_adjoint_inner_used", "vls_adjoint_init_dot", "vls_device_bytes", "vls_write_restart",
     "vls_restart_info", "vls_read_restart",
     "vls_spline2d_create", "vls_spline2d_destroy", "vls_spline2d_dims", "vls_spline2d_scale",
     "vls_spline2d_assign", "vls_spline2d_build", "vls_spline2d_coefficients",
@@ -169,6 +169,7 @@ def load(path: str = LIB_PATH):
         "vls_adjoint_backward": [H, P(d), i64, P(d), ctypes.c_size_t, P(d), i64],
         "vls_adjoint_set_inner": [H, i32],
         "vls_adjoint_inner_used": [H, P(i32)],
+        "vls_adjoint_init_dot": [H, P(InitDesc), P(InitDesc), P(d), P(d)],
         "vls_device_bytes": [H, P(ctypes.c_size_t)],
         "vls_spline2d_create": [P(Spline2dDesc), i64, P(H)],
         "vls_spline2d_destroy": [H],

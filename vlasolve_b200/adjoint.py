@@ -9,8 +9,9 @@ with checkpoints every K steps and recomputation of each segment.  It yields
 dL/df0 and dL/d(initial chain values).  The map from the parameters theta to
 the initial state (the analytic distribution function and its
 renormalisation, vlasovSolver21::renormalize) is differentiated by central
-differences of that map alone, evaluated in FP64, which costs two
-initial-state evaluations per parameter and no time steps.
+differences of that map alone, in FP64, with no time steps: the two grids
+of each parameter are evaluated on the device and contracted there with
+dL/df0 (vls_adjoint_init_dot).
 
 FinalDensity wraps this as a torch.autograd.Function: forward(theta) returns
 the radial density of the final state, backward(grad) returns grad_theta.
@@ -66,16 +67,16 @@ class DensityProblem:
         g = np.asarray(grad_rho, dtype=np.float64)
         dbins = np.zeros(self.solver.nr)
         dbins[:-1] = g / self.vol
-        df0, dch0 = self.solver.adjoint_backward(dbins)
+        self.solver.adjoint_backward(dbins)
         out = np.zeros(len(self.params))
         for k in range(len(self.params)):
             h = self.ic_step * max(1.0, abs(self.theta[k]))
             tp, tm = self.theta.copy(), self.theta.copy()
             tp[k] += h
             tm[k] -= h
-            fp, cp = self.initial_state(tp)
-            fm, cm = self.initial_state(tm)
-            out[k] = (np.vdot(df0, fp - fm) + np.vdot(dch0, cp - cm)) / (2 * h)
+            dg, dc = self.solver.adjoint_init_dot(dict(zip(self.params, map(float, tp))),
+                                                  dict(zip(self.params, map(float, tm))))
+            out[k] = (dg + dc) / (2 * h)
         return out
 
 

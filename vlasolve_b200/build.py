@@ -18,6 +18,7 @@ DRIVER = os.path.join(HERE, "vlasolve_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["vls_kernels.cu", "vls_rc.cu", "vls_adjoint.cu", "vls_noalloc.cu", "vls_spline.cu",
+           "vls_profile.cu",
            "vls_api.cpp",
            "vls_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

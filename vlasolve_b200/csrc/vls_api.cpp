@@ -132,6 +132,13 @@ struct vls_handle {
   uint2 *inv_geo = nullptr;
   double *inv_vperm = nullptr;
   bool adj_ready = false;
+  // the last backward pass's dL/d(initial chain values), logical order, and
+  // whether ab_lam still holds its dL/df0 (vls_adjoint_init_dot)
+  std::vector<double> adj_dch0;
+  bool adj_grad = false;
+  // coordinates R, U, J, JV, the quadrature's row sums and the dot's block
+  // sums for vls_adjoint_init_dot
+  double *ip_xyz = nullptr, *ip_rows = nullptr, *ip_part = nullptr;
   std::vector<void *> adj_allocs;
 };
 
@@ -1524,7 +1531,10 @@ extern "C" int vls_read_ndfield(vls_handle *h, const char *path) {
 // Device buffers of the adjoint stay with the handle between runs (every
 // forward/backward pair of an optimisation loop would otherwise allocate and
 // free ~10 grids); vls_destroy frees them.
-static void adj_release(vls_handle *h) { h->adj_ready = false; }
+static void adj_release(vls_handle *h) {
+  h->adj_ready = false;
+  h->adj_grad = false;
+}
 
 template <typename P>
 static int adj_alloc(vls_handle *h, P **p, size_t bytes) {
@@ -1860,17 +1870,104 @@ static int adjoint_backward_impl(vls_handle *h, const double *dbins, double *df0
     CK(h, cudaMemcpyAsync(rb.data(), b.ringb, rb.size() * sizeof(double),
                           cudaMemcpyDeviceToHost, h->st));
   CK(h, cudaStreamSynchronize(h->st));
-  if (dchain0) {
+  h->adj_dch0.assign((size_t)h->nel, 0.0);
+  {
     const int64_t nd0 = h->adj_ck[0].ndrift;
     for (int64_t c = 0; c < h->nch; ++c) {
       const int64_t s0 = h->ch_start_h[c];
       const int32_t L = h->ch_len_h[c];
-      for (int32_t e = 0; e < L; e++) dchain0[s0 + e] = rb[s0 + (nd0 + e) % L];
+      for (int32_t e = 0; e < L; e++) h->adj_dch0[s0 + e] = rb[s0 + (nd0 + e) % L];
     }
   }
+  if (dchain0 && h->nel) std::memcpy(dchain0, h->adj_dch0.data(), sizeof(double) * h->nel);
+  h->adj_grad = true;
   // back to the final state of the forward run
   TRY(ckpt_load(h, h->adj_final));
   CK(h, cudaGetLastError());
+  return VLS_OK;
+}
+
+// <dL/df0, f(plus) - f(minus)> and <dL/dc0, c(plus) - c(minus)> for the last
+// backward pass's dL/df0 (still in ab_lam) and dL/dc0: f and c the
+// renormalised initial grid and chain values of two parameter sets, the grid
+// evaluated on the device (vls_profile.cu) into the backward's scratch
+// arrays, its mass by the reference's quadrature with the rows summed in
+// (j, u) order, the chain values on the host as vls_init_profile makes them
+extern "C" int vls_adjoint_init_dot(vls_handle *h, const vls_init_desc *plus,
+                                    const vls_init_desc *minus, double *dgrid, double *dchain) {
+  if (!h) return VLS_EINVAL;
+  if (!plus || !minus || !dgrid || !dchain)
+    return fail(h, VLS_EINVAL, "vls_adjoint_init_dot: NULL argument");
+  for (const vls_init_desc *d : {plus, minus})
+    if (d->type < VLS_INIT_UDF || d->type > VLS_INIT_HERNQUIST)
+      return fail(h, VLS_EINVAL, "unknown initial conditions type");
+  if (!h->adj_grad)
+    return fail(h, VLS_ESTATE, "vls_adjoint_init_dot before vls_adjoint_backward");
+  CK(h, cudaSetDevice(h->solver.device));
+  const Coords &c = h->co;
+  const size_t cells = h->cells, nrow = (size_t)c.nu * c.nj;
+  const int nb = profile_dot_blocks();
+  if (!h->ip_xyz) {
+    std::vector<double> xyz;
+    xyz.insert(xyz.end(), c.R.begin(), c.R.end());
+    xyz.insert(xyz.end(), c.U.begin(), c.U.end());
+    xyz.insert(xyz.end(), c.J.begin(), c.J.end());
+    xyz.insert(xyz.end(), c.JV.begin(), c.JV.end());
+    TRY(adj_alloc(h, &h->ip_xyz, xyz.size() * sizeof(double)));
+    TRY(adj_alloc(h, &h->ip_rows, nrow * sizeof(double)));
+    TRY(adj_alloc(h, &h->ip_part, (size_t)nb * sizeof(double)));
+    TRY(upload(h, h->ip_xyz, xyz.data(), xyz.size() * sizeof(double)));
+  }
+  double *fgrid[2] = {h->ab_Gb, h->ab_Cb};  // each holds at least one grid
+  double fac[2];
+  std::vector<double> vals[2];
+  std::vector<double> rows(nrow);
+  for (int s = 0; s < 2; ++s) {
+    const vls_init_desc &d = s ? *minus : *plus;
+    Profile pr;
+    pr.setup(d, h->solver.G);
+    ProfileConsts pc;
+    pc.type = pr.d.type;
+    pc.R0 = pr.d.R0;
+    pc.smoothingRadius = pr.d.smoothingRadius;
+    pc.gap0 = pr.d.gap[0];
+    pc.gap1 = pr.d.gap[1];
+    pc.n = pr.d.n;
+    pc.M = pr.d.M;
+    pc.Ra = pr.d.Ra;
+    pc.G = pr.G;
+    pc.C0 = pr.C0;
+    pc.C1 = pr.C1;
+    pc.C2 = pr.C2;
+    pc.Vg = pr.Vg;
+    CK(h, launch_profile_grid(pc, h->ip_xyz, fgrid[s], c.nr, c.nu, c.nj, h->st));
+    CK(h, launch_profile_rows(fgrid[s], h->ip_xyz, h->ip_rows, c.nr, c.nu, c.nj, h->st));
+    CK(h, cudaMemcpyAsync(rows.data(), h->ip_rows, nrow * sizeof(double),
+                          cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    double mass = 0.0;
+    for (size_t i = 0; i < nrow; ++i) mass += rows[i];
+    fac[s] = d.M > 0 ? d.M / mass : 1.0;
+    vals[s].assign((size_t)h->nel, 0.0);
+    for (int64_t k = 0; k < h->nch; k++) {
+      const int j = (int)(h->ch_cell_h[k] / ((int64_t)c.nr * c.nu));
+      const int64_t s0 = h->ch_start_h[k];
+      for (int32_t e = 0; e + 1 < h->ch_len_h[k]; e++)
+        vals[s][s0 + e] = pr.value(h->ch_R_h[s0 + e], h->ch_U_h[s0 + e], c.J[j]) * fac[s];
+    }
+  }
+  std::vector<double> part((size_t)nb);
+  CK(h, launch_profile_dot(h->ab_lam, fgrid[0], fgrid[1], fac[0], fac[1], cells, h->ip_part,
+                           h->st));
+  CK(h, cudaMemcpyAsync(part.data(), h->ip_part, (size_t)nb * sizeof(double),
+                        cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  double dg = 0.0;
+  for (int b = 0; b < nb; ++b) dg += part[b];
+  double dc = 0.0;
+  for (int64_t i = 0; i < h->nel; ++i) dc += h->adj_dch0[i] * (vals[0][i] - vals[1][i]);
+  *dgrid = dg;
+  *dchain = dc;
   return VLS_OK;
 }
 

@@ -226,4 +226,21 @@ template <typename T>
 cudaError_t launch_nonfinite(const T *f, size_t n, unsigned int *flag,
                              cudaStream_t st);
 
+// analytic initial profiles on the device (vls_profile.cu): the constants
+// Profile::setup derives (vls_setup.cpp), the type a VLS_INIT_* value
+struct ProfileConsts {
+  int type;
+  double R0, smoothingRadius, gap0, gap1, n, M, Ra, G, C0, C1, C2, Vg;
+};
+// f of every cell from the coordinates xyz = R (nr), U (nu), J (nj), JV (nj + 1)
+cudaError_t launch_profile_grid(const ProfileConsts &p, const double *xyz, double *f, int nr,
+                                int nu, int nj, cudaStream_t st);
+// the mass quadrature of each (j, u) row of f (rows: nu * nj)
+cudaError_t launch_profile_rows(const double *f, const double *xyz, double *rows, int nr,
+                                int nu, int nj, cudaStream_t st);
+// partial sums (profile_dot_blocks() of them) of w (a fp - b fm) over n cells
+int profile_dot_blocks();
+cudaError_t launch_profile_dot(const double *w, const double *fp, const double *fm, double a,
+                               double b, size_t n, double *partial, cudaStream_t st);
+
 }  // namespace vls

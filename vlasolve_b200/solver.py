@@ -422,6 +422,28 @@ class VlasovSolver21Spline:
         from free device memory; vls_adjoint_set_inner)."""
         self._ck(self._L.vls_adjoint_set_inner(self._h, int(inner_every)))
 
+    def init_desc(self, **kw) -> "_lib.InitDesc":
+        """A copy of the handle's init.* parameters with some changed."""
+        d = _lib.InitDesc()
+        ctypes.pointer(d)[0] = self._init_desc
+        for k, v in kw.items():
+            if not hasattr(d, k):
+                raise KeyError(k)
+            setattr(d, k, v)
+            if k == "R0":
+                d.R0_given = 1
+        return d
+
+    def adjoint_init_dot(self, plus: dict, minus: dict):
+        """(<dL/df0, f(plus) - f(minus)>, <dL/dc0, c(plus) - c(minus)>) for the
+        last adjoint_backward and the initial states of two sets of init.*
+        parameters (vls_adjoint_init_dot)."""
+        dg, dc = ctypes.c_double(), ctypes.c_double()
+        self._ck(self._L.vls_adjoint_init_dot(self._h, ctypes.byref(self.init_desc(**plus)),
+                                              ctypes.byref(self.init_desc(**minus)),
+                                              ctypes.byref(dg), ctypes.byref(dc)))
+        return dg.value, dc.value
+
     def adjoint_inner_used(self) -> int:
         """Second-level spacing the last backward pass used (0: one level)."""
         v = ctypes.c_int32()
