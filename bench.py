@@ -503,7 +503,7 @@ def adjoint_block(nsteps, K):
                          - np.linalg.norm(p.run(tm) - target)) / (2 * h)
             out["fd_grad"] = fd.tolist()
             out["fp64_vs_fd_rel"] = float(np.max(np.abs(grads["fp64"] - fd)) / np.max(np.abs(fd)))
-        p.solver.close()
+        p.close()
     out["fp32_vs_fp64_rel"] = float(np.max(np.abs(grads["fp32"] - grads["fp64"]))
                                     / np.max(np.abs(grads["fp64"])))
     out["seconds"] = time.perf_counter() - t_all
@@ -606,11 +606,9 @@ def large_block(nsteps, K):
     out["backward_s"] = t3 - t2
     out["hbm_gb"] = {"step_handle_forward": fwd_bytes / 1e9,
                      "step_handle_with_adjoint": s.device_bytes() / 1e9,
-                     "initial_state_handle_fp64": p.ic.device_bytes() / 1e9,
                      "device_used_after_backward": (total - free1) / 1e9,
                      "device_used_before": (total - free0) / 1e9}
-    p.ic.close()
-    s.close()
+    p.close()
     del p
     # gradient of the FP32-storage adjoint against the FP64 adjoint, 257 x 257 x 128
     grads, rhos = {}, {}
@@ -625,9 +623,7 @@ def large_block(nsteps, K):
         Lq = torch.linalg.norm(rq - torch.as_tensor(tgt))
         Lq.backward()
         grads[prec] = th.grad.numpy().copy()
-        if q.ic is not q.solver:
-            q.ic.close()
-        q.solver.close()
+        q.close()
     # the loss differences rho - rho_target, which are 1e-2 of rho, so the FP32
     # storage's error in rho reaches the gradient amplified by
     # ||rho|| / ||rho - rho_target||

@@ -37,15 +37,30 @@ class DensityProblem:
         # second-level checkpoint spacing of the backward pass (0: chosen from
         # free device memory)
         self.solver.adjoint_set_inner(inner_every)
-        # the initial-state map is differenced in FP64 whatever the storage
-        # precision (differences of FP32-rounded grids would lose the digits)
-        self.ic = (self.solver if precision == "fp64" else
-                   VlasovSolver21Spline(cfg, precision="fp64", device=device, init=False))
+        # initial_state() makes FP64 grids whatever the storage precision: an
+        # FP64 handle of its own for FP32 storage, created on first use
+        self._cfg, self._device, self._precision = cfg, device, precision
+        self._ic = self.solver if precision == "fp64" else None
         self.nsteps, self.K = int(nsteps), int(checkpoint_every)
         self.params = tuple(params)
         self.ic_step = ic_step
         self.vol = None
         self.theta = None
+
+    @property
+    def ic(self) -> VlasovSolver21Spline:
+        """The FP64 handle initial_state() evaluates on."""
+        if self._ic is None:
+            self._ic = VlasovSolver21Spline(self._cfg, precision="fp64", device=self._device,
+                                            init=False)
+        return self._ic
+
+    def close(self):
+        """Frees the device memory of the handles."""
+        if self._ic is not None and self._ic is not self.solver:
+            self._ic.close()
+        self._ic = None
+        self.solver.close()
 
     def initial_state(self, theta):
         """FP64 initial grid and chain values for parameters theta."""
