@@ -423,7 +423,8 @@ def adjoint_block(nsteps, K):
     final radial density; gradient by the adjoint (FP64 and FP32 storage)
     against central differences of full FP64 runs (h = 1e-4).  Times: the
     whole backward pass of the autograd function (step adjoint plus the
-    initial-state map), the step adjoint alone (vls_adjoint_backward, with
+    initial-state map; median of three, and the first), the step adjoint
+    alone (vls_adjoint_backward, with
     its recomputation), and the plain forward of the same steps, the last two
     as device time on the solver's stream (and wall time), medians of three
     runs each; adjoint_over_forward is the step adjoint over that forward."""
@@ -441,17 +442,27 @@ def adjoint_block(nsteps, K):
     for prec in ("fp64", "fp32"):
         p = DensityProblem(ADJOINT, precision=prec, nsteps=nsteps, checkpoint_every=K)
         target = p.run(theta + dtheta) if prec == "fp64" else target
-        th = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        rho = final_density(th, p)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        L = torch.linalg.norm(rho - torch.as_tensor(target))
-        L.backward()
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        grads[prec] = th.grad.numpy().copy()
+        # the autograd forward and backward three times (wall time; the first
+        # backward also builds the inverse footpoint map), the medians reported
+        fwd_wall, bwd_wall = [], []
+        for rep in range(3):
+            th = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rho = final_density(th, p)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            L = torch.linalg.norm(rho - torch.as_tensor(target))
+            L.backward()
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            fwd_wall.append(t1 - t0)
+            bwd_wall.append(t2 - t1)
+            if rep == 0:
+                grads[prec] = th.grad.numpy().copy()
+                repeatable = True
+            else:
+                repeatable &= bool(np.array_equal(th.grad.numpy(), grads[prec]))
         # the step adjoint alone (recomputation included, initial-state map
         # excluded): three more backward passes with the same seed, and three
         # plain forward runs of the same steps; the medians are reported
@@ -485,7 +496,9 @@ def adjoint_block(nsteps, K):
         # device times (CUDA events on the solver's stream) and the wall times
         # around the same calls (host launch overhead included)
         out[prec] = {"grad": grads[prec].tolist(), "loss": float(L.detach()),
-                     "forward_checkpointed_s": t1 - t0, "backward_s": t2 - t1,
+                     "forward_checkpointed_s": float(np.median(fwd_wall)),
+                     "backward_s": float(np.median(bwd_wall)),
+                     "backward_first_s": bwd_wall[0], "grad_bitwise_repeatable": repeatable,
                      "step_adjoint_s": adj_dev, "forward_s": fwd_dev,
                      "step_adjoint_runs_s": [a[0] for a in adj],
                      "forward_runs_s": [f[0] for f in fwd],
