@@ -235,6 +235,17 @@ class vlasovSolver21_spline {
   }
   // second checkpoint level inside a segment (0: chosen from free memory)
   void adjointSetInner(int innerEvery) { check(vls_adjoint_set_inner(h_, innerEvery), h_); }
+  // for d/d(init.* parameter) by central differences: <dL/df0, f(plus) -
+  // f(minus)> + <dL/dc0, c(plus) - c(minus)> for the last adjointBackward,
+  // the two initial states made and contracted on the device
+  double adjointInitDot(const vls_init_desc &plus, const vls_init_desc &minus) {
+    double dg = 0, dc = 0;
+    check(vls_adjoint_init_dot(h_, &plus, &minus, &dg, &dc), h_);
+    return dg + dc;
+  }
+  // the mass of the most recent step, copied to *pinnedDst without waiting
+  // (valid after the next synchronising call)
+  void lastMassAsync(double *pinnedDst) { check(vls_last_mass_async(h_, pinnedDst), h_); }
   // device memory the handle holds (also its peak)
   size_t deviceBytes() {
     size_t b = 0;

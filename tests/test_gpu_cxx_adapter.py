@@ -1,7 +1,7 @@
 """The header-only C++ adapter (include/vlasolve_b200.hpp): a small program
 built against it runs the UDF profile, steps, and takes the adjoint of the
-steps through the adapter's methods; its grid and gradients equal those of
-the Python mirror of the same C-ABI calls."""
+steps through the adapter's methods; its grid, gradients and initial-state
+contraction equal those of the Python mirror of the same C-ABI calls."""
 import os
 import subprocess
 
@@ -32,9 +32,14 @@ int main(int argc, char **argv) {
   for (size_t r = 0; r < dbins.size(); ++r) dbins[r] = 0.1 * (double)r;
   solver.adjointSetInner(2);  // second checkpoint level inside each segment
   solver.adjointBackward(dbins, df0, &dch);
+  vls_init_desc plus = init, minus = init;
+  plus.alpha = init.alpha * (1 + 1e-6);
+  minus.alpha = init.alpha * (1 - 1e-6);
+  const double idot = solver.adjointInitDot(plus, minus);
   FILE *o = std::fopen(argv[1], "wb");
   size_t n[3] = {f.size(), df0.size(), dch.size()};
   std::fwrite(n, sizeof(size_t), 3, o);
+  std::fwrite(&idot, sizeof(double), 1, o);
   std::fwrite(f.data(), sizeof(double), f.size(), o);
   std::fwrite(df0.data(), sizeof(double), df0.size(), o);
   std::fwrite(dch.data(), sizeof(double), dch.size(), o);
@@ -61,7 +66,8 @@ def test_cxx_adapter_adjoint_matches_python(tmp_path):
     assert int(r.stdout.split()[-1]) > 0
     raw = out.read_bytes()
     n = np.frombuffer(raw[:24], dtype=np.uint64)
-    vals = np.frombuffer(raw[24:], dtype=np.float64)
+    idot_c = float(np.frombuffer(raw[24:32], dtype=np.float64)[0])
+    vals = np.frombuffer(raw[32:], dtype=np.float64)
     f_c = vals[:n[0]]
     df0_c = vals[n[0]:n[0] + n[1]]
     dch_c = vals[n[0] + n[1]:]
@@ -79,6 +85,11 @@ def test_cxx_adapter_adjoint_matches_python(tmp_path):
     if dch.size:
         np.testing.assert_allclose(dch_c, dch, rtol=1e-12,
                                    atol=1e-14 * max(np.max(np.abs(dch)), 1e-300))
+    # the initial-state contraction through the adapter and through Python
+    a = s.init_desc().alpha
+    dg, dc = s.adjoint_init_dot({"alpha": a * (1 + 1e-6)}, {"alpha": a * (1 - 1e-6)})
+    assert idot_c != 0.0
+    np.testing.assert_allclose(idot_c, dg + dc, rtol=1e-12)
 
 
 SPLINE_PROGRAM = r"""
